@@ -1,0 +1,218 @@
+/*
+ * pst_c.h - C ABI of the B200 static priority search tree library (libpst_b200.so).
+ *
+ * Plain C types only: device pointers are void*, sizes are uint64_t, streams are
+ * cudaStream_t-compatible handles (NULL = the legacy default stream).  Every
+ * function returns a pst_status and never throws; pst_last_error() gives the
+ * calling thread's last error message.
+ *
+ * Each entry point names the reference interface it replaces (paths relative to
+ * the reference project, arraylistnumstring/static-priority-search-tree).  The
+ * reference exposes C++ class templates only; these are the calls a binding for
+ * that surface binds, and the C++ facade in
+ * static-priority-search-tree_b200/cpp/static-pst-gpu.h re-creates the
+ * reference's template signatures on top of them.
+ *
+ * Point records are the reference's PointStruct layouts
+ * (helpers/point-struct.h:25-33, :106-117):
+ *   PST_ID_U32:  { T dim1_val; T dim2_val; uint32_t id; }  (natural alignment)
+ *   PST_ID_NONE: { T dim1_val; T dim2_val; }
+ * Result sets are bit-exact with the reference's StaticPSTCPUIter; their order
+ * on the GPU is unspecified, as it is in the reference's GPU searches.
+ */
+#ifndef PST_C_H
+#define PST_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *pst_stream_t;
+
+typedef enum pst_status {
+	PST_OK = 0,
+	PST_ERR_INVALID = 1,     /* bad argument (null handle, dtype, sizes) */
+	PST_ERR_CUDA = 2,        /* a CUDA runtime call failed, or no CUDA device */
+	PST_ERR_NOMEM = 3,       /* device memory allocation failed */
+	PST_ERR_CAPACITY = 4,    /* caller-provided output buffer too small */
+	PST_ERR_UNSUPPORTED = 5, /* combination not supported (e.g. ids from an id-less tree) */
+	PST_ERR_INTERNAL = 6,    /* a device-side consistency check failed */
+	PST_ERR_BUSY = 7,        /* server queue full / request not admitted */
+	PST_ERR_TIMEOUT = 8      /* a bounded wait ran out */
+} pst_status;
+
+typedef enum pst_dtype { PST_F32 = 0, PST_F64 = 1, PST_I32 = 2 } pst_dtype;
+typedef enum pst_idtype { PST_ID_NONE = 0, PST_ID_U32 = 1 } pst_idtype;
+/* RetType of the reference searches: IDType or the whole PointStruct. */
+typedef enum pst_ret { PST_RET_IDS = 0, PST_RET_POINTS = 1 } pst_ret;
+typedef enum pst_qkind { PST_Q_THREE = 0, PST_Q_LEFT = 1, PST_Q_RIGHT = 2 } pst_qkind;
+
+/* A bound in the tree's value type. */
+typedef union pst_value {
+	float f32;
+	double f64;
+	int32_t i32;
+} pst_value;
+
+/* One query.  THREE: min1 <= dim1 <= max1 and dim2 >= min2;
+ * LEFT: dim1 <= max1 and dim2 >= min2; RIGHT: dim1 >= min1 and dim2 >= min2.
+ * Bounds a kind does not use are ignored. */
+typedef struct pst_query {
+	int32_t kind;
+	int32_t reserved;
+	pst_value min1, max1, min2;
+} pst_query;
+
+typedef struct pst_tree pst_tree;
+typedef struct pst_batch pst_batch;
+
+/* ------------------------------------------------------------------------- */
+/* Library                                                                    */
+
+const char *pst_last_error(void);
+const char *pst_version(void);
+/* sizeof the PointStruct record for (dtype, idtype); 0 for an invalid pair. */
+size_t pst_point_size(pst_dtype dtype, pst_idtype idtype);
+
+/* cudaFree of a buffer a drop-in call allocated (pst_search, pst_ips_search), for
+ * bindings that do not link the CUDA runtime themselves.  The reference's callers
+ * free those results with cudaFree (testers/pst-tester-functions.tu:711-713). */
+pst_status pst_free(void *ptr_d);
+
+/* ------------------------------------------------------------------------- */
+/* Tree                                                                       */
+
+/* Device bytes needed to build and hold a tree of n points, including the
+ * construction working set.  Replaces StaticPSTGPU::calcGlobalMemNeeded
+ * (pst/static-pst-gpu.h:132, pst/static-pst-gpu.tu:648-671). */
+pst_status pst_mem_needed(pst_dtype dtype, pst_idtype idtype, uint64_t n, uint64_t *bytes);
+
+/* Builds a tree from n PointStruct records in device memory.  The input is only
+ * read; the tree keeps its own copy of the values.  Returns after construction
+ * has completed.  n == 0 gives an empty tree.  Replaces the StaticPSTGPU
+ * constructor (pst/static-pst-gpu.h:76-78, pst/static-pst-gpu.tu:21-437) and the
+ * StaticPSTGPUArr constructor (pst/static-pst-gpu-arr.h:51-54). */
+pst_status pst_create(pst_tree **out, pst_dtype dtype, pst_idtype idtype, const void *pts_d,
+                      uint64_t n, pst_stream_t stream);
+
+/* Frees the tree.  Replaces ~StaticPSTGPU (pst/static-pst-gpu.h:80-88). */
+pst_status pst_destroy(pst_tree *tree);
+
+/* Tree facts: number of points, levels, slots of the reference's layout
+ * (2^levels - 1), device bytes held.  Any output pointer may be NULL.
+ * Replaces the getters of pst/static-pst-gpu.h:96-98 and the slot count of
+ * pst/static-pst-gpu.h:345-353. */
+pst_status pst_info(const pst_tree *tree, uint64_t *n, uint32_t *levels, uint64_t *slots,
+                    uint64_t *device_bytes, pst_dtype *dtype, pst_idtype *idtype);
+
+/* Copies the tree to host buffers in the reference's field layout (slot s = heap
+ * index with the root at 0; each array holds `slots` entries; ids may be NULL for
+ * an id-less tree).  Unused slots are zero, as in the reference's value-initialised
+ * allocation.  This is the data StaticPSTGPU::print walks
+ * (pst/static-pst-gpu.h:93, pst/static-pst-gpu.tu:440-483). */
+pst_status pst_export(const pst_tree *tree, void *dim1, void *dim2, void *med, uint32_t *ids,
+                      uint8_t *bitcodes);
+
+/* One query, drop-in mode: allocates the result with cudaMalloc (exactly *count
+ * records; the caller frees it with cudaFree), blocks until the result is
+ * complete, and sets *out_d = NULL, *count = 0 for an empty tree or an empty
+ * result.  Replaces StaticPSTGPU::threeSidedSearch / twoSidedLeftSearch /
+ * twoSidedRightSearch (pst/static-pst-gpu.h:103-128, pst/static-pst-gpu.tu:496-642)
+ * and StaticPSTGPUArr::twoSidedLeftSearch (pst/static-pst-gpu-arr.h:85-91). */
+pst_status pst_search(pst_tree *tree, const pst_query *query, pst_ret ret, void **out_d,
+                      uint64_t *count, pst_stream_t stream);
+
+/* The three reference search calls with the reference's bound order. */
+pst_status pst_three_sided(pst_tree *tree, pst_value min1, pst_value max1, pst_value min2,
+                           pst_ret ret, void **out_d, uint64_t *count, pst_stream_t stream);
+pst_status pst_two_sided_left(pst_tree *tree, pst_value max1, pst_value min2, pst_ret ret,
+                              void **out_d, uint64_t *count, pst_stream_t stream);
+pst_status pst_two_sided_right(pst_tree *tree, pst_value min1, pst_value min2, pst_ret ret,
+                               void **out_d, uint64_t *count, pst_stream_t stream);
+
+/* One query into a caller buffer of `capacity` records.  *count always receives
+ * the full result size; PST_ERR_CAPACITY (nothing written) when it exceeds
+ * capacity.  Blocks until complete.  No reference counterpart takes a caller
+ * buffer; this is the search of pst/static-pst-gpu.tu:548-591 without its
+ * per-call cudaMalloc. */
+pst_status pst_search_into(pst_tree *tree, const pst_query *query, pst_ret ret, void *out_d,
+                           uint64_t capacity, uint64_t *count, pst_stream_t stream);
+
+/* ------------------------------------------------------------------------- */
+/* Batched queries: many queries of mixed kinds in one level-synchronous pass
+ * (count prepass, exact offsets, emit), replayed from a captured CUDA graph.
+ * The reference has one query per launch (pst/static-pst-gpu.tu:496-642); this
+ * is the batched form of the same searches. */
+
+typedef struct pst_batch_opts {
+	uint32_t max_queries;      /* capacity of the query buffer */
+	uint64_t task_capacity;    /* initial frontier capacity in 32-slot chunks (0 = auto) */
+	uint32_t block_threads;    /* 0 = autotuned */
+	uint32_t blocks_per_sm;    /* 0 = autotuned */
+	int32_t use_graph;         /* replay the pass from a captured CUDA graph */
+} pst_batch_opts;
+
+pst_status pst_batch_create(pst_batch **out, pst_tree *tree, const pst_batch_opts *opts);
+pst_status pst_batch_destroy(pst_batch *batch);
+
+/* Runs nq queries (host or device array of pst_query).  Results of query i are
+ * records [offsets[i], offsets[i+1]) of out_d; offsets_d receives nq + 1 uint64
+ * values (device memory).  *total (host) receives the number of records.  When
+ * the result exceeds out_capacity records, nothing is written to out_d,
+ * offsets are still valid and PST_ERR_CAPACITY is returned.  sync = 0 makes the
+ * call asynchronous on `stream` (then *total is only valid after a stream sync
+ * and capacity overflow is reported by pst_batch_status). */
+pst_status pst_batch_run(pst_batch *batch, const pst_query *queries, uint32_t nq, int queries_on_device,
+                         pst_ret ret, void *out_d, uint64_t out_capacity, uint64_t *offsets_d,
+                         uint64_t *total, int sync, pst_stream_t stream);
+
+/* Count prepass only: per-query result sizes into counts_d (nq uint64 values,
+ * device memory; may be NULL).  Blocks until complete. */
+pst_status pst_batch_count(pst_batch *batch, const pst_query *queries, uint32_t nq, int queries_on_device,
+                           uint64_t *counts_d, uint64_t *total, pst_stream_t stream);
+
+/* After an asynchronous run: PST_OK, PST_ERR_CAPACITY or PST_ERR_INTERNAL. */
+pst_status pst_batch_status(pst_batch *batch, uint64_t *total);
+
+/* ------------------------------------------------------------------------- */
+/* Interval parallel search: every point with dim1 <= v <= dim2, by a full scan.
+ * Drop-in mode: like the reference, the result buffer is cudaMalloc'd with room
+ * for all n points (the caller frees it) and *count records are valid; it is
+ * NULL for n == 0.  Blocks until complete.
+ * Replaces intervalParallelSearch (interval-parallel-search/interval-parallel-search.h:29-66);
+ * num_blocks is a launch hint (0 = automatic), threads_per_block is ignored. */
+pst_status pst_ips_search(pst_dtype dtype, pst_idtype idtype, const void *pts_d, uint64_t n,
+                          pst_value v, pst_ret ret, void **out_d, uint64_t *count,
+                          uint32_t num_blocks, uint32_t threads_per_block, pst_stream_t stream);
+
+/* Same scan into a caller buffer of `capacity` records (PST_ERR_CAPACITY when the
+ * result is larger; *count is the full size either way). */
+pst_status pst_ips_search_into(pst_dtype dtype, pst_idtype idtype, const void *pts_d, uint64_t n,
+                               pst_value v, pst_ret ret, void *out_d, uint64_t capacity,
+                               uint64_t *count, pst_stream_t stream);
+
+/* ------------------------------------------------------------------------- */
+/* Metacell formation over a scalar vertex volume (x fastest, then y, then z).  */
+
+/* Metacell grid dims and count: ceil((pt_dims[i] - 1) / mc_dims[i]) per axis.
+ * Replaces calcNumMetacells (helpers/isosurface-data-processing.h:23-36). */
+pst_status pst_num_metacells(const uint32_t pt_dims[3], const uint32_t mc_dims[3],
+                             uint32_t mc_grid[3], uint64_t *n_metacells);
+
+/* Writes one PointStruct (min vertex value, max vertex value[, id]) per metacell,
+ * at index id = mx + (my + mz*My)*Mx, into out_d (device, n_metacells records).
+ * A metacell covers the vertices [m*mc, min(m*mc + mc, P - 1)] of each axis.
+ * Replaces formMetacellTags (helpers/isosurface-data-processing.h:69-137) and,
+ * with mc_dims = {1,1,1}, formVoxelTags (:140-203). */
+pst_status pst_form_metacells(pst_dtype dtype, pst_idtype idtype, const void *vert_d,
+                              const uint32_t pt_dims[3], const uint32_t mc_dims[3], void *out_d,
+                              pst_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PST_C_H */

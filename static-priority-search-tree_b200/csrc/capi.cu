@@ -1,0 +1,539 @@
+// C ABI (include/pst_c.h): argument checks, error translation, and the drop-in
+// search semantics of the reference (callee-allocated results, blocking calls).
+#include <cstdio>
+#include <memory>
+#include <new>
+#include <string>
+
+#include "scan_kernels.cuh"
+#include "search.cuh"
+#include "tree.cuh"
+
+struct pst_tree {
+	pst::TreeStorage t;
+};
+
+struct pst_batch {
+	pst::Batch b;
+	pst_tree *tree;
+};
+
+namespace pst {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void fail(pst_status st, const std::string &msg) { throw Error{st, msg}; }
+
+void check_cuda(cudaError_t e, const char *what)
+{
+	if (e == cudaSuccess)
+		return;
+	cudaGetLastError();
+	fail(e == cudaErrorMemoryAllocation ? PST_ERR_NOMEM : PST_ERR_CUDA,
+	     std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+}
+
+const DeviceInfo &device_info()
+{
+	static thread_local DeviceInfo cache[64];
+	static thread_local bool have[64] = {};
+	int dev = 0;
+	check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+	if (dev < 0 || dev >= 64)
+		fail(PST_ERR_CUDA, "device index out of range");
+	if (!have[dev]) {
+		DeviceInfo d{};
+		d.device = dev;
+		check_cuda(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+		int smem = 0;
+		check_cuda(cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "cudaDeviceGetAttribute");
+		d.smem_optin = (size_t) smem;
+		cache[dev] = d;
+		have[dev] = true;
+	}
+	return cache[dev];
+}
+
+static void require_device()
+{
+	int n = 0;
+	cudaError_t e = cudaGetDeviceCount(&n);
+	if (e != cudaSuccess || n == 0) {
+		cudaGetLastError();
+		fail(PST_ERR_CUDA, std::string("no CUDA device available: ") + cudaGetErrorString(e));
+	}
+}
+
+static void check_types(pst_dtype dt, pst_idtype it)
+{
+	if (point_size(dt, it) == 0)
+		fail(PST_ERR_INVALID, "invalid dtype/idtype");
+}
+
+static pst_status translate(const std::exception_ptr &ep)
+{
+	try {
+		std::rethrow_exception(ep);
+	} catch (const Error &e) {
+		g_last_error = e.msg;
+		return e.status;
+	} catch (const std::bad_alloc &) {
+		g_last_error = "host allocation failed";
+		return PST_ERR_NOMEM;
+	} catch (const std::exception &e) {
+		g_last_error = e.what();
+		return PST_ERR_INTERNAL;
+	} catch (...) {
+		g_last_error = "unknown error";
+		return PST_ERR_INTERNAL;
+	}
+}
+
+template <typename F>
+static pst_status guarded(F &&f)
+{
+	try {
+		f();
+		g_last_error.clear();
+		return PST_OK;
+	} catch (...) {
+		return translate(std::current_exception());
+	}
+}
+
+static void malloc_result(void **out, uint64_t bytes)
+{
+	cudaError_t e = cudaMalloc(out, bytes);
+	if (e != cudaSuccess) {
+		*out = nullptr;
+		check_cuda(e, "cudaMalloc(result)");
+	}
+}
+
+static Batch &single_engine(pst_tree *tr)
+{
+	if (!tr->t.single) {
+		pst_batch_opts o{};
+		o.max_queries = 1;
+		o.use_graph = 1;
+		auto *b = new Batch();
+		try {
+			b->init(&tr->t, o);
+		} catch (...) {
+			delete b;
+			throw;
+		}
+		tr->t.single = b;
+	}
+	return *tr->t.single;
+}
+
+// One query; out_d either caller-owned (capacity) or allocated here (alloc = true).
+static uint64_t run_single(pst_tree *tr, const pst_query *q, pst_ret ret, void **out_d, uint64_t capacity, bool alloc,
+                           cudaStream_t s)
+{
+	if (!tr || !q)
+		fail(PST_ERR_INVALID, "null tree or query");
+	if (q->kind < PST_Q_THREE || q->kind > PST_Q_RIGHT)
+		fail(PST_ERR_INVALID, "query kind must be PST_Q_THREE, PST_Q_LEFT or PST_Q_RIGHT");
+	if (ret != PST_RET_IDS && ret != PST_RET_POINTS)
+		fail(PST_ERR_INVALID, "bad return type");
+	if (ret == PST_RET_IDS && tr->t.idtype != PST_ID_U32)
+		fail(PST_ERR_UNSUPPORTED, "an id-less tree can only return points");
+	if (alloc)
+		*out_d = nullptr;
+	if (tr->t.n == 0)
+		return 0;
+	std::lock_guard<std::mutex> lk(tr->t.mu);
+	Batch &b = single_engine(tr);
+	b.stage_queries(q, 1, false, s);
+	uint64_t total = 0;
+	b.count_sync(s, &total);
+	if (total == 0)
+		return 0;
+	if (alloc) {
+		malloc_result(out_d, total * b.record_size(ret));
+	} else if (total > capacity) {
+		return total;
+	}
+	b.enqueue_emit(ret, *out_d, alloc ? total : capacity, s);
+	uint64_t t2 = 0;
+	const pst_status st = b.read_ctl(s, &t2);
+	if (st != PST_OK) {
+		if (alloc) {
+			cudaFree(*out_d);
+			*out_d = nullptr;
+		}
+		fail(st, "search emit failed");
+	}
+	return total;
+}
+
+}  // namespace pst
+
+using namespace pst;
+
+extern "C" {
+
+const char *pst_last_error(void) { return g_last_error.c_str(); }
+
+const char *pst_version(void) { return "pst_b200 1.0 (sm_100a)"; }
+
+size_t pst_point_size(pst_dtype dtype, pst_idtype idtype) { return point_size(dtype, idtype); }
+
+pst_status pst_free(void *ptr_d)
+{
+	return guarded([&] {
+		if (ptr_d)
+			check_cuda(cudaFree(ptr_d), "cudaFree");
+	});
+}
+
+pst_status pst_mem_needed(pst_dtype dtype, pst_idtype idtype, uint64_t n, uint64_t *bytes)
+{
+	return guarded([&] {
+		check_types(dtype, idtype);
+		if (!bytes)
+			fail(PST_ERR_INVALID, "null output");
+		*bytes = build_bytes_needed(dtype, idtype, n);
+	});
+}
+
+pst_status pst_create(pst_tree **out, pst_dtype dtype, pst_idtype idtype, const void *pts_d, uint64_t n,
+                      pst_stream_t stream)
+{
+	return guarded([&] {
+		if (!out)
+			fail(PST_ERR_INVALID, "null output handle");
+		*out = nullptr;
+		check_types(dtype, idtype);
+		require_device();
+		auto tr = std::make_unique<pst_tree>();
+		tr->t.dtype = dtype;
+		tr->t.idtype = idtype;
+		check_cuda(cudaGetDevice(&tr->t.device), "cudaGetDevice");
+		build_tree(tr->t, pts_d, n, reinterpret_cast<cudaStream_t>(stream));
+		*out = tr.release();
+	});
+}
+
+pst_status pst_destroy(pst_tree *tree)
+{
+	return guarded([&] {
+		if (!tree)
+			return;
+		delete tree->t.single;
+		tree->t.single = nullptr;
+		free_tree(tree->t);
+		delete tree;
+	});
+}
+
+pst_status pst_info(const pst_tree *tree, uint64_t *n, uint32_t *levels, uint64_t *slots, uint64_t *device_bytes,
+                    pst_dtype *dtype, pst_idtype *idtype)
+{
+	return guarded([&] {
+		if (!tree)
+			fail(PST_ERR_INVALID, "null tree");
+		if (n)
+			*n = tree->t.n;
+		if (levels)
+			*levels = tree->t.levels;
+		if (slots)
+			*slots = tree->t.levels ? (1ull << tree->t.levels) - 1 : 0;
+		if (device_bytes)
+			*device_bytes = tree->t.bytes;
+		if (dtype)
+			*dtype = tree->t.dtype;
+		if (idtype)
+			*idtype = tree->t.idtype;
+	});
+}
+
+pst_status pst_export(const pst_tree *tree, void *dim1, void *dim2, void *med, uint32_t *ids, uint8_t *bitcodes)
+{
+	return guarded([&] {
+		if (!tree)
+			fail(PST_ERR_INVALID, "null tree");
+		if (tree->t.n && (!dim1 || !dim2 || !med || !bitcodes || (tree->t.idtype == PST_ID_U32 && !ids)))
+			fail(PST_ERR_INVALID, "null export buffer");
+		export_tree(tree->t, dim1, dim2, med, tree->t.idtype == PST_ID_U32 ? ids : nullptr, bitcodes);
+	});
+}
+
+pst_status pst_search(pst_tree *tree, const pst_query *query, pst_ret ret, void **out_d, uint64_t *count,
+                      pst_stream_t stream)
+{
+	return guarded([&] {
+		if (!out_d || !count)
+			fail(PST_ERR_INVALID, "null output");
+		*count = 0;
+		*count = run_single(tree, query, ret, out_d, 0, true, reinterpret_cast<cudaStream_t>(stream));
+	});
+}
+
+pst_status pst_three_sided(pst_tree *tree, pst_value min1, pst_value max1, pst_value min2, pst_ret ret, void **out_d,
+                           uint64_t *count, pst_stream_t stream)
+{
+	pst_query q{};
+	q.kind = PST_Q_THREE;
+	q.min1 = min1;
+	q.max1 = max1;
+	q.min2 = min2;
+	return pst_search(tree, &q, ret, out_d, count, stream);
+}
+
+pst_status pst_two_sided_left(pst_tree *tree, pst_value max1, pst_value min2, pst_ret ret, void **out_d,
+                              uint64_t *count, pst_stream_t stream)
+{
+	pst_query q{};
+	q.kind = PST_Q_LEFT;
+	q.max1 = max1;
+	q.min2 = min2;
+	return pst_search(tree, &q, ret, out_d, count, stream);
+}
+
+pst_status pst_two_sided_right(pst_tree *tree, pst_value min1, pst_value min2, pst_ret ret, void **out_d,
+                               uint64_t *count, pst_stream_t stream)
+{
+	pst_query q{};
+	q.kind = PST_Q_RIGHT;
+	q.min1 = min1;
+	q.min2 = min2;
+	return pst_search(tree, &q, ret, out_d, count, stream);
+}
+
+pst_status pst_search_into(pst_tree *tree, const pst_query *query, pst_ret ret, void *out_d, uint64_t capacity,
+                           uint64_t *count, pst_stream_t stream)
+{
+	uint64_t total = 0;
+	pst_status st = guarded([&] {
+		if (!count)
+			fail(PST_ERR_INVALID, "null count");
+		void *o = out_d;
+		total = run_single(tree, query, ret, &o, capacity, false, reinterpret_cast<cudaStream_t>(stream));
+		*count = total;
+	});
+	if (st == PST_OK && total > capacity) {
+		g_last_error = "result of " + std::to_string(total) + " records exceeds capacity " + std::to_string(capacity);
+		return PST_ERR_CAPACITY;
+	}
+	return st;
+}
+
+pst_status pst_batch_create(pst_batch **out, pst_tree *tree, const pst_batch_opts *opts)
+{
+	return guarded([&] {
+		if (!out || !tree)
+			fail(PST_ERR_INVALID, "null argument");
+		*out = nullptr;
+		pst_batch_opts o{};
+		if (opts)
+			o = *opts;
+		else
+			o.use_graph = 1;
+		if (o.max_queries == 0)
+			fail(PST_ERR_INVALID, "max_queries must be positive");
+		auto b = std::make_unique<pst_batch>();
+		b->tree = tree;
+		b->b.init(&tree->t, o);
+		*out = b.release();
+	});
+}
+
+pst_status pst_batch_destroy(pst_batch *batch)
+{
+	return guarded([&] { delete batch; });
+}
+
+pst_status pst_batch_run(pst_batch *batch, const pst_query *queries, uint32_t nq, int queries_on_device, pst_ret ret,
+                         void *out_d, uint64_t out_capacity, uint64_t *offsets_d, uint64_t *total, int sync,
+                         pst_stream_t stream)
+{
+	pst_status result = PST_OK;
+	pst_status st = guarded([&] {
+		if (!batch)
+			fail(PST_ERR_INVALID, "null batch");
+		Batch &b = batch->b;
+		cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+		if (ret != PST_RET_IDS && ret != PST_RET_POINTS)
+			fail(PST_ERR_INVALID, "bad return type");
+		if (ret == PST_RET_IDS && b.tree->idtype != PST_ID_U32)
+			fail(PST_ERR_UNSUPPORTED, "an id-less tree can only return points");
+		b.stage_queries(queries, nq, queries_on_device != 0, s);
+		uint64_t tot = 0;
+		if (sync) {
+			b.count_sync(s, &tot);
+			if (offsets_d)
+				check_cuda(cudaMemcpyAsync(offsets_d, b.offsets, ((size_t) nq + 1) * 8, cudaMemcpyDeviceToDevice, s),
+				           "copy offsets");
+			if (total)
+				*total = tot;
+			if (tot > out_capacity) {
+				check_cuda(cudaStreamSynchronize(s), "sync");
+				result = PST_ERR_CAPACITY;
+				return;
+			}
+			if (tot)
+				b.enqueue_emit(ret, out_d, out_capacity, s);
+			result = b.read_ctl(s, nullptr);
+		} else {
+			b.launch_count(s);
+			b.enqueue_emit(ret, out_d, out_capacity, s);
+			if (offsets_d)
+				check_cuda(cudaMemcpyAsync(offsets_d, b.offsets, ((size_t) nq + 1) * 8, cudaMemcpyDeviceToDevice, s),
+				           "copy offsets");
+			if (total)
+				check_cuda(cudaMemcpyAsync(total, &b.ctl->total, 8, cudaMemcpyDeviceToHost, s), "copy total");
+		}
+	});
+	if (st != PST_OK)
+		return st;
+	if (result != PST_OK)
+		g_last_error = result == PST_ERR_CAPACITY ? "batch result exceeds out_capacity" : "batch pass failed";
+	return result;
+}
+
+pst_status pst_batch_count(pst_batch *batch, const pst_query *queries, uint32_t nq, int queries_on_device,
+                           uint64_t *counts_d, uint64_t *total, pst_stream_t stream)
+{
+	return guarded([&] {
+		if (!batch)
+			fail(PST_ERR_INVALID, "null batch");
+		Batch &b = batch->b;
+		cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+		b.stage_queries(queries, nq, queries_on_device != 0, s);
+		uint64_t tot = 0;
+		b.count_sync(s, &tot);
+		if (counts_d && nq)
+			check_cuda(cudaMemcpyAsync(counts_d, b.counts, (size_t) nq * 8, cudaMemcpyDeviceToDevice, s), "copy counts");
+		check_cuda(cudaStreamSynchronize(s), "sync");
+		if (total)
+			*total = tot;
+	});
+}
+
+pst_status pst_batch_status(pst_batch *batch, uint64_t *total)
+{
+	pst_status result = PST_OK;
+	pst_status st = guarded([&] {
+		if (!batch)
+			fail(PST_ERR_INVALID, "null batch");
+		result = batch->b.read_ctl(nullptr, total);
+	});
+	return st != PST_OK ? st : result;
+}
+
+static uint64_t ips_common(pst_dtype dtype, pst_idtype idtype, const void *pts_d, uint64_t n, pst_value v, pst_ret ret,
+                           void *out, uint64_t cap, uint32_t blocks, cudaStream_t s)
+{
+	unsigned long long *ctr = nullptr;
+	check_cuda(cudaMallocAsync((void **) &ctr, 8, s), "cudaMallocAsync");
+	struct F {
+		unsigned long long *p;
+		cudaStream_t s;
+		~F() { cudaFreeAsync(p, s); }
+	} f{ctr, s};
+	check_cuda(cudaMemsetAsync(ctr, 0, 8, s), "memset");
+	ips_run(dtype, idtype, ret, pts_d, n, v, out, cap, ctr, blocks, s);
+	unsigned long long c = 0;
+	check_cuda(cudaMemcpyAsync(&c, ctr, 8, cudaMemcpyDeviceToHost, s), "copy count");
+	check_cuda(cudaStreamSynchronize(s), "sync");
+	return c;
+}
+
+pst_status pst_ips_search(pst_dtype dtype, pst_idtype idtype, const void *pts_d, uint64_t n, pst_value v, pst_ret ret,
+                          void **out_d, uint64_t *count, uint32_t num_blocks, uint32_t threads_per_block,
+                          pst_stream_t stream)
+{
+	(void) threads_per_block;
+	return guarded([&] {
+		if (!out_d || !count)
+			fail(PST_ERR_INVALID, "null output");
+		check_types(dtype, idtype);
+		*out_d = nullptr;
+		*count = 0;
+		if (n == 0)
+			return;
+		if (!pts_d)
+			fail(PST_ERR_INVALID, "null point array");
+		require_device();
+		const uint64_t rs = ret == PST_RET_IDS ? 4 : point_size(dtype, idtype);
+		// The reference allocates room for every point (interval-parallel-search.h:35).
+		malloc_result(out_d, n * rs);
+		try {
+			*count = ips_common(dtype, idtype, pts_d, n, v, ret, *out_d, n, num_blocks,
+			                    reinterpret_cast<cudaStream_t>(stream));
+		} catch (...) {
+			cudaFree(*out_d);
+			*out_d = nullptr;
+			throw;
+		}
+	});
+}
+
+pst_status pst_ips_search_into(pst_dtype dtype, pst_idtype idtype, const void *pts_d, uint64_t n, pst_value v,
+                               pst_ret ret, void *out_d, uint64_t capacity, uint64_t *count, pst_stream_t stream)
+{
+	uint64_t c = 0;
+	pst_status st = guarded([&] {
+		if (!count)
+			fail(PST_ERR_INVALID, "null count");
+		check_types(dtype, idtype);
+		*count = 0;
+		if (n == 0)
+			return;
+		if (!pts_d)
+			fail(PST_ERR_INVALID, "null point array");
+		require_device();
+		c = ips_common(dtype, idtype, pts_d, n, v, ret, out_d, capacity, 0, reinterpret_cast<cudaStream_t>(stream));
+		*count = c;
+	});
+	if (st == PST_OK && c > capacity) {
+		g_last_error = "interval search result exceeds capacity";
+		return PST_ERR_CAPACITY;
+	}
+	return st;
+}
+
+pst_status pst_num_metacells(const uint32_t pt_dims[3], const uint32_t mc_dims[3], uint32_t mc_grid[3],
+                             uint64_t *n_metacells)
+{
+	return guarded([&] {
+		if (!pt_dims || !mc_dims)
+			fail(PST_ERR_INVALID, "null dims");
+		uint64_t n = 1;
+		for (int i = 0; i < 3; i++) {
+			if (mc_dims[i] == 0 || pt_dims[i] < 2)
+				fail(PST_ERR_INVALID, "each vertex dim must be >= 2 and each metacell dim >= 1");
+			const uint32_t m = (pt_dims[i] - 1) / mc_dims[i] + ((pt_dims[i] - 1) % mc_dims[i] ? 1 : 0);
+			if (mc_grid)
+				mc_grid[i] = m;
+			n *= m;
+		}
+		if (n_metacells)
+			*n_metacells = n;
+	});
+}
+
+pst_status pst_form_metacells(pst_dtype dtype, pst_idtype idtype, const void *vert_d, const uint32_t pt_dims[3],
+                              const uint32_t mc_dims[3], void *out_d, pst_stream_t stream)
+{
+	return guarded([&] {
+		check_types(dtype, idtype);
+		uint32_t M[3];
+		uint64_t nm = 0;
+		if (pst_num_metacells(pt_dims, mc_dims, M, &nm) != PST_OK)
+			fail(PST_ERR_INVALID, g_last_error);
+		if (nm >= (1ull << 32) && idtype == PST_ID_U32)
+			fail(PST_ERR_INVALID, "metacell ids must fit in 32 bits");
+		if (!vert_d || !out_d)
+			fail(PST_ERR_INVALID, "null buffer");
+		require_device();
+		metacells_run(dtype, idtype, vert_d, pt_dims, mc_dims, M, out_d, reinterpret_cast<cudaStream_t>(stream));
+	});
+}
+
+}  // extern "C"

@@ -1,0 +1,188 @@
+// Shared definitions of the B200 static priority search tree library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <string>
+
+#include "pst_c.h"
+
+namespace pst {
+
+// ---------------------------------------------------------------------------
+// Errors.  Library code throws pst::Error internally; the C ABI layer turns it
+// into a pst_status plus a thread-local message.
+
+struct Error {
+	pst_status status;
+	std::string msg;
+};
+
+[[noreturn]] void fail(pst_status st, const std::string &msg);
+void check_cuda(cudaError_t e, const char *what);
+
+#define PST_CUDA(call) ::pst::check_cuda((call), #call)
+
+// ---------------------------------------------------------------------------
+// Point records: the reference's PointStruct layouts (helpers/point-struct.h).
+
+template <typename T, bool HAS_ID>
+struct Point;
+template <typename T>
+struct Point<T, true> {
+	T dim1;
+	T dim2;
+	uint32_t id;
+};
+template <typename T>
+struct Point<T, false> {
+	T dim1;
+	T dim2;
+};
+
+// ---------------------------------------------------------------------------
+// Order-preserving unsigned keys.  Comparing keys as unsigned integers gives the
+// order of the values under the C++ `<` of the reference's comparators
+// (helpers/point-struct.h:62-81); -0.0 is mapped onto +0.0 because `!=` treats
+// them as equal there, so ties between them fall to the id/index tiebreak.
+// NaN inputs are outside the contract (the reference's comparators are not a
+// strict weak order on them).
+
+template <typename T>
+struct KeyOf;
+
+template <>
+struct KeyOf<float> {
+	using K = uint32_t;
+	__host__ __device__ static K key(float v)
+	{
+		uint32_t u;
+		memcpy(&u, &v, 4);
+		if (v == 0.0f)
+			u = 0;
+		return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+	}
+};
+
+template <>
+struct KeyOf<double> {
+	using K = uint64_t;
+	__host__ __device__ static K key(double v)
+	{
+		uint64_t u;
+		memcpy(&u, &v, 8);
+		if (v == 0.0)
+			u = 0;
+		return (u & 0x8000000000000000ull) ? ~u : (u | 0x8000000000000000ull);
+	}
+};
+
+template <>
+struct KeyOf<int32_t> {
+	using K = uint32_t;
+	__host__ __device__ static K key(int32_t v) { return static_cast<uint32_t>(v) ^ 0x80000000u; }
+};
+
+// ---------------------------------------------------------------------------
+// Device tree.  Heap positions are 1-based (root = 1, children 2h and 2h+1), so
+// level d occupies [2^d, 2^(d+1)) and every 32-slot chunk at levels >= 5 starts
+// on a 128-byte boundary of a 4-byte field.  Arrays hold 2^levels entries
+// (position 0 unused); med holds 2^(levels-1) (internal levels only).
+// All levels but the last are full; occ has one bit per position.
+
+template <typename T>
+struct TreeDev {
+	const T *dim1;
+	const T *dim2;
+	const T *med;
+	const uint32_t *id;   // null for id-less trees
+	const uint32_t *occ;  // occupancy bitmap, 2^levels bits
+	uint64_t n;
+	uint32_t levels;      // D = floor(log2 n) + 1
+};
+
+// Number of levels of a tree of n points: floor(log2 n) + 1 (0 for n == 0).
+inline uint32_t tree_levels(uint64_t n)
+{
+	uint32_t d = 0;
+	while ((n >> d) != 0)
+		d++;
+	return d;
+}
+
+// Point count of the node at level d, index j within the level.  Construction
+// gives a node of c points a left child of floor(c/2) and a right child of
+// c - 1 - floor(c/2) points (pst/static-pst-cpu-iter.tpp:512-541), so counts
+// depend on n and the node's path only.
+__host__ __device__ inline uint64_t node_count(uint64_t n, uint32_t d, uint64_t j)
+{
+	uint64_t c = n;
+	for (int b = (int) d - 1; b >= 0 && c != 0; b--)
+		c = ((j >> b) & 1) ? c - 1 - c / 2 : c / 2;
+	return c;
+}
+
+// ---------------------------------------------------------------------------
+// Warp helpers.
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ uint32_t lanemask_lt() { return (1u << lane_id()) - 1u; }
+
+// Spreads the 16 low bits of x so that bit j lands on bits 2j and 2j+1: the
+// children of the 16 parents of a half chunk fill one whole chunk.
+__host__ __device__ __forceinline__ uint32_t spread16(uint32_t x)
+{
+	x &= 0xFFFFu;
+	x = (x | (x << 8)) & 0x00FF00FFu;
+	x = (x | (x << 4)) & 0x0F0F0F0Fu;
+	x = (x | (x << 2)) & 0x33333333u;
+	x = (x | (x << 1)) & 0x55555555u;
+	return x | (x << 1);
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T v)
+{
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		T t = __shfl_up_sync(0xFFFFFFFFu, v, o);
+		if ((int) lane_id() >= o)
+			v += t;
+	}
+	return v;
+}
+
+// Segmented inclusive sum over lanes whose `key` equals the previous lane's key
+// (runs of equal keys).  Returns the run-inclusive sum; *last is true on the last
+// lane of each run.
+__device__ __forceinline__ uint64_t warp_run_sum(uint32_t key, uint64_t v, bool *last)
+{
+	const uint32_t lane = lane_id();
+	uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, key, 1);
+	uint32_t head = (lane == 0 || prev != key) ? 1u : 0u;
+	uint32_t heads = __ballot_sync(0xFFFFFFFFu, head);
+	// start lane of my run = highest head lane <= lane
+	uint32_t mask_le = heads & (0xFFFFFFFFu >> (31 - lane));
+	uint32_t start = 31 - __clz(mask_le);
+#pragma unroll
+	for (int o = 1; o < 32; o <<= 1) {
+		uint64_t t = __shfl_up_sync(0xFFFFFFFFu, v, o);
+		if (lane >= start + o)
+			v += t;
+	}
+	uint32_t next = __shfl_down_sync(0xFFFFFFFFu, key, 1);
+	*last = (lane == 31) || (next != key);
+	return v;
+}
+
+// Per-stream device facts used for grid sizing.
+struct DeviceInfo {
+	int device;
+	int sms;
+	size_t smem_optin;
+};
+const DeviceInfo &device_info();
+
+}  // namespace pst

@@ -1,0 +1,588 @@
+// Searches of the static priority search tree: one query or a batch of mixed
+// 3-sided / 2-sided-left / 2-sided-right queries, in one level-synchronous pass.
+//
+// The reference walks the tree with one thread block per query, handing subtrees
+// to idle threads through shared memory and to child grids when none are idle
+// (pst/static-pst-gpu-search-functions.tu:12-722, pst/static-pst-gpu.tu:819-1148).
+// Here every query of a batch advances one tree level per kernel:
+//   - "path" tasks follow the O(log n) boundary nodes of a query with the
+//     reference's delegation rules (do3SidedSearchDelegation, doLeftSearchDelegation,
+//     doRightSearchDelegation: pst/static-pst-cpu-iter.tpp:602-714);
+//   - every subtree the reference would "report above" becomes chunk tasks.  In a
+//     max-heap on dim2 a node is reported exactly when its own dim2 passes
+//     (its ancestors' dim2 are at least as large), so a chunk task is just the
+//     32 consecutive slots of one level, tested by one warp with one coalesced
+//     load; the survivors' 32 children fill two chunks of the next level.
+// Chunk tasks record their survivor masks.  A count of every query falls out of
+// the pass; an exclusive scan gives each query's exact output offset and a flat
+// emit kernel writes ids (or points) from the recorded masks.
+#include <algorithm>
+#include <type_traits>
+#include <vector>
+
+#include "scan_sort.cuh"
+#include "search.cuh"
+
+namespace pst {
+
+namespace {
+
+constexpr uint32_t TASK_RECORD = 1u;  // task holds an already-tested result (no expansion)
+constexpr uint32_t MODE_THREE = 3, MODE_LEFT = 1, MODE_RIGHT = 2;
+
+__device__ __forceinline__ bool occ_bit(const uint32_t *occ, uint32_t h) { return (occ[h >> 5] >> (h & 31)) & 1u; }
+
+template <typename T>
+struct QDev {
+	const uint32_t *kind;
+	const T *min1;
+	const T *max1;
+	const T *min2;
+};
+
+struct WorkDev {
+	uint4 *tasks;
+	uint32_t *amask;
+	uint64_t task_cap;
+	uint4 *path0;
+	uint4 *path1;
+	uint32_t path_cap;
+	uint64_t *counts;
+	uint64_t *cursor;
+	const uint64_t *offsets;
+	BatchCtl *ctl;
+};
+
+// Appends k consecutive task slots to the region of level `lvl`; returns the first
+// slot index or ~0 when the buffer is full (the overflow is recorded).
+__device__ __forceinline__ uint64_t reserve_tasks(const WorkDev &w, uint64_t region_base, uint32_t lvl, uint32_t k)
+{
+	const uint32_t off = atomicAdd(&w.ctl->lvl_cnt[lvl], k);
+	const uint64_t slot = region_base + off;
+	if (slot + k > w.task_cap) {
+		atomicMax((unsigned long long *) &w.ctl->need_tasks, (unsigned long long) (slot + k));
+		atomicOr(&w.ctl->flags, BATCH_FLAG_TASK_OVERFLOW);
+		return ~0ull;
+	}
+	return slot;
+}
+
+template <typename T>
+__device__ void path_step(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev &w, uint32_t d, uint64_t base_next,
+                          uint4 task)
+{
+	const uint32_t h = task.x, q = task.y, mode = task.z;
+	const T min2 = qd.min2[q];
+	const T v2 = t.dim2[h];
+	if (!(min2 <= v2))
+		return;
+	const uint32_t kind = qd.kind[q];
+	const T min1 = qd.min1[q], max1 = qd.max1[q];
+	const T v1 = t.dim1[h];
+	const bool rep = kind == PST_Q_THREE ? (min1 <= v1 && v1 <= max1) : kind == PST_Q_LEFT ? (v1 <= max1) : (v1 >= min1);
+	if (rep) {
+		const uint64_t slot = reserve_tasks(w, base_next, d + 1, 1);
+		if (slot != ~0ull) {
+			w.tasks[slot] = make_uint4(h & ~31u, q, 1u << (h & 31), TASK_RECORD);
+			w.amask[slot] = 1u << (h & 31);
+		}
+		atomicAdd((unsigned long long *) &w.counts[q], 1ull);
+	}
+	if (d + 1 >= t.levels)
+		return;
+	const uint32_t l = 2 * h, r = 2 * h + 1;
+	const bool hl = occ_bit(t.occ, l), hr = occ_bit(t.occ, r);
+	if (!hl && !hr)
+		return;
+	const T m = t.med[h];
+	uint32_t pl = 0, pr = 0;  // continue as path task with this mode (0 = no)
+	bool rl = false, rr = false;  // report-above subtree
+	if (mode == MODE_THREE) {
+		if (min1 <= m && m <= max1) {
+			pl = hl ? MODE_RIGHT : 0;
+			pr = hr ? MODE_LEFT : 0;
+		} else if (max1 < m && hl) {
+			pl = MODE_THREE;
+		} else if (m < min1 && hr) {
+			pr = MODE_THREE;
+		}
+	} else if (mode == MODE_LEFT) {
+		if (m <= max1) {
+			rl = hl;
+			pr = hr ? MODE_LEFT : 0;
+		} else if (hl) {
+			pl = MODE_LEFT;
+		}
+	} else {
+		if (m >= min1) {
+			pl = hl ? MODE_RIGHT : 0;
+			rr = hr;
+		} else if (hr) {
+			pr = MODE_RIGHT;
+		}
+	}
+	uint4 *pout = ((d + 1) & 1) ? w.path1 : w.path0;
+	// at most two boundary paths per query and level, so path_cap = 2 * max_q holds them
+	if (pl) {
+		const uint32_t i = atomicAdd(&w.ctl->path_cnt[d + 1], 1u);
+		if (i < w.path_cap)
+			pout[i] = make_uint4(l, q, pl, 0);
+		else
+			atomicOr(&w.ctl->flags, BATCH_FLAG_INTERNAL);
+	}
+	if (pr) {
+		const uint32_t i = atomicAdd(&w.ctl->path_cnt[d + 1], 1u);
+		if (i < w.path_cap)
+			pout[i] = make_uint4(r, q, pr, 0);
+		else
+			atomicOr(&w.ctl->flags, BATCH_FLAG_INTERNAL);
+	}
+	if (rl || rr) {
+		// l and r share a chunk; both seeds fit one task
+		const uint32_t bits = (rl ? 1u << (l & 31) : 0u) | (rr ? 1u << (r & 31) : 0u);
+		const uint64_t slot = reserve_tasks(w, base_next, d + 1, 1);
+		if (slot != ~0ull)
+			w.tasks[slot] = make_uint4(l & ~31u, q, bits, 0u);
+	}
+}
+
+template <typename T>
+__global__ void __launch_bounds__(BFS_THREADS) k_bfs_level(TreeDev<T> t, QDev<T> qd, WorkDev w, uint32_t d)
+{
+	__shared__ uint64_t s_base[2];
+	if (threadIdx.x == 0) {
+		uint64_t b = 0;
+		for (uint32_t e = 0; e < d; e++)
+			b += w.ctl->lvl_cnt[e];
+		s_base[0] = b;
+		s_base[1] = b + w.ctl->lvl_cnt[d];
+	}
+	__syncthreads();
+	const uint64_t base_d = s_base[0], base_next = s_base[1];
+	// after a frontier overflow the counters run past what was stored: never read beyond it
+	const uint64_t n_d = base_next <= w.task_cap ? base_next - base_d : (base_d < w.task_cap ? w.task_cap - base_d : 0);
+	const uint64_t gthreads = (uint64_t) gridDim.x * blockDim.x;
+	const uint64_t gtid = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	const bool more = d + 1 < t.levels;
+
+	// boundary paths
+	const uint32_t np = min(w.ctl->path_cnt[d], w.path_cap);
+	const uint4 *pin = (d & 1) ? w.path1 : w.path0;
+	for (uint64_t i = gtid; i < np; i += gthreads)
+		path_step<T>(t, qd, w, d, base_next, pin[i]);
+	__syncwarp();
+
+	// report-above chunks, 32 tasks per warp iteration
+	const uint32_t lane = lane_id();
+	const uint64_t gwarps = gthreads / 32, gwarp = gtid / 32;
+	for (uint64_t wb = gwarp * 32; wb < n_d; wb += gwarps * 32) {
+		const uint64_t idx = base_d + wb + lane;
+		const bool valid = wb + lane < n_d;
+		uint4 tk = valid ? w.tasks[idx] : make_uint4(0, 0, 0, TASK_RECORD);
+		const bool rec = tk.w & TASK_RECORD;
+		uint32_t cand = (!rec) ? (tk.z & t.occ[tk.x >> 5]) : 0u;
+		const T m2 = cand ? qd.min2[tk.y] : T(0);
+		uint32_t my_am = 0;
+#pragma unroll
+		for (int g = 0; g < 32; g += 4) {
+			T v[4];
+			bool ld[4];
+			T mm[4];
+#pragma unroll
+			for (int u = 0; u < 4; u++) {
+				const uint32_t c = __shfl_sync(0xFFFFFFFFu, cand, g + u);
+				const uint32_t p = __shfl_sync(0xFFFFFFFFu, tk.x, g + u);
+				mm[u] = __shfl_sync(0xFFFFFFFFu, m2, g + u);
+				ld[u] = (c >> lane) & 1u;
+				v[u] = ld[u] ? t.dim2[p + lane] : T(0);
+			}
+#pragma unroll
+			for (int u = 0; u < 4; u++) {
+				const uint32_t am = __ballot_sync(0xFFFFFFFFu, ld[u] && (mm[u] <= v[u]));
+				if (lane == (uint32_t) (g + u))
+					my_am = am;
+			}
+		}
+		if (valid && !rec)
+			w.amask[idx] = my_am;
+		// per-query counts: one atomic per run of equal query ids
+		bool last;
+		const uint64_t run = warp_run_sum(tk.y, (uint64_t) __popc(my_am), &last);
+		if (last && run)
+			atomicAdd((unsigned long long *) &w.counts[tk.y], (unsigned long long) run);
+		if (more) {
+			const uint32_t lo = spread16(my_am), hi = spread16(my_am >> 16);
+			const uint32_t nc = (lo ? 1u : 0u) + (hi ? 1u : 0u);
+			const uint32_t inc = warp_incl_scan(nc);
+			const uint32_t tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
+			uint64_t slot0 = 0;
+			if (lane == 31 && tot)
+				slot0 = reserve_tasks(w, base_next, d + 1, tot);
+			slot0 = __shfl_sync(0xFFFFFFFFu, slot0, 31);
+			if (tot && slot0 != ~0ull) {
+				uint64_t s = slot0 + inc - nc;
+				const uint32_t p2 = 2 * tk.x;
+				if (lo)
+					w.tasks[s++] = make_uint4(p2, tk.y, lo, 0u);
+				if (hi)
+					w.tasks[s] = make_uint4(p2 + 32, tk.y, hi, 0u);
+			}
+		}
+	}
+}
+
+template <typename T>
+__global__ void k_unpack_queries(const pst_query *raw, BatchCtl *ctl, uint32_t *kind, T *min1, T *max1, T *min2,
+                                 uint4 *path0)
+{
+	const uint32_t nq = ctl->nq;
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
+		const pst_query q = raw[i];
+		T a, b, c;
+		if constexpr (sizeof(T) == 8) {
+			a = q.min1.f64; b = q.max1.f64; c = q.min2.f64;
+		} else if constexpr (std::is_same<T, float>::value) {
+			a = q.min1.f32; b = q.max1.f32; c = q.min2.f32;
+		} else {
+			a = q.min1.i32; b = q.max1.i32; c = q.min2.i32;
+		}
+		const uint32_t k = (uint32_t) q.kind;
+		kind[i] = k;
+		min1[i] = a;
+		max1[i] = b;
+		min2[i] = c;
+		const uint32_t mode = k == PST_Q_THREE ? MODE_THREE : k == PST_Q_LEFT ? MODE_LEFT : MODE_RIGHT;
+		path0[i] = make_uint4(1u, i, mode, 0u);
+	}
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+		ctl->path_cnt[0] = nq;
+}
+
+__global__ void k_check_kinds(const pst_query *raw, BatchCtl *ctl)
+{
+	const uint32_t nq = ctl->nq;
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
+		const int32_t k = raw[i].kind;
+		if (k < PST_Q_THREE || k > PST_Q_RIGHT)
+			atomicOr(&ctl->flags, BATCH_FLAG_BAD_QUERY);
+	}
+}
+
+template <typename T, bool HAS_ID, bool POINTS>
+__global__ void __launch_bounds__(BFS_THREADS) k_emit(TreeDev<T> t, WorkDev w, void *out, uint64_t capacity)
+{
+	using Pt = Point<T, HAS_ID>;
+	__shared__ uint64_t s_total;
+	if (threadIdx.x == 0) {
+		uint64_t b = 0;
+		for (uint32_t e = 0; e <= t.levels; e++)
+			b += w.ctl->lvl_cnt[e];
+		s_total = b;
+	}
+	__syncthreads();
+	if (w.ctl->total > capacity || (w.ctl->flags & BATCH_FLAG_TASK_OVERFLOW)) {
+		if (blockIdx.x == 0 && threadIdx.x == 0 && w.ctl->total > capacity)
+			atomicOr(&w.ctl->flags, BATCH_FLAG_OUT_OVERFLOW);
+		return;
+	}
+	const uint64_t total = s_total < w.task_cap ? s_total : w.task_cap;
+	const uint32_t lane = lane_id();
+	const uint64_t gtid = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	const uint64_t gwarps = (uint64_t) gridDim.x * blockDim.x / 32, gwarp = gtid / 32;
+	for (uint64_t wb = gwarp * 32; wb < total; wb += gwarps * 32) {
+		const uint64_t idx = wb + lane;
+		const bool valid = idx < total;
+		const uint32_t am = valid ? w.amask[idx] : 0u;
+		const uint4 tk = valid ? w.tasks[idx] : make_uint4(0, 0, 0, 0);
+		const uint32_t pc = __popc(am);
+		bool last;
+		const uint64_t run = warp_run_sum(tk.y, pc, &last);
+		// first slot of this lane's results inside its query's output
+		const uint32_t lastmask = __ballot_sync(0xFFFFFFFFu, last);
+		const uint32_t run_last = (uint32_t) (__ffs(lastmask & (0xFFFFFFFFu << lane)) - 1);
+		uint64_t rb = 0;
+		if (last && run)
+			rb = atomicAdd((unsigned long long *) &w.cursor[tk.y], (unsigned long long) run);
+		rb = __shfl_sync(0xFFFFFFFFu, rb, run_last);
+		const uint64_t my_base = am ? w.offsets[tk.y] + rb + run - pc : 0;
+		for (uint32_t tt = 0; tt < 32; tt++) {
+			const uint32_t a = __shfl_sync(0xFFFFFFFFu, am, tt);
+			if (!a)
+				continue;
+			const uint32_t p = __shfl_sync(0xFFFFFFFFu, tk.x, tt);
+			const uint64_t ob = __shfl_sync(0xFFFFFFFFu, my_base, tt);
+			if ((a >> lane) & 1u) {
+				const uint32_t h = p + lane;
+				const uint64_t o = ob + __popc(a & lanemask_lt());
+				if (o >= capacity)
+					continue;
+				if constexpr (POINTS) {
+					Pt rec;
+					rec.dim1 = t.dim1[h];
+					rec.dim2 = t.dim2[h];
+					if constexpr (HAS_ID)
+						rec.id = t.id[h];
+					static_cast<Pt *>(out)[o] = rec;
+				} else {
+					static_cast<uint32_t *>(out)[o] = t.id[h];
+				}
+			}
+		}
+	}
+}
+
+template <typename T>
+const void *bfs_kernel_ptr()
+{
+	return reinterpret_cast<const void *>(&k_bfs_level<T>);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host side.
+
+Batch::~Batch() { release(); }
+
+void Batch::release()
+{
+	if (graph_exec)
+		cudaGraphExecDestroy(graph_exec);
+	graph_exec = nullptr;
+	for (void *p : {(void *) q_raw, (void *) kind, min1, max1, min2, (void *) path0, (void *) path1, (void *) counts,
+	                (void *) cursor, (void *) offsets, (void *) scan_tmp, (void *) ctl, (void *) tasks, (void *) amask})
+		if (p)
+			cudaFree(p);
+	if (ctl_host)
+		cudaFreeHost(ctl_host);
+	if (q_stage)
+		cudaFreeHost(q_stage);
+	q_raw = nullptr;
+	ctl_host = nullptr;
+	q_stage = nullptr;
+}
+
+static void dmalloc(void **p, size_t bytes)
+{
+	cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+	if (e == cudaErrorMemoryAllocation) {
+		cudaGetLastError();
+		fail(PST_ERR_NOMEM, "batch workspace allocation of " + std::to_string(bytes) + " B failed");
+	}
+	check_cuda(e, "cudaMalloc(batch)");
+}
+
+void Batch::init(TreeStorage *t, const pst_batch_opts &o)
+{
+	tree = t;
+	max_q = std::max<uint32_t>(o.max_queries, 1);
+	use_graph = o.use_graph != 0;
+	threads = o.block_threads ? o.block_threads : BFS_THREADS;
+	if (threads != BFS_THREADS)
+		fail(PST_ERR_INVALID, "block_threads must be 0 or " + std::to_string(BFS_THREADS));
+	int occ = 0;
+	const void *kfn = nullptr;
+	switch (t->dtype) {
+	case PST_F32: kfn = bfs_kernel_ptr<float>(); break;
+	case PST_F64: kfn = bfs_kernel_ptr<double>(); break;
+	case PST_I32: kfn = bfs_kernel_ptr<int32_t>(); break;
+	}
+	PST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, threads, 0));
+	blocks_per_sm = o.blocks_per_sm ? std::min<uint32_t>(o.blocks_per_sm, (uint32_t) std::max(occ, 1))
+	                                : (uint32_t) std::max(occ, 1);
+	grid = (uint32_t) device_info().sms * blocks_per_sm;
+	const size_t vs = value_size(t->dtype);
+	dmalloc((void **) &q_raw, (size_t) max_q * sizeof(pst_query));
+	dmalloc((void **) &kind, (size_t) max_q * 4);
+	dmalloc(&min1, (size_t) max_q * vs);
+	dmalloc(&max1, (size_t) max_q * vs);
+	dmalloc(&min2, (size_t) max_q * vs);
+	dmalloc((void **) &path0, (size_t) max_q * 2 * sizeof(uint4));
+	dmalloc((void **) &path1, (size_t) max_q * 2 * sizeof(uint4));
+	dmalloc((void **) &counts, (size_t) max_q * 8);
+	dmalloc((void **) &cursor, (size_t) max_q * 8);
+	dmalloc((void **) &offsets, ((size_t) max_q + 1) * 8);
+	dmalloc((void **) &scan_tmp, scan_tmp_elems(max_q) * 8);
+	dmalloc((void **) &ctl, sizeof(BatchCtl));
+	PST_CUDA(cudaMallocHost((void **) &ctl_host, sizeof(BatchCtl)));
+	PST_CUDA(cudaMallocHost((void **) &q_stage, (size_t) max_q * sizeof(pst_query)));
+	memset(ctl_host, 0, sizeof(BatchCtl));
+	const uint64_t want = o.task_capacity ? o.task_capacity : std::max<uint64_t>(1ull << 16, (uint64_t) max_q * 64);
+	grow_tasks(want);
+}
+
+void Batch::grow_tasks(uint64_t cap)
+{
+	if (tasks)
+		cudaFree(tasks);
+	if (amask)
+		cudaFree(amask);
+	tasks = nullptr;
+	amask = nullptr;
+	dmalloc((void **) &tasks, cap * sizeof(uint4));
+	dmalloc((void **) &amask, cap * 4);
+	task_cap = cap;
+	if (graph_exec) {
+		cudaGraphExecDestroy(graph_exec);
+		graph_exec = nullptr;
+	}
+}
+
+template <typename T>
+void Batch::enqueue_count(cudaStream_t s)
+{
+	TreeDev<T> tv = tree->view<T>();
+	QDev<T> qd{kind, static_cast<const T *>(min1), static_cast<const T *>(max1), static_cast<const T *>(min2)};
+	WorkDev w{tasks, amask, task_cap, path0, path1, 2 * max_q, counts, cursor, offsets, ctl};
+	PST_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
+	PST_CUDA(cudaMemsetAsync(counts, 0, (size_t) max_q * 8, s));
+	PST_CUDA(cudaMemsetAsync(cursor, 0, (size_t) max_q * 8, s));
+	const unsigned ug = (unsigned) std::min<uint64_t>((max_q + 255) / 256, (uint64_t) device_info().sms * 4);
+	k_check_kinds<<<ug, 256, 0, s>>>(q_raw, ctl);
+	k_unpack_queries<T><<<ug, 256, 0, s>>>(q_raw, ctl, kind, static_cast<T *>(min1), static_cast<T *>(max1),
+	                                       static_cast<T *>(min2), path0);
+	for (uint32_t d = 0; d < tv.levels; d++)
+		k_bfs_level<T><<<grid, threads, 0, s>>>(tv, qd, w, d);
+	exclusive_scan<uint64_t>(counts, offsets, max_q, scan_tmp, &ctl->total, s);
+	PST_CUDA(cudaMemcpyAsync(offsets + max_q, &ctl->total, 8, cudaMemcpyDeviceToDevice, s));
+	PST_CUDA(cudaGetLastError());
+}
+
+template <typename T, bool HAS_ID, bool POINTS>
+void Batch::enqueue_emit_t(void *out, uint64_t capacity, cudaStream_t s)
+{
+	TreeDev<T> tv = tree->view<T>();
+	WorkDev w{tasks, amask, task_cap, path0, path1, 2 * max_q, counts, cursor, offsets, ctl};
+	k_emit<T, HAS_ID, POINTS><<<grid, threads, 0, s>>>(tv, w, out, capacity);
+	PST_CUDA(cudaGetLastError());
+}
+
+template <typename T>
+void Batch::enqueue_emit_v(pst_ret ret, void *out, uint64_t capacity, cudaStream_t s)
+{
+	const bool has_id = tree->idtype == PST_ID_U32;
+	if (ret == PST_RET_IDS) {
+		if (!has_id)
+			fail(PST_ERR_UNSUPPORTED, "an id-less tree can only return points");
+		enqueue_emit_t<T, true, false>(out, capacity, s);
+	} else if (has_id) {
+		enqueue_emit_t<T, true, true>(out, capacity, s);
+	} else {
+		enqueue_emit_t<T, false, true>(out, capacity, s);
+	}
+}
+
+void Batch::enqueue_counting(cudaStream_t s)
+{
+	switch (tree->dtype) {
+	case PST_F32: enqueue_count<float>(s); break;
+	case PST_F64: enqueue_count<double>(s); break;
+	case PST_I32: enqueue_count<int32_t>(s); break;
+	}
+}
+
+void Batch::enqueue_emit(pst_ret ret, void *out, uint64_t capacity, cudaStream_t s)
+{
+	switch (tree->dtype) {
+	case PST_F32: enqueue_emit_v<float>(ret, out, capacity, s); break;
+	case PST_F64: enqueue_emit_v<double>(ret, out, capacity, s); break;
+	case PST_I32: enqueue_emit_v<int32_t>(ret, out, capacity, s); break;
+	}
+}
+
+void Batch::launch_count(cudaStream_t s)
+{
+	if (!use_graph) {
+		enqueue_counting(s);
+		return;
+	}
+	if (!graph_exec || graph_stream_key != s) {
+		if (graph_exec)
+			cudaGraphExecDestroy(graph_exec);
+		graph_exec = nullptr;
+		cudaStream_t cs;
+		PST_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+		cudaGraph_t g;
+		PST_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+		try {
+			enqueue_counting(cs);
+		} catch (...) {
+			cudaStreamEndCapture(cs, &g);
+			cudaStreamDestroy(cs);
+			throw;
+		}
+		PST_CUDA(cudaStreamEndCapture(cs, &g));
+		PST_CUDA(cudaGraphInstantiate(&graph_exec, g, 0));
+		cudaGraphDestroy(g);
+		cudaStreamDestroy(cs);
+		graph_stream_key = s;
+	}
+	PST_CUDA(cudaGraphLaunch(graph_exec, s));
+}
+
+void Batch::stage_queries(const pst_query *q, uint32_t nq, bool on_device, cudaStream_t s)
+{
+	if (nq > max_q)
+		fail(PST_ERR_INVALID, "batch of " + std::to_string(nq) + " queries exceeds max_queries " +
+		                          std::to_string(max_q));
+	if (nq && !q)
+		fail(PST_ERR_INVALID, "null query array");
+	// the pinned control block and query staging may still feed an earlier pass
+	PST_CUDA(cudaStreamSynchronize(s));
+	ctl_host->nq = nq;
+	if (nq) {
+		if (on_device) {
+			PST_CUDA(cudaMemcpyAsync(q_raw, q, (size_t) nq * sizeof(pst_query), cudaMemcpyDeviceToDevice, s));
+		} else {
+			memcpy(q_stage, q, (size_t) nq * sizeof(pst_query));
+			PST_CUDA(cudaMemcpyAsync(q_raw, q_stage, (size_t) nq * sizeof(pst_query), cudaMemcpyHostToDevice, s));
+		}
+	}
+}
+
+pst_status Batch::read_ctl(cudaStream_t s, uint64_t *total)
+{
+	BatchCtl h;
+	PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
+	PST_CUDA(cudaStreamSynchronize(s));
+	last = h;
+	if (total)
+		*total = h.total;
+	if (h.flags & BATCH_FLAG_BAD_QUERY)
+		return PST_ERR_INVALID;
+	if (h.flags & (BATCH_FLAG_TASK_OVERFLOW | BATCH_FLAG_INTERNAL))
+		return PST_ERR_INTERNAL;
+	if (h.flags & BATCH_FLAG_OUT_OVERFLOW)
+		return PST_ERR_CAPACITY;
+	return PST_OK;
+}
+
+// Count pass with automatic growth of the frontier buffer.
+void Batch::count_sync(cudaStream_t s, uint64_t *total)
+{
+	for (int attempt = 0;; attempt++) {
+		launch_count(s);
+		BatchCtl h;
+		PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
+		PST_CUDA(cudaStreamSynchronize(s));
+		last = h;
+		if (h.flags & BATCH_FLAG_BAD_QUERY)
+			fail(PST_ERR_INVALID, "query kind must be PST_Q_THREE, PST_Q_LEFT or PST_Q_RIGHT");
+		if (h.flags & BATCH_FLAG_INTERNAL)
+			fail(PST_ERR_INTERNAL, "search consistency check failed");
+		if (!(h.flags & BATCH_FLAG_TASK_OVERFLOW)) {
+			*total = h.total;
+			return;
+		}
+		if (attempt > 8)
+			fail(PST_ERR_INTERNAL, "frontier did not fit after growth");
+		grow_tasks(std::max<uint64_t>(h.need_tasks + h.need_tasks / 4, task_cap * 2));
+	}
+}
+
+uint64_t Batch::record_size(pst_ret ret) const
+{
+	return ret == PST_RET_IDS ? 4 : point_size(tree->dtype, tree->idtype);
+}
+
+}  // namespace pst

@@ -1,0 +1,73 @@
+// Batched / single-query search engine (host side).
+#pragma once
+
+#include "tree.cuh"
+
+namespace pst {
+
+constexpr int BFS_THREADS = 256;
+
+enum : uint32_t {
+	BATCH_FLAG_TASK_OVERFLOW = 1u,  // frontier buffer too small (results incomplete)
+	BATCH_FLAG_OUT_OVERFLOW = 2u,   // output buffer too small (nothing written)
+	BATCH_FLAG_BAD_QUERY = 4u,      // a query kind out of range
+	BATCH_FLAG_INTERNAL = 8u,       // a device-side consistency check failed
+};
+
+// Device control block of one pass; the host uploads a zeroed copy (with nq set)
+// at the start of every pass.
+struct BatchCtl {
+	uint32_t lvl_cnt[40];   // chunk tasks appended per level region
+	uint32_t path_cnt[40];  // boundary-path tasks per level
+	uint32_t nq;
+	uint32_t flags;
+	uint64_t need_tasks;
+	uint64_t total;
+};
+
+struct Batch {
+	TreeStorage *tree = nullptr;
+	uint32_t max_q = 0;
+	bool use_graph = true;
+	uint32_t threads = BFS_THREADS;
+	uint32_t blocks_per_sm = 0;
+	uint32_t grid = 0;
+	// queries
+	pst_query *q_raw = nullptr;
+	pst_query *q_stage = nullptr;  // pinned staging for host query arrays
+	uint32_t *kind = nullptr;
+	void *min1 = nullptr, *max1 = nullptr, *min2 = nullptr;
+	// frontier and results
+	uint4 *tasks = nullptr;
+	uint32_t *amask = nullptr;
+	uint64_t task_cap = 0;
+	uint4 *path0 = nullptr, *path1 = nullptr;
+	uint64_t *counts = nullptr, *cursor = nullptr, *offsets = nullptr, *scan_tmp = nullptr;
+	BatchCtl *ctl = nullptr;
+	BatchCtl *ctl_host = nullptr;  // pinned, zeroed except nq
+	BatchCtl last{};
+	cudaGraphExec_t graph_exec = nullptr;
+	cudaStream_t graph_stream_key = nullptr;
+
+	~Batch();
+	void init(TreeStorage *t, const pst_batch_opts &o);
+	void release();
+	void grow_tasks(uint64_t cap);
+	void stage_queries(const pst_query *q, uint32_t nq, bool on_device, cudaStream_t s);
+	void launch_count(cudaStream_t s);
+	void count_sync(cudaStream_t s, uint64_t *total);
+	void enqueue_counting(cudaStream_t s);
+	void enqueue_emit(pst_ret ret, void *out, uint64_t capacity, cudaStream_t s);
+	pst_status read_ctl(cudaStream_t s, uint64_t *total);
+	uint64_t record_size(pst_ret ret) const;
+
+  private:
+	template <typename T>
+	void enqueue_count(cudaStream_t s);
+	template <typename T>
+	void enqueue_emit_v(pst_ret ret, void *out, uint64_t capacity, cudaStream_t s);
+	template <typename T, bool HAS_ID, bool POINTS>
+	void enqueue_emit_t(void *out, uint64_t capacity, cudaStream_t s);
+};
+
+}  // namespace pst

@@ -1,0 +1,49 @@
+// Tree storage and the entry points of construction and search (host side).
+#pragma once
+
+#include <mutex>
+
+#include "common.cuh"
+
+namespace pst {
+
+struct Batch;
+
+// Owns the device arrays of one tree (see TreeDev for the layout).
+struct TreeStorage {
+	pst_dtype dtype = PST_F32;
+	pst_idtype idtype = PST_ID_NONE;
+	uint64_t n = 0;
+	uint32_t levels = 0;
+	void *mem = nullptr;  // single cudaMalloc holding every field
+	size_t bytes = 0;
+	void *dim1 = nullptr;
+	void *dim2 = nullptr;
+	void *med = nullptr;
+	uint32_t *id = nullptr;
+	uint32_t *occ = nullptr;
+	int device = 0;
+	std::mutex mu;        // serialises the single-query engine
+	Batch *single = nullptr;
+
+	template <typename T>
+	TreeDev<T> view() const
+	{
+		return TreeDev<T>{static_cast<const T *>(dim1), static_cast<const T *>(dim2), static_cast<const T *>(med),
+		                  id, occ, n, levels};
+	}
+};
+
+size_t value_size(pst_dtype dt);
+size_t point_size(pst_dtype dt, pst_idtype it);
+// Device bytes of the tree arrays alone.
+uint64_t tree_bytes(pst_dtype dt, pst_idtype it, uint64_t n);
+// Tree arrays plus the peak construction working set.
+uint64_t build_bytes_needed(pst_dtype dt, pst_idtype it, uint64_t n);
+
+void build_tree(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s);
+void free_tree(TreeStorage &t);
+// Host copy in the reference's field layout (slot = heap index - 1).
+void export_tree(const TreeStorage &t, void *dim1, void *dim2, void *med, uint32_t *ids, uint8_t *bitcodes);
+
+}  // namespace pst

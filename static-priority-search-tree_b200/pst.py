@@ -1,0 +1,377 @@
+"""ctypes binding of libpst_b200.so (include/pst_c.h) with the reference's API shape."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+library_path = _PKG / "libpst_b200.so"
+
+DTYPE = {"f32": 0, "f64": 1, "i32": 2}
+NP = {"f32": np.float32, "f64": np.float64, "i32": np.int32}
+IDTYPE = {False: 0, True: 1}
+RET = {"ids": 0, "points": 1}
+KIND = {"three": 0, "left": 1, "right": 2}
+STATUS = {0: "PST_OK", 1: "PST_ERR_INVALID", 2: "PST_ERR_CUDA", 3: "PST_ERR_NOMEM", 4: "PST_ERR_CAPACITY",
+          5: "PST_ERR_UNSUPPORTED", 6: "PST_ERR_INTERNAL", 7: "PST_ERR_BUSY", 8: "PST_ERR_TIMEOUT"}
+
+
+class PSTError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Value(C.Union):
+    _fields_ = [("f32", C.c_float), ("f64", C.c_double), ("i32", C.c_int32)]
+
+
+class Query(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32), ("min1", Value), ("max1", Value), ("min2", Value)]
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [("max_queries", C.c_uint32), ("task_capacity", C.c_uint64), ("block_threads", C.c_uint32),
+                ("blocks_per_sm", C.c_uint32), ("use_graph", C.c_int32)]
+
+
+QUERY_NP = np.dtype([("kind", "<i4"), ("reserved", "<i4"), ("min1", "<u8"), ("max1", "<u8"), ("min2", "<u8")])
+
+_lib = None
+
+
+def lib():
+    """Loads libpst_b200.so (raises PSTError if it is missing: no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not library_path.exists():
+        raise PSTError(2, f"{library_path.name} is not built; run __graft_entry__.build()")
+    L = C.CDLL(str(library_path))
+    vp, u64, u32, i32 = C.c_void_p, C.c_uint64, C.c_uint32, C.c_int32
+    P = C.POINTER
+    sigs = {
+        "pst_last_error": (C.c_char_p, []),
+        "pst_version": (C.c_char_p, []),
+        "pst_point_size": (C.c_size_t, [i32, i32]),
+        "pst_free": (i32, [vp]),
+        "pst_mem_needed": (i32, [i32, i32, u64, P(u64)]),
+        "pst_create": (i32, [P(vp), i32, i32, vp, u64, vp]),
+        "pst_destroy": (i32, [vp]),
+        "pst_info": (i32, [vp, P(u64), P(u32), P(u64), P(u64), P(i32), P(i32)]),
+        "pst_export": (i32, [vp, vp, vp, vp, vp, vp]),
+        "pst_search": (i32, [vp, P(Query), i32, P(vp), P(u64), vp]),
+        "pst_three_sided": (i32, [vp, Value, Value, Value, i32, P(vp), P(u64), vp]),
+        "pst_two_sided_left": (i32, [vp, Value, Value, i32, P(vp), P(u64), vp]),
+        "pst_two_sided_right": (i32, [vp, Value, Value, i32, P(vp), P(u64), vp]),
+        "pst_search_into": (i32, [vp, P(Query), i32, vp, u64, P(u64), vp]),
+        "pst_batch_create": (i32, [P(vp), vp, P(BatchOpts)]),
+        "pst_batch_destroy": (i32, [vp]),
+        "pst_batch_run": (i32, [vp, vp, u32, i32, i32, vp, u64, vp, P(u64), i32, vp]),
+        "pst_batch_count": (i32, [vp, vp, u32, i32, vp, P(u64), vp]),
+        "pst_batch_status": (i32, [vp, P(u64)]),
+        "pst_ips_search": (i32, [i32, i32, vp, u64, Value, i32, P(vp), P(u64), u32, u32, vp]),
+        "pst_ips_search_into": (i32, [i32, i32, vp, u64, Value, i32, vp, u64, P(u64), vp]),
+        "pst_num_metacells": (i32, [P(u32), P(u32), P(u32), P(u64)]),
+        "pst_form_metacells": (i32, [i32, i32, vp, P(u32), P(u32), vp, vp]),
+    }
+    for name, (res, args) in sigs.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(st: int):
+    if st != 0:
+        raise PSTError(st, lib().pst_last_error().decode())
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise PSTError(2, "no CUDA device available")
+    return torch
+
+
+def _stream(stream=None):
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def point_dtype(dt: str, has_id: bool) -> np.dtype:
+    """numpy layout of the reference's PointStruct (helpers/point-struct.h)."""
+    fields = [("dim1", NP[dt]), ("dim2", NP[dt])]
+    if has_id:
+        fields.append(("id", np.uint32))
+    return np.dtype(fields, align=True)
+
+
+def value(dt: str, v) -> Value:
+    x = Value()
+    setattr(x, dt, NP[dt](v).item())
+    return x
+
+
+def points_to_device(pts: np.ndarray):
+    """Copies a structured PointStruct array to a device byte tensor."""
+    torch = _torch()
+    raw = np.ascontiguousarray(pts).view(np.uint8).reshape(-1)
+    return torch.from_numpy(raw.copy()).to("cuda")
+
+
+class _DevView:
+    """__cuda_array_interface__ over a raw device pointer (no ownership)."""
+
+    def __init__(self, ptr: int, nbytes: int):
+        self.__cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False), "version": 3}
+
+
+def _take_device_result(ptr: int, count: int, rec: np.dtype | type) -> np.ndarray:
+    """Copies a library-allocated result to host memory and frees it."""
+    torch = _torch()
+    rec = np.dtype(rec)
+    try:
+        if count == 0 or not ptr:
+            return np.zeros(0, rec)
+        t = torch.as_tensor(_DevView(ptr, count * rec.itemsize), device="cuda")
+        host = t.cpu().numpy()
+        return host.view(rec).copy()
+    finally:
+        if ptr:
+            _check(lib().pst_free(C.c_void_p(ptr)))
+
+
+def make_queries(kinds, min1, max1, min2, dt: str) -> np.ndarray:
+    """pst_query records (kind, bounds in the tree's value type)."""
+    n = len(kinds)
+    q = np.zeros(n, QUERY_NP)
+    q["kind"] = np.asarray(kinds, np.int32)
+    for f, v in (("min1", min1), ("max1", max1), ("min2", min2)):
+        vals = np.asarray(v, NP[dt])
+        buf = np.zeros(n, np.uint64)
+        buf.view(np.uint8).reshape(n, 8)[:, :vals.itemsize] = vals.view(np.uint8).reshape(n, vals.itemsize)
+        q[f] = buf
+    return q
+
+
+class StaticPSTGPU:
+    """Mirror of the reference's StaticPSTGPU<T, PointStruct, IDType, num_IDs>
+    (pst/static-pst-gpu.h:72-132).  Built from device PointStruct records."""
+
+    def __init__(self, pts_d, num_elems: int, dt: str = "f32", has_id: bool = True, stream=None):
+        self.dt, self.has_id, self.n = dt, has_id, int(num_elems)
+        self._h = C.c_void_p()
+        ptr = C.c_void_p(pts_d.data_ptr() if hasattr(pts_d, "data_ptr") else (pts_d or 0))
+        _check(lib().pst_create(C.byref(self._h), DTYPE[dt], IDTYPE[has_id], ptr, self.n, _stream(stream)))
+        self.rec_point = point_dtype(dt, has_id)
+
+    @classmethod
+    def from_numpy(cls, pts: np.ndarray, dt: str):
+        has_id = "id" in pts.dtype.names
+        d = points_to_device(pts)
+        return cls(d, len(pts), dt, has_id)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _check(lib().pst_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        n, lv, sl, by = C.c_uint64(), C.c_uint32(), C.c_uint64(), C.c_uint64()
+        d, i = C.c_int32(), C.c_int32()
+        _check(lib().pst_info(self._h, C.byref(n), C.byref(lv), C.byref(sl), C.byref(by), C.byref(d), C.byref(i)))
+        return {"n": n.value, "levels": lv.value, "slots": sl.value, "device_bytes": by.value}
+
+    def export(self):
+        """Tree in the reference's field layout (for bit-exact comparison)."""
+        S = self.info()["slots"]
+        t = NP[self.dt]
+        out = {"dim1": np.zeros(S, t), "dim2": np.zeros(S, t), "med": np.zeros(S, t),
+               "ids": np.zeros(S, np.uint32) if self.has_id else None, "bitcodes": np.zeros(S, np.uint8)}
+        p = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        _check(lib().pst_export(self._h, p(out["dim1"]), p(out["dim2"]), p(out["med"]), p(out["ids"]),
+                                p(out["bitcodes"])))
+        return out
+
+    def _ret(self, ret):
+        r = ret if isinstance(ret, str) else ("ids" if ret is np.uint32 else "points")
+        return r, (np.uint32 if r == "ids" else self.rec_point)
+
+    def search(self, kind: str, min1=0, max1=0, min2=0, ret="ids", stream=None) -> np.ndarray:
+        """One query through the drop-in call (callee-allocated result)."""
+        r, rec = self._ret(ret)
+        q = Query(KIND[kind], 0, value(self.dt, min1), value(self.dt, max1), value(self.dt, min2))
+        out, cnt = C.c_void_p(), C.c_uint64()
+        _check(lib().pst_search(self._h, C.byref(q), RET[r], C.byref(out), C.byref(cnt), _stream(stream)))
+        return _take_device_result(out.value or 0, cnt.value, rec)
+
+    # reference names (pst/static-pst-gpu.h:103-128)
+    def threeSidedSearch(self, min_dim1_val, max_dim1_val, min_dim2_val, ret="points"):
+        r, rec = self._ret(ret)
+        out, cnt = C.c_void_p(), C.c_uint64()
+        _check(lib().pst_three_sided(self._h, value(self.dt, min_dim1_val), value(self.dt, max_dim1_val),
+                                     value(self.dt, min_dim2_val), RET[r], C.byref(out), C.byref(cnt), _stream()))
+        return _take_device_result(out.value or 0, cnt.value, rec)
+
+    def twoSidedLeftSearch(self, max_dim1_val, min_dim2_val, ret="points"):
+        r, rec = self._ret(ret)
+        out, cnt = C.c_void_p(), C.c_uint64()
+        _check(lib().pst_two_sided_left(self._h, value(self.dt, max_dim1_val), value(self.dt, min_dim2_val),
+                                        RET[r], C.byref(out), C.byref(cnt), _stream()))
+        return _take_device_result(out.value or 0, cnt.value, rec)
+
+    def twoSidedRightSearch(self, min_dim1_val, min_dim2_val, ret="points"):
+        r, rec = self._ret(ret)
+        out, cnt = C.c_void_p(), C.c_uint64()
+        _check(lib().pst_two_sided_right(self._h, value(self.dt, min_dim1_val), value(self.dt, min_dim2_val),
+                                         RET[r], C.byref(out), C.byref(cnt), _stream()))
+        return _take_device_result(out.value or 0, cnt.value, rec)
+
+    def search_into(self, kind: str, out_d, capacity: int, min1=0, max1=0, min2=0, ret="ids", stream=None) -> int:
+        r, _ = self._ret(ret)
+        q = Query(KIND[kind], 0, value(self.dt, min1), value(self.dt, max1), value(self.dt, min2))
+        cnt = C.c_uint64()
+        st = lib().pst_search_into(self._h, C.byref(q), RET[r], C.c_void_p(out_d.data_ptr()), capacity,
+                                   C.byref(cnt), _stream(stream))
+        if st == 4:
+            return -int(cnt.value)
+        _check(st)
+        return int(cnt.value)
+
+    @staticmethod
+    def calcGlobalMemNeeded(num_elems: int, dt: str = "f32", has_id: bool = True) -> int:
+        b = C.c_uint64()
+        _check(lib().pst_mem_needed(DTYPE[dt], IDTYPE[has_id], num_elems, C.byref(b)))
+        return b.value
+
+
+class StaticPSTGPUArr(StaticPSTGPU):
+    """Mirror of StaticPSTGPUArr (pst/static-pst-gpu-arr.h:45-103).  The reference
+    splits the input into per-block shallow trees and implements only
+    twoSidedLeftSearch; here the same surface runs on the one complete tree, so its
+    3-sided and 2-sided-right searches work too and every result equals the
+    reference's StaticPSTCPUIter."""
+
+    def __init__(self, pts_d, num_elems: int, threads_per_block: int = 128, dt: str = "f32", has_id: bool = True,
+                 stream=None):
+        super().__init__(pts_d, num_elems, dt, has_id, stream)
+        self.threads_per_block = threads_per_block
+
+
+class BatchEngine:
+    """Batched queries on one resident tree (pst_batch_*)."""
+
+    def __init__(self, tree: StaticPSTGPU, max_queries: int, task_capacity: int = 0, use_graph: bool = True,
+                 blocks_per_sm: int = 0):
+        self.tree = tree
+        self.max_queries = max_queries
+        o = BatchOpts(max_queries, task_capacity, 0, blocks_per_sm, int(use_graph))
+        self._h = C.c_void_p()
+        _check(lib().pst_batch_create(C.byref(self._h), tree.handle, C.byref(o)))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _check(lib().pst_batch_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def count(self, queries: np.ndarray, stream=None):
+        torch = _torch()
+        nq = len(queries)
+        counts = torch.zeros(max(nq, 1), dtype=torch.int64, device="cuda")
+        tot = C.c_uint64()
+        q = np.ascontiguousarray(queries)
+        _check(lib().pst_batch_count(self._h, q.ctypes.data_as(C.c_void_p), nq, 0, C.c_void_p(counts.data_ptr()),
+                                     C.byref(tot), _stream(stream)))
+        return counts[:nq], tot.value
+
+    def run(self, queries, out_d, offsets_d, ret="ids", queries_on_device=False, sync=True, stream=None):
+        """Returns (status, total).  queries: host numpy pst_query array or device tensor."""
+        nq = len(queries)
+        if queries_on_device:
+            qp = C.c_void_p(queries.data_ptr())
+        else:
+            queries = np.ascontiguousarray(queries)
+            qp = queries.ctypes.data_as(C.c_void_p)
+        rec = 4 if ret == "ids" else self.tree.rec_point.itemsize
+        cap = out_d.numel() * out_d.element_size() // rec
+        tot = C.c_uint64()
+        st = lib().pst_batch_run(self._h, qp, nq, int(queries_on_device), RET[ret], C.c_void_p(out_d.data_ptr()),
+                                 cap, C.c_void_p(offsets_d.data_ptr()), C.byref(tot), int(sync), _stream(stream))
+        if st not in (0, 4):
+            _check(st)
+        return st, tot.value
+
+    def search(self, queries: np.ndarray, ret="ids"):
+        """Convenience: returns (offsets, results) on the host."""
+        torch = _torch()
+        counts, total = self.count(queries)
+        rec = np.uint32 if ret == "ids" else self.tree.rec_point
+        rsz = np.dtype(rec).itemsize
+        out = torch.empty(max(total * rsz, 16), dtype=torch.uint8, device="cuda")
+        offs = torch.empty(len(queries) + 1, dtype=torch.int64, device="cuda")
+        st, tot = self.run(queries, out, offs, ret=ret)
+        _check(st)
+        torch.cuda.synchronize()
+        res = out[: tot * rsz].cpu().numpy().view(rec)
+        return offs.cpu().numpy().astype(np.uint64), res
+
+
+def intervalParallelSearch(pts_d, num_elems: int, search_val, dt: str = "f32", has_id: bool = True, ret="ids",
+                           num_thread_blocks: int = 0, threads_per_block: int = 0, stream=None) -> np.ndarray:
+    """Mirror of intervalParallelSearch (interval-parallel-search/interval-parallel-search.h:29)."""
+    out, cnt = C.c_void_p(), C.c_uint64()
+    _check(lib().pst_ips_search(DTYPE[dt], IDTYPE[has_id], C.c_void_p(pts_d.data_ptr()), num_elems,
+                                value(dt, search_val), RET[ret], C.byref(out), C.byref(cnt), num_thread_blocks,
+                                threads_per_block, _stream(stream)))
+    rec = np.uint32 if ret == "ids" else point_dtype(dt, has_id)
+    return _take_device_result(out.value or 0, cnt.value, rec)
+
+
+def calcNumMetacells(pt_grid_dims, metacell_dims):
+    """Mirror of calcNumMetacells (helpers/isosurface-data-processing.h:23-36)."""
+    P = (C.c_uint32 * 3)(*pt_grid_dims)
+    M = (C.c_uint32 * 3)(*metacell_dims)
+    G = (C.c_uint32 * 3)()
+    n = C.c_uint64()
+    _check(lib().pst_num_metacells(P, M, G, C.byref(n)))
+    return list(G), n.value
+
+
+def formMetacellTags(vert_d, pt_grid_dims, metacell_dims, dt: str = "f32", has_id: bool = True, stream=None):
+    """Mirror of formMetacellTags (helpers/isosurface-data-processing.h:69-137): returns a
+    device byte tensor of PointStruct records, one per metacell, indexed by metacell id."""
+    torch = _torch()
+    _, n = calcNumMetacells(pt_grid_dims, metacell_dims)
+    rec = point_dtype(dt, has_id)
+    out = torch.empty(max(n * rec.itemsize, 16), dtype=torch.uint8, device="cuda")
+    P = (C.c_uint32 * 3)(*pt_grid_dims)
+    M = (C.c_uint32 * 3)(*metacell_dims)
+    _check(lib().pst_form_metacells(DTYPE[dt], IDTYPE[has_id], C.c_void_p(vert_d.data_ptr()), P, M,
+                                    C.c_void_p(out.data_ptr()), _stream(stream)))
+    return out[: n * rec.itemsize], n
+
+
+def _env_flag(name: str) -> bool:
+    return os.environ.get(name, "") not in ("", "0")

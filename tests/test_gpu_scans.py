@@ -1,0 +1,54 @@
+"""GPU parity of the streaming kernels: interval parallel search and metacells."""
+import numpy as np
+import pytest
+
+from datagen import rand_points
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("dt", ["f32", "f64", "i32"])
+@pytest.mark.parametrize("ids", ["arange", "random", "none"])
+def test_ips(pst, oracle, dt, ids):
+    pts = rand_points(123457, dt, ids=ids, dup=(dt == "i32"), seed=7)
+    d = pst.points_to_device(pts)
+    for v in [pts["dim1"][5], pts["dim2"][77], 500, -1e9 if dt != "i32" else -10**9]:
+        idx = oracle.Orc.ips(pts, dt, v)
+        if ids != "none":
+            got = pst.intervalParallelSearch(d, len(pts), v, dt, True, ret="ids")
+            assert np.array_equal(np.sort(got), np.sort(pts["id"][idx]))
+        gotp = pst.intervalParallelSearch(d, len(pts), v, dt, ids != "none", ret="points")
+        assert np.array_equal(oracle.canon(gotp), oracle.canon(pts[idx]))
+
+
+def test_ips_equals_pst_left(pst, oracle):
+    """IPS(v) is the 2-sided-left query (v, v)."""
+    pts = rand_points(200000, "f32", ids="arange", seed=12)
+    d = pst.points_to_device(pts)
+    tr = pst.StaticPSTGPU(d, len(pts), "f32", True)
+    for v in [100.0, 333.25, 999.0]:
+        a = pst.intervalParallelSearch(d, len(pts), v, "f32", True)
+        b = tr.twoSidedLeftSearch(v, v, ret="ids")
+        assert np.array_equal(np.sort(a), np.sort(b))
+    tr.close()
+
+
+@pytest.mark.parametrize("dims,mc", [((17, 13, 9), (4, 4, 4)), ((33, 33, 33), (4, 4, 4)), ((20, 7, 11), (3, 2, 5)),
+                                     ((9, 10, 11), (1, 1, 1)), ((66, 40, 35), (4, 4, 4)), ((2, 2, 2), (4, 4, 4))])
+@pytest.mark.parametrize("dt", ["f32", "f64"])
+def test_metacells(pst, oracle, dims, mc, dt):
+    import torch
+    rng = np.random.default_rng(sum(dims))
+    px, py, pz = dims
+    vol = rng.standard_normal((pz, py, px)).astype(np.float32 if dt == "f32" else np.float64)
+    lo, hi, ids = oracle.Orc.metacells(vol, dt, dims, mc)
+    vd = torch.from_numpy(vol.reshape(-1).copy()).to("cuda")
+    out, n = pst.formMetacellTags(vd, dims, mc, dt, True)
+    rec = out.cpu().numpy().view(pst.point_dtype(dt, True))
+    assert n == len(lo)
+    assert rec["dim1"].tobytes() == lo.tobytes()
+    assert rec["dim2"].tobytes() == hi.tobytes()
+    assert np.array_equal(rec["id"], ids)
+    out2, _ = pst.formMetacellTags(vd, dims, mc, dt, False)
+    rec2 = out2.cpu().numpy().view(pst.point_dtype(dt, False))
+    assert rec2["dim1"].tobytes() == lo.tobytes() and rec2["dim2"].tobytes() == hi.tobytes()
