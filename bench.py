@@ -1,0 +1,453 @@
+"""Benchmark of the static priority search tree hot path on B200.
+
+Workload (one "step" = one batched launch): 4096 queries (50% 3-sided, 25% 2-sided
+left, 25% 2-sided right) with target selectivities log-uniform in [1e-7, 1e-2], on
+a resident tree of 2^28 float32 points with uint32 ids, dim1 ~ U[0, 2^24) and
+dim2 = dim1 + U[0, 2^16) (seeded synthetic data; the tree alone is ~9 GB, far
+larger than L2, so no flush is needed between steps).  Query bounds are fixed
+once by bisection on exact counts.
+
+Metric: points reported per second (value: inputs resident in HBM, results to a
+device buffer; e2e: the same call from host memory with the query upload and the
+result download inside the timed region).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG_DIR = ROOT / "static-priority-search-tree_b200"
+sys.path.insert(0, str(ROOT / "oracle"))
+
+METRIC = "reported pts/s & queries/s at 2^28 pts, batched vs per-query; serving p50/p99 ms"
+UNIT = "pts/s"
+N_POINTS = 1 << 28
+NQ = 4096
+SEL_LO, SEL_HI = 1e-7, 1e-2
+BYTES_PER_PT = 12  # dim2 tested (4) + id read (4) + id written (4), float32 tree returning ids
+
+
+def load_package():
+    if "pst_b200" in sys.modules:
+        return sys.modules["pst_b200"]
+    spec = importlib.util.spec_from_file_location("pst_b200", PKG_DIR / "__init__.py",
+                                                  submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["pst_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# data
+
+def gen_points_device(n, seed, torch):
+    """(n, 3) int32 tensor = PointStruct<float, uint32_t, 1> records."""
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    d1 = torch.rand(n, generator=g, device="cuda", dtype=torch.float32) * float(1 << 24)
+    d2 = d1 + torch.rand(n, generator=g, device="cuda", dtype=torch.float32) * float(1 << 16)
+    rec = torch.empty((n, 3), dtype=torch.int32, device="cuda")
+    rec[:, 0] = d1.view(torch.int32)
+    rec[:, 1] = d2.view(torch.int32)
+    rec[:, 2] = torch.arange(n, device="cuda", dtype=torch.int32)
+    del d1, d2
+    return rec
+
+
+def gen_points_host(n, seed):
+    rng = np.random.default_rng(seed)
+    d1 = (rng.random(n, dtype=np.float32) * np.float32(1 << 24)).astype(np.float32)
+    d2 = (d1 + rng.random(n, dtype=np.float32) * np.float32(1 << 16)).astype(np.float32)
+    import oracle
+    return oracle.make_points(d1, d2, np.arange(n, dtype=np.uint32), "f32")
+
+
+def query_plan(nq, seed):
+    rng = np.random.default_rng(seed)
+    kinds = np.empty(nq, np.int32)
+    kinds[: nq // 2] = 0
+    kinds[nq // 2: 3 * nq // 4] = 1
+    kinds[3 * nq // 4:] = 2
+    rng.shuffle(kinds)
+    sel = np.exp(rng.uniform(np.log(SEL_LO), np.log(SEL_HI), nq))
+    anchor = rng.uniform(0, 1 << 24, nq)
+    return kinds, sel, anchor
+
+
+def calibrate(count_fn, kinds, sel, anchor, n, iters=24, domain=float(1 << 24)):
+    """Bisection of each query's free bound so that its exact count is ~sel * n,
+    over brackets that keep every trial count within ~4x of the target (a trial
+    never asks for a large fraction of the tree).  dim1 ~ U[0, domain),
+    dim2 = dim1 + U[0, 2^16).
+      3-sided [a, a + W] with min2 = a: W free in [0, 4 s domain];
+      left (b, c): dim2 bound c free in [b - 2 s domain - 2^16, b + 2^16];
+      right (a, c): c free in [max(a, domain - 2 s domain - 2^16), domain + 2^16].
+    count_fn(kinds, min1, max1, min2) -> exact counts."""
+    nq = len(kinds)
+    target = sel * n
+    three, left, right = kinds == 0, kinds == 1, kinds == 2
+    w = 1 << 16
+    lo = np.where(three, 0.0, np.where(left, anchor - 2 * sel * domain - w,
+                                        np.maximum(anchor, domain - 2 * sel * domain - w)))
+    hi = np.where(three, 4 * sel * domain + 64, np.where(left, anchor + w, domain + w))
+    best = (lo + hi) / 2
+    best_err = np.full(nq, np.inf)
+
+    def bounds(x):
+        min1 = np.where(three | right, anchor, 0.0)
+        max1 = np.where(three, anchor + x, np.where(left, anchor, 0.0))
+        min2 = np.where(three, anchor, x)
+        return min1.astype(np.float32), max1.astype(np.float32), min2.astype(np.float32)
+
+    for _ in range(iters):
+        mid = (lo + hi) / 2
+        c = count_fn(kinds, *bounds(mid)).astype(np.float64)
+        err = np.abs(c - target) / np.maximum(target, 1)
+        upd = err < best_err
+        best[upd] = mid[upd]
+        best_err[upd] = err[upd]
+        grow = np.where(three, c < target, c > target)  # move the free bound up
+        lo = np.where(grow, mid, lo)
+        hi = np.where(grow, hi, mid)
+    return bounds(best)
+
+
+# ---------------------------------------------------------------------------
+# clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index=0):
+        self.samples = []
+        self.proc = None
+        self.dev = device_index
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for nm, v in zip(names, s[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (the reference's StaticPSTCPUIter, compiled from its sources)
+
+_REF_CACHE = {}
+
+
+def reference_sample(n_sample, nq_sample, seed=1):
+    """The reference's StaticPSTCPUIter built over a sample of the workload and
+    queries of the same kind mix and selectivities, calibrated once with the
+    oracle's brute-force counts (threaded C scans, not timed)."""
+    key = (n_sample, nq_sample, seed)
+    if key in _REF_CACHE:
+        return _REF_CACHE[key]
+    import oracle
+    from concurrent.futures import ThreadPoolExecutor
+    pts = gen_points_host(n_sample, seed)
+    t0 = time.perf_counter()
+    ref = oracle.Ref(pts, "f32")
+    build_s = time.perf_counter() - t0
+    kinds, sel, anchor = query_plan(nq_sample, seed + 1)
+    names = {0: "three", 1: "left", 2: "right"}
+
+    def count_fn(k, a, b, c):
+        def one(i):
+            return len(oracle.Orc.brute(pts, "f32", names[int(k[i])], a[i], b[i], c[i]))
+        with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+            return np.array(list(ex.map(one, range(len(k)))), np.int64)
+    min1, max1, min2 = calibrate(count_fn, kinds, sel, anchor, n_sample, iters=16)
+    qs = [(names[int(kinds[i])], float(min1[i]), float(max1[i]), float(min2[i])) for i in range(nq_sample)]
+    _REF_CACHE[key] = (ref, qs, build_s)
+    return _REF_CACHE[key]
+
+
+def cpu_reference_time(ref, qs, threads):
+    """One timed pass of the reference's searches over qs; returns (pts/s, q/s, s, pts)."""
+    from concurrent.futures import ThreadPoolExecutor
+    t0 = time.perf_counter()
+    if threads == 1:
+        counts = [ref.count(*q) for q in qs]
+    else:
+        with ThreadPoolExecutor(max_workers=threads) as ex:
+            counts = list(ex.map(lambda q: ref.count(*q), qs))
+    dt = time.perf_counter() - t0
+    total = int(sum(counts))
+    return total / dt, len(qs) / dt, dt, total
+
+
+def ref_kind():
+    import oracle
+    return "reference" if oracle.Ref.available() else "port"
+
+
+# ---------------------------------------------------------------------------
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle
+    if not oracle.Ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libpstref.so was not built"}))
+        return 0
+    threads = os.cpu_count() or 1
+    n_sample, nq_sample = 1 << 22, 512
+    ref, qs, build_s = reference_sample(n_sample, nq_sample)
+    # Each reference search allocates a result array of n records (new[]), and
+    # those allocations contend across threads; use whichever of one thread or
+    # all host threads is faster on this box.
+    t_one = cpu_reference_time(ref, qs[:64], 1)[0]
+    t_all = cpu_reference_time(ref, qs[:64], threads)[0]
+    if t_one > t_all:
+        threads = 1
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, qps, dt, tot = cpu_reference_time(ref, qs, threads)
+        if i >= args.warmup:
+            vals.append((v, qps, {"search_s": dt}))
+    info0 = {"build_s": build_s}
+    v = statistics.median(x[0] for x in vals)
+    qps = statistics.median(x[1] for x in vals)
+    sample = (f"StaticPSTCPUIter over a 2^22-point sample of the workload, {nq_sample} queries per step "
+              f"with the same kind mix and selectivities, {threads} thread(s) (faster of 1 and all {os.cpu_count()})")
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.median(x[2]["search_s"] for x in vals),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "queries_per_s": qps,
+            "config": {"workload": "batched-4096-mixed-queries-2^28-f32 (reference CPU sample)", "n_points": N_POINTS,
+                       "queries_per_step": NQ, "selectivity": [SEL_LO, SEL_HI]},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample,
+                             "build_s_sample": info0["build_s"]},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200")
+    ap.add_argument("--points-log2", type=int, default=28)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--plain-queries", type=int, default=256)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    pst = load_package()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    n = 1 << args.points_log2
+    stream = torch.cuda.current_stream()
+
+    # ---- construction (timed separately, reported as extra keys)
+    pts_d = gen_points_device(n, seed=1 + rank, torch=torch)
+    torch.cuda.synchronize()
+    c0 = time.perf_counter()
+    tree = pst.StaticPSTGPU(pts_d, n, "f32", True)
+    torch.cuda.synchronize()
+    construct_ms = 1000 * (time.perf_counter() - c0)
+    del pts_d
+    torch.cuda.empty_cache()
+
+    # ---- queries
+    eng = pst.BatchEngine(tree, max_queries=NQ, task_capacity=1 << 26)
+    kinds, sel, anchor = query_plan(NQ, 7 + rank)
+
+    def count_fn(k, a, b, c):
+        q = pst.make_queries(k, a, b, c, "f32")
+        counts, _ = eng.count(q)
+        return counts.cpu().numpy()
+    min1, max1, min2 = calibrate(count_fn, kinds, sel, anchor, n)
+    q_host = pst.make_queries(kinds, min1, max1, min2, "f32")
+    counts, total = eng.count(q_host)
+    q_dev = torch.from_numpy(q_host.view(np.uint8).copy()).to("cuda")
+    out = torch.empty(total * 4 + 16, dtype=torch.uint8, device="cuda")
+    offs = torch.empty(NQ + 1, dtype=torch.int64, device="cuda")
+    st, tot = eng.run(q_dev, out, offs, queries_on_device=True, sync=True)
+    assert st == 0 and tot == total
+
+    # ---- device-resident timing (value)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for _ in range(args.warmup):
+        eng.run(q_dev, out, offs, queries_on_device=True, sync=False)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    step_ms = []
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            ev[0].record(stream)
+            eng.run(q_dev, out, offs, queries_on_device=True, sync=False)
+            ev[1].record(stream)
+            ev[1].synchronize()
+            step_ms.append(ev[0].elapsed_time(ev[1]))
+        torch.cuda.synchronize()
+    st_, tot2 = eng.run(q_dev, out, offs, queries_on_device=True, sync=True)
+    assert st_ == 0 and tot2 == total
+    my_ms = statistics.mean(step_ms)
+    pts_all, ms_all = float(total), my_ms
+    if dist:
+        t = torch.tensor([my_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_all = float(t.item())
+        p = torch.tensor([float(total)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(p, op=dist.ReduceOp.SUM)
+        pts_all = float(p.item())
+    value = pts_all / (ms_all / 1000.0)
+    qps = world * NQ / (ms_all / 1000.0)
+
+    # ---- end to end through the public call with host buffers
+    q_pin = torch.from_numpy(q_host.view(np.uint8).copy()).pin_memory()
+    out_pin = torch.empty(total * 4 + 16, dtype=torch.uint8).pin_memory()
+    offs_pin = torch.empty(NQ + 1, dtype=torch.int64).pin_memory()
+    e2e_ms = []
+    for i in range(args.warmup + max(3, args.steps // 4)):
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        q_dev.copy_(q_pin, non_blocking=True)
+        eng.run(q_dev, out, offs, queries_on_device=True, sync=True)
+        out_pin.copy_(out, non_blocking=True)
+        offs_pin.copy_(offs, non_blocking=True)
+        ev[1].record(stream)
+        ev[1].synchronize()
+        if i >= args.warmup:
+            e2e_ms.append(ev[0].elapsed_time(ev[1]))
+    e2e_val = total / (statistics.mean(e2e_ms) / 1000.0) * world
+
+    # ---- plain per-query drop-in path on a sample of the same queries
+    plain_n = min(args.plain_queries, NQ)
+    names = {0: "three", 1: "left", 2: "right"}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain_pts = 0
+    for i in range(plain_n):
+        r = tree.search(names[int(kinds[i])], float(min1[i]), float(max1[i]), float(min2[i]))
+        plain_pts += len(r)
+    plain_s = time.perf_counter() - t0
+    plain_qps = plain_n / plain_s
+
+    # ---- roofline of the batched search pass
+    peak, peak_kind = measured_peak()
+    achieved = total * BYTES_PER_PT / (my_ms / 1000.0) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None, "kernel": "batched search pass (k_bfs_level x levels + scan + k_emit)",
+            "bytes_per_unit": BYTES_PER_PT, "units_per_launch": total, "peak_source": f"{peak_kind} hbm_gbs"}
+    prof = ROOT / "profiles" / "traffic.json"
+    if prof.exists():
+        try:
+            roof["traffic"] = json.loads(prof.read_text()).get("search_bytes_per_step")
+        except Exception:
+            pass
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        try:
+            ref, qs, build_s = reference_sample(1 << 22, 128)
+            v, q, dt, tot = cpu_reference_time(ref, qs, 1)
+            cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": ref_kind(),
+                   "sample": "StaticPSTCPUIter, 2^22-point sample tree of the same distribution, 128 queries of the "
+                             "same kind mix and selectivities, 1 thread", "queries_per_s": q,
+                   "build_s_sample": build_s}
+        except Exception as e:  # the baseline must never sink the GPU number
+            cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": ref_kind(), "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_all, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "batched-4096-mixed-queries-2^28-f32", "n_points": n, "ids": "u32",
+                           "queries_per_step": NQ, "mix": "50% three / 25% left / 25% right",
+                           "selectivity": [SEL_LO, SEL_HI], "results": "ids",
+                           "l2": "inputs larger than L2 (tree ~9 GB)", "parallelism": f"{world} independent shards"},
+                "queries_per_s": qps, "points_per_step": total,
+                "plain_queries_per_s": plain_qps, "batched_vs_plain_qps": qps / world / plain_qps,
+                "construct_ms": construct_ms, "construct_pts_per_s": n / (construct_ms / 1000.0),
+                "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(q_host.nbytes),
+                        "d2h_bytes_per_step": int(total * 4 + (NQ + 1) * 8)},
+                "gpu_launches": None, "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary()}
+        levels = tree.info()["levels"]
+        line["gpu_launches"] = (levels + 6) * args.steps  # unpack+check + levels + 3 scan + emit per step
+        print(json.dumps(line))
+    eng.close()
+    tree.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

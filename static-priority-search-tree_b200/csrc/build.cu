@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(AM_THREADS) k_level_argmax(const uint32_t *__r
 		uint32_t ma = 0, mb = 0;
 		const uint64_t base = t0 + (uint64_t) threadIdx.x * AM_ITEMS;
 		uint32_t v[AM_ITEMS];
-		if (base + AM_ITEMS <= n) {
+		if (base + AM_ITEMS <= n && (reinterpret_cast<uintptr_t>(r2p1 + base) & 15) == 0) {
 			const uint4 a = *reinterpret_cast<const uint4 *>(r2p1 + base);
 			const uint4 b = *reinterpret_cast<const uint4 *>(r2p1 + base + 4);
 			v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
@@ -333,6 +333,20 @@ __global__ void k_level_nodes(BuildCtx<T, HAS_ID> c, uint32_t d, const uint32_t 
 // ---------------------------------------------------------------------------
 // Subtree builder: one CTA per node of level L0 finishes its whole subtree.
 
+// Shared-memory carve-up of k_subtree, in 32-bit words.
+constexpr uint32_t ST_OFF_KEYA = 0;
+constexpr uint32_t ST_OFF_POSA = ST_OFF_KEYA + ST_CAP;
+constexpr uint32_t ST_OFF_KEYB = ST_OFF_POSA + ST_CAP;
+constexpr uint32_t ST_OFF_POSB = ST_OFF_KEYB + ST_CAP;
+constexpr uint32_t ST_OFF_CNT = ST_OFF_POSB + ST_CAP;
+constexpr uint32_t ST_OFF_CNT2 = ST_OFF_CNT + ST_CAP;
+constexpr uint32_t ST_OFF_START = ST_OFF_CNT2 + ST_CAP;
+constexpr uint32_t ST_OFF_TOPI = ST_OFF_START + ST_CAP + 1;
+constexpr uint32_t ST_OFF_WS = ST_OFF_TOPI + ST_CAP;
+constexpr uint32_t ST_WORDS = ST_OFF_WS + 33;
+constexpr size_t st_smem_bytes() { return (size_t) ST_WORDS * 4; }
+static_assert(st_smem_bytes() <= 227 * 1024, "subtree builder shared memory");
+
 template <typename U>
 __device__ void block_scan_array(const U *in, U *out, uint32_t n, U *ws)
 {
@@ -357,15 +371,15 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
                                                        const uint32_t *__restrict__ B)
 {
 	extern __shared__ __align__(16) uint32_t st_smem[];
-	uint32_t *keyA = st_smem;
-	uint32_t *posA = keyA + ST_CAP;
-	uint32_t *keyB = posA + ST_CAP;
-	uint32_t *posB = keyB + ST_CAP;
-	uint32_t *cnt = posB + ST_CAP;       // [ST_CAP] counts of the current sub-level
-	uint32_t *cnt2 = cnt + ST_CAP;       // [ST_CAP] counts of the next sub-level
-	uint32_t *start = cnt2 + ST_CAP;     // [ST_CAP + 1]
-	uint32_t *topi = start + ST_CAP + 1; // [ST_CAP]
-	uint32_t *ws = topi + ST_CAP;        // [33]
+	uint32_t *keyA = st_smem + ST_OFF_KEYA;
+	uint32_t *posA = st_smem + ST_OFF_POSA;
+	uint32_t *keyB = st_smem + ST_OFF_KEYB;
+	uint32_t *posB = st_smem + ST_OFF_POSB;
+	uint32_t *cnt = st_smem + ST_OFF_CNT;     // [ST_CAP] counts of the current sub-level
+	uint32_t *cnt2 = st_smem + ST_OFF_CNT2;   // [ST_CAP] counts of the next sub-level
+	uint32_t *start = st_smem + ST_OFF_START; // [ST_CAP + 1]
+	uint32_t *topi = st_smem + ST_OFF_TOPI;   // [ST_CAP]
+	uint32_t *ws = st_smem + ST_OFF_WS;       // [33]
 	__shared__ uint32_t s_n;
 
 	const uint32_t j = blockIdx.x;
@@ -519,7 +533,6 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 	}
 }
 
-constexpr size_t st_smem_bytes() { return (size_t) (7 * ST_CAP + 1 + 33) * 4; }
 
 template <typename T>
 T *as(void *p)

@@ -64,17 +64,17 @@ def lib():
         "pst_info": (i32, [vp, P(u64), P(u32), P(u64), P(u64), P(i32), P(i32)]),
         "pst_export": (i32, [vp, vp, vp, vp, vp, vp]),
         "pst_search": (i32, [vp, P(Query), i32, P(vp), P(u64), vp]),
-        "pst_three_sided": (i32, [vp, Value, Value, Value, i32, P(vp), P(u64), vp]),
-        "pst_two_sided_left": (i32, [vp, Value, Value, i32, P(vp), P(u64), vp]),
-        "pst_two_sided_right": (i32, [vp, Value, Value, i32, P(vp), P(u64), vp]),
+        "pst_three_sided": (i32, [vp, u64, u64, u64, i32, P(vp), P(u64), vp]),
+        "pst_two_sided_left": (i32, [vp, u64, u64, i32, P(vp), P(u64), vp]),
+        "pst_two_sided_right": (i32, [vp, u64, u64, i32, P(vp), P(u64), vp]),
         "pst_search_into": (i32, [vp, P(Query), i32, vp, u64, P(u64), vp]),
         "pst_batch_create": (i32, [P(vp), vp, P(BatchOpts)]),
         "pst_batch_destroy": (i32, [vp]),
         "pst_batch_run": (i32, [vp, vp, u32, i32, i32, vp, u64, vp, P(u64), i32, vp]),
         "pst_batch_count": (i32, [vp, vp, u32, i32, vp, P(u64), vp]),
         "pst_batch_status": (i32, [vp, P(u64)]),
-        "pst_ips_search": (i32, [i32, i32, vp, u64, Value, i32, P(vp), P(u64), u32, u32, vp]),
-        "pst_ips_search_into": (i32, [i32, i32, vp, u64, Value, i32, vp, u64, P(u64), vp]),
+        "pst_ips_search": (i32, [i32, i32, vp, u64, u64, i32, P(vp), P(u64), u32, u32, vp]),
+        "pst_ips_search_into": (i32, [i32, i32, vp, u64, u64, i32, vp, u64, P(u64), vp]),
         "pst_num_metacells": (i32, [P(u32), P(u32), P(u32), P(u64)]),
         "pst_form_metacells": (i32, [i32, i32, vp, P(u32), P(u32), vp, vp]),
     }
@@ -116,6 +116,14 @@ def value(dt: str, v) -> Value:
     x = Value()
     setattr(x, dt, NP[dt](v).item())
     return x
+
+
+def value_arg(dt: str, v) -> int:
+    """A pst_value passed by value.  ctypes cannot pass unions by value, but on
+    x86-64 (System V) this 8-byte union of float/double/int32 is classified INTEGER
+    and travels in one general-purpose register, exactly like a uint64 holding its
+    bytes (4-byte members in the low half)."""
+    return int.from_bytes(bytes(value(dt, v)), "little")
 
 
 def points_to_device(pts: np.ndarray):
@@ -225,21 +233,21 @@ class StaticPSTGPU:
     def threeSidedSearch(self, min_dim1_val, max_dim1_val, min_dim2_val, ret="points"):
         r, rec = self._ret(ret)
         out, cnt = C.c_void_p(), C.c_uint64()
-        _check(lib().pst_three_sided(self._h, value(self.dt, min_dim1_val), value(self.dt, max_dim1_val),
-                                     value(self.dt, min_dim2_val), RET[r], C.byref(out), C.byref(cnt), _stream()))
+        _check(lib().pst_three_sided(self._h, value_arg(self.dt, min_dim1_val), value_arg(self.dt, max_dim1_val),
+                                     value_arg(self.dt, min_dim2_val), RET[r], C.byref(out), C.byref(cnt), _stream()))
         return _take_device_result(out.value or 0, cnt.value, rec)
 
     def twoSidedLeftSearch(self, max_dim1_val, min_dim2_val, ret="points"):
         r, rec = self._ret(ret)
         out, cnt = C.c_void_p(), C.c_uint64()
-        _check(lib().pst_two_sided_left(self._h, value(self.dt, max_dim1_val), value(self.dt, min_dim2_val),
+        _check(lib().pst_two_sided_left(self._h, value_arg(self.dt, max_dim1_val), value_arg(self.dt, min_dim2_val),
                                         RET[r], C.byref(out), C.byref(cnt), _stream()))
         return _take_device_result(out.value or 0, cnt.value, rec)
 
     def twoSidedRightSearch(self, min_dim1_val, min_dim2_val, ret="points"):
         r, rec = self._ret(ret)
         out, cnt = C.c_void_p(), C.c_uint64()
-        _check(lib().pst_two_sided_right(self._h, value(self.dt, min_dim1_val), value(self.dt, min_dim2_val),
+        _check(lib().pst_two_sided_right(self._h, value_arg(self.dt, min_dim1_val), value_arg(self.dt, min_dim2_val),
                                          RET[r], C.byref(out), C.byref(cnt), _stream()))
         return _take_device_result(out.value or 0, cnt.value, rec)
 
@@ -343,7 +351,7 @@ def intervalParallelSearch(pts_d, num_elems: int, search_val, dt: str = "f32", h
     """Mirror of intervalParallelSearch (interval-parallel-search/interval-parallel-search.h:29)."""
     out, cnt = C.c_void_p(), C.c_uint64()
     _check(lib().pst_ips_search(DTYPE[dt], IDTYPE[has_id], C.c_void_p(pts_d.data_ptr()), num_elems,
-                                value(dt, search_val), RET[ret], C.byref(out), C.byref(cnt), num_thread_blocks,
+                                value_arg(dt, search_val), RET[ret], C.byref(out), C.byref(cnt), num_thread_blocks,
                                 threads_per_block, _stream(stream)))
     rec = np.uint32 if ret == "ids" else point_dtype(dt, has_id)
     return _take_device_result(out.value or 0, cnt.value, rec)
