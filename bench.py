@@ -40,6 +40,14 @@ SEL_LO, SEL_HI = 1e-7, 1e-2
 BYTES_PER_PT = 12  # dim2 tested (4) + id read (4) + id written (4), float32 tree returning ids
 
 
+_T0 = time.perf_counter()
+
+
+def log(msg):
+    """Progress on stderr (stdout carries only the JSON line)."""
+    print(f"[bench {time.perf_counter() - _T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
 def load_package():
     if "pst_b200" in sys.modules:
         return sys.modules["pst_b200"]
@@ -318,11 +326,12 @@ def main():
     tree = pst.StaticPSTGPU(pts_d, n, "f32", True)
     torch.cuda.synchronize()
     construct_ms = 1000 * (time.perf_counter() - c0)
+    log(f"constructed 2^{args.points_log2} points in {construct_ms:.1f} ms")
     del pts_d
     torch.cuda.empty_cache()
 
     # ---- queries
-    eng = pst.BatchEngine(tree, max_queries=NQ, task_capacity=1 << 26)
+    eng = pst.BatchEngine(tree, max_queries=NQ, task_capacity=max(1 << 20, n >> 2))
     kinds, sel, anchor = query_plan(NQ, 7 + rank)
 
     def count_fn(k, a, b, c):
@@ -330,6 +339,7 @@ def main():
         counts, _ = eng.count(q)
         return counts.cpu().numpy()
     min1, max1, min2 = calibrate(count_fn, kinds, sel, anchor, n)
+    log("calibrated query bounds")
     q_host = pst.make_queries(kinds, min1, max1, min2, "f32")
     counts, total = eng.count(q_host)
     q_dev = torch.from_numpy(q_host.view(np.uint8).copy()).to("cuda")
@@ -348,16 +358,19 @@ def main():
     step_ms = []
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("timed")
         for _ in range(args.steps):
             ev[0].record(stream)
             eng.run(q_dev, out, offs, queries_on_device=True, sync=False)
             ev[1].record(stream)
             ev[1].synchronize()
             step_ms.append(ev[0].elapsed_time(ev[1]))
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
     st_, tot2 = eng.run(q_dev, out, offs, queries_on_device=True, sync=True)
     assert st_ == 0 and tot2 == total
     my_ms = statistics.mean(step_ms)
+    log(f"timed {args.steps} steps: {my_ms:.3f} ms/step, {total} points/step")
     pts_all, ms_all = float(total), my_ms
     if dist:
         t = torch.tensor([my_ms], device="cuda")
@@ -386,6 +399,7 @@ def main():
         if i >= args.warmup:
             e2e_ms.append(ev[0].elapsed_time(ev[1]))
     e2e_val = total / (statistics.mean(e2e_ms) / 1000.0) * world
+    log(f"e2e {statistics.mean(e2e_ms):.3f} ms/step")
 
     # ---- plain per-query drop-in path on a sample of the same queries
     plain_n = min(args.plain_queries, NQ)
@@ -398,6 +412,7 @@ def main():
         plain_pts += len(r)
     plain_s = time.perf_counter() - t0
     plain_qps = plain_n / plain_s
+    log(f"plain per-query path: {plain_qps:.1f} queries/s")
 
     # ---- roofline of the batched search pass
     peak, peak_kind = measured_peak()

@@ -316,11 +316,12 @@ class BatchEngine:
 
     def run(self, queries, out_d, offsets_d, ret="ids", queries_on_device=False, sync=True, stream=None):
         """Returns (status, total).  queries: host numpy pst_query array or device tensor."""
-        nq = len(queries)
         if queries_on_device:
+            nq = queries.numel() * queries.element_size() // QUERY_NP.itemsize
             qp = C.c_void_p(queries.data_ptr())
         else:
             queries = np.ascontiguousarray(queries)
+            nq = len(queries)
             qp = queries.ctypes.data_as(C.c_void_p)
         rec = 4 if ret == "ids" else self.tree.rec_point.itemsize
         cap = out_d.numel() * out_d.element_size() // rec

@@ -62,3 +62,22 @@ def rand_queries(pts: np.ndarray, k: int, seed: int = 2):
             m2 = rng.choice(d1)
         out.append((kind, a, b, m2))
     return out
+
+
+def blob_volume(px: int, py: int, pz: int, nblobs: int = 32, seed: int = 1, noise: float = 0.01,
+                sigma=(8.0, 40.0), amp=(0.5, 1.0)) -> np.ndarray:
+    """Sum of isotropic Gaussian blobs (centres uniform over the grid, sigma and
+    amplitude uniform in the given ranges) plus N(0, noise) in float32, shape
+    (pz, py, px), x fastest.  Each blob is evaluated separably over its 4-sigma box."""
+    rng = np.random.default_rng(seed)
+    vol = np.zeros((pz, py, px), np.float32)
+    for _ in range(nblobs):
+        c = rng.uniform([0, 0, 0], [px, py, pz])
+        s = rng.uniform(*sigma)
+        a = np.float32(rng.uniform(*amp))
+        lo = np.maximum(np.floor(c - 4 * s).astype(int), 0)
+        hi = np.minimum(np.ceil(c + 4 * s).astype(int) + 1, [px, py, pz])
+        g = [np.exp(-0.5 * ((np.arange(lo[i], hi[i]) - c[i]) / s) ** 2).astype(np.float32) for i in range(3)]
+        vol[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]] += a * (g[2][:, None, None] * g[1][None, :, None] * g[0][None, None, :])
+    vol += rng.normal(0.0, noise, vol.shape).astype(np.float32)
+    return vol
