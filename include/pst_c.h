@@ -178,6 +178,56 @@ pst_status pst_batch_count(pst_batch *batch, const pst_query *queries, uint32_t 
 pst_status pst_batch_status(pst_batch *batch, uint64_t *total);
 
 /* ------------------------------------------------------------------------- */
+/* Serving: a request loop over several resident trees with continuous batching.
+ * Requests that arrive while other batches are on the device join the next free
+ * batch slot; each batch runs its count pass, and its emit is admitted when the
+ * exact output bytes that pass predicts fit the free result arena.  Batches of
+ * different trees and slots run on separate streams and overlap on the device.
+ * Latency is measured from each request's arrival time to the moment its result
+ * is in host memory.  The reference has no serving layer; each request is the
+ * search of pst/static-pst-gpu.tu:496-642. */
+
+typedef struct pst_server pst_server;
+
+typedef struct pst_server_opts {
+	uint32_t max_batch;        /* queries per batch (0 = 1024) */
+	uint32_t slots_per_tree;   /* batches in flight per tree (0 = 2) */
+	uint64_t out_budget_bytes; /* device bytes for results in flight (0 = 1 GiB) */
+	int32_t use_graph;         /* replay each slot's pass from a CUDA graph */
+	int32_t keep_results;      /* 1: results copied to host and kept for pst_server_take;
+	                              2: copied to host (latency includes it) then dropped;
+	                              0: results stay in device memory, only counts are kept */
+} pst_server_opts;
+
+typedef struct pst_server_stats {
+	uint64_t submitted, completed, failed, cancelled, batches, points;
+	uint64_t peak_out_bytes;   /* largest arena use seen */
+	double p50_ms, p90_ms, p99_ms, mean_ms, max_ms; /* over requests completed since the last reset */
+	double busy_s;             /* wall time from the first arrival to the last completion */
+} pst_server_stats;
+
+pst_status pst_server_create(pst_server **out, const pst_server_opts *opts);
+/* Registers a resident tree (it must outlive the server); returns its index. */
+pst_status pst_server_add_tree(pst_server *srv, pst_tree *tree, uint32_t *tree_index);
+/* Queues n requests.  arrival_ns (CLOCK_MONOTONIC, may be NULL = now) is the
+ * arrival time latency is measured from.  ids receives request ids. */
+pst_status pst_server_submit(pst_server *srv, uint32_t n, const uint32_t *tree_index, const pst_query *queries,
+                             pst_ret ret, const uint64_t *arrival_ns, uint64_t *ids);
+/* Waits (bounded by timeout_ms) until request id is done; PST_ERR_TIMEOUT otherwise.
+ * *status receives the request's own status, *count its result size. */
+pst_status pst_server_wait(pst_server *srv, uint64_t id, uint32_t timeout_ms, pst_status *status, uint64_t *count);
+/* Copies a finished request's result (kept results only) to host memory of
+ * `capacity` records and forgets the request. */
+pst_status pst_server_take(pst_server *srv, uint64_t id, void *host_out, uint64_t capacity, uint64_t *count);
+/* Cancels a request that has not completed; its result is dropped. */
+pst_status pst_server_cancel(pst_server *srv, uint64_t id);
+/* Waits (bounded) until every submitted request is done. */
+pst_status pst_server_drain(pst_server *srv, uint32_t timeout_ms);
+pst_status pst_server_get_stats(pst_server *srv, pst_server_stats *stats);
+pst_status pst_server_reset_stats(pst_server *srv);
+pst_status pst_server_destroy(pst_server *srv);
+
+/* ------------------------------------------------------------------------- */
 /* Interval parallel search: every point with dim1 <= v <= dim2, by a full scan.
  * Drop-in mode: like the reference, the result buffer is cudaMalloc'd with room
  * for all n points (the caller frees it) and *count records are valid; it is

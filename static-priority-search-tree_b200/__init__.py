@@ -14,6 +14,7 @@ StaticPSTGPU with threeSidedSearch / twoSidedLeftSearch / twoSidedRightSearch
 from .pst import (  # noqa: F401
     BatchEngine,
     PSTError,
+    Server,
     StaticPSTGPU,
     StaticPSTGPUArr,
     calcNumMetacells,

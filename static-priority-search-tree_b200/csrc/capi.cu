@@ -1,6 +1,7 @@
 // C ABI (include/pst_c.h): argument checks, error translation, and the drop-in
 // search semantics of the reference (callee-allocated results, blocking calls).
 #include <cstdio>
+#include <functional>
 #include <memory>
 #include <new>
 #include <string>
@@ -8,10 +9,6 @@
 #include "scan_kernels.cuh"
 #include "search.cuh"
 #include "tree.cuh"
-
-struct pst_tree {
-	pst::TreeStorage t;
-};
 
 struct pst_batch {
 	pst::Batch b;
@@ -102,6 +99,8 @@ static pst_status guarded(F &&f)
 		return translate(std::current_exception());
 	}
 }
+
+pst_status guarded_call(const std::function<void()> &f) { return guarded(f); }
 
 static void malloc_result(void **out, uint64_t bytes)
 {

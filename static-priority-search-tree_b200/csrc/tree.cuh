@@ -47,3 +47,8 @@ void free_tree(TreeStorage &t);
 void export_tree(const TreeStorage &t, void *dim1, void *dim2, void *med, uint32_t *ids, uint8_t *bitcodes);
 
 }  // namespace pst
+
+// Opaque handle of the C ABI.
+struct pst_tree {
+	pst::TreeStorage t;
+};

@@ -38,6 +38,18 @@ class BatchOpts(C.Structure):
                 ("blocks_per_sm", C.c_uint32), ("use_graph", C.c_int32)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("max_batch", C.c_uint32), ("slots_per_tree", C.c_uint32), ("out_budget_bytes", C.c_uint64),
+                ("use_graph", C.c_int32), ("keep_results", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("cancelled", C.c_uint64), ("batches", C.c_uint64), ("points", C.c_uint64),
+                ("peak_out_bytes", C.c_uint64), ("p50_ms", C.c_double), ("p90_ms", C.c_double),
+                ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double), ("busy_s", C.c_double)]
+
+
 QUERY_NP = np.dtype([("kind", "<i4"), ("reserved", "<i4"), ("min1", "<u8"), ("max1", "<u8"), ("min2", "<u8")])
 
 _lib = None
@@ -76,6 +88,16 @@ def lib():
         "pst_ips_search": (i32, [i32, i32, vp, u64, u64, i32, P(vp), P(u64), u32, u32, vp]),
         "pst_ips_search_into": (i32, [i32, i32, vp, u64, u64, i32, vp, u64, P(u64), vp]),
         "pst_num_metacells": (i32, [P(u32), P(u32), P(u32), P(u64)]),
+        "pst_server_create": (i32, [P(vp), P(ServerOpts)]),
+        "pst_server_add_tree": (i32, [vp, vp, P(u32)]),
+        "pst_server_submit": (i32, [vp, u32, vp, vp, i32, vp, vp]),
+        "pst_server_wait": (i32, [vp, u64, u32, P(i32), P(u64)]),
+        "pst_server_take": (i32, [vp, u64, vp, u64, P(u64)]),
+        "pst_server_cancel": (i32, [vp, u64]),
+        "pst_server_drain": (i32, [vp, u32]),
+        "pst_server_get_stats": (i32, [vp, P(ServerStats)]),
+        "pst_server_reset_stats": (i32, [vp]),
+        "pst_server_destroy": (i32, [vp]),
         "pst_form_metacells": (i32, [i32, i32, vp, P(u32), P(u32), vp, vp]),
     }
     for name, (res, args) in sigs.items():
@@ -345,6 +367,76 @@ class BatchEngine:
         torch.cuda.synchronize()
         res = out[: tot * rsz].cpu().numpy().view(rec)
         return offs.cpu().numpy().astype(np.uint64), res
+
+
+class Server:
+    """Serving loop over resident trees (pst_server_*)."""
+
+    def __init__(self, max_batch=1024, slots_per_tree=2, out_budget_bytes=1 << 30, use_graph=True,
+                 keep_results=1):
+        keep_results = int(keep_results)
+        self.keep_results = keep_results
+        o = ServerOpts(max_batch, slots_per_tree, out_budget_bytes, int(use_graph), int(keep_results))
+        self._h = C.c_void_p()
+        _check(lib().pst_server_create(C.byref(self._h), C.byref(o)))
+        self.trees = []
+
+    def add_tree(self, tree: StaticPSTGPU) -> int:
+        idx = C.c_uint32()
+        _check(lib().pst_server_add_tree(self._h, tree.handle, C.byref(idx)))
+        self.trees.append(tree)
+        return idx.value
+
+    def submit(self, tree_index, queries: np.ndarray, ret="ids", arrival_ns=None) -> np.ndarray:
+        """Queues requests; tree_index is an int or an array (one per query)."""
+        q = np.ascontiguousarray(queries)
+        n = len(q)
+        ti = np.ascontiguousarray(np.broadcast_to(np.asarray(tree_index, np.uint32), (n,)))
+        ids = np.zeros(n, np.uint64)
+        arr = None if arrival_ns is None else np.ascontiguousarray(np.asarray(arrival_ns, np.uint64))
+        p = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        _check(lib().pst_server_submit(self._h, n, p(ti), p(q), RET[ret], p(arr), p(ids)))
+        return ids
+
+    def wait(self, rid: int, timeout_ms: int = 10000):
+        """Returns (status, count) or raises PSTError(PST_ERR_TIMEOUT)."""
+        st, cnt = C.c_int32(), C.c_uint64()
+        _check(lib().pst_server_wait(self._h, int(rid), timeout_ms, C.byref(st), C.byref(cnt)))
+        return st.value, cnt.value
+
+    def take(self, rid: int, rec) -> np.ndarray:
+        _, cnt = self.wait(rid)
+        rec = np.dtype(rec)
+        out = np.zeros(max(cnt, 1), rec)
+        c = C.c_uint64()
+        _check(lib().pst_server_take(self._h, int(rid), out.ctypes.data_as(C.c_void_p) if self.keep_results == 1 else None,
+                                     len(out), C.byref(c)))
+        return out[: c.value]
+
+    def cancel(self, rid: int):
+        _check(lib().pst_server_cancel(self._h, int(rid)))
+
+    def drain(self, timeout_ms: int = 60000):
+        _check(lib().pst_server_drain(self._h, timeout_ms))
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().pst_server_get_stats(self._h, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+
+    def reset_stats(self):
+        _check(lib().pst_server_reset_stats(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _check(lib().pst_server_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def intervalParallelSearch(pts_d, num_elems: int, search_val, dt: str = "f32", has_id: bool = True, ret="ids",
