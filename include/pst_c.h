@@ -141,6 +141,23 @@ pst_status pst_two_sided_right(pst_tree *tree, pst_value min1, pst_value min2, p
 pst_status pst_search_into(pst_tree *tree, const pst_query *query, pst_ret ret, void *out_d,
                            uint64_t capacity, uint64_t *count, pst_stream_t stream);
 
+/* One query into a caller buffer without allocating anything.  It has no
+ * counterpart in the reference.  It is for callers that cannot allocate device
+ * memory while they search: code whose device memory is all held by its own
+ * allocator, and latency-critical loops that cannot take the device-wide
+ * synchronisation of cudaMalloc/cudaFree.  Its working memory is a static 8 MiB
+ * device array in the library (held by every GPU that loads it until the process
+ * exits), which bounds the tree: at most 2^22 - 1 = 4,194,303 points, larger trees
+ * are rejected with PST_ERR_CAPACITY before any work.  The result contract is
+ * pst_search_into's: *count is the full size, PST_ERR_CAPACITY (nothing written)
+ * when it exceeds `capacity`.  Blocks until complete.  The first call on a device
+ * looks up the array's device address; make that first call before any stream
+ * capture.  All calls on a device share the array, so calls whose GPU work
+ * overlapped would race; calls from one process are serialised (each holds a lock
+ * until its work has completed). */
+pst_status pst_search_noalloc(pst_tree *tree, const pst_query *query, pst_ret ret, void *out_d,
+                              uint64_t capacity, uint64_t *count, pst_stream_t stream);
+
 /* ------------------------------------------------------------------------- */
 /* Batched queries: many queries of mixed kinds in one level-synchronous pass
  * (count prepass, exact offsets, emit), replayed from a captured CUDA graph.

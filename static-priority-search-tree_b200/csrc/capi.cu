@@ -322,6 +322,32 @@ pst_status pst_search_into(pst_tree *tree, const pst_query *query, pst_ret ret, 
 	return st;
 }
 
+pst_status pst_search_noalloc(pst_tree *tree, const pst_query *query, pst_ret ret, void *out_d, uint64_t capacity,
+                              uint64_t *count, pst_stream_t stream)
+{
+	uint64_t total = 0;
+	pst_status st = guarded([&] {
+		if (!tree || !query || !count)
+			fail(PST_ERR_INVALID, "null tree, query or count");
+		if (ret != PST_RET_IDS && ret != PST_RET_POINTS)
+			fail(PST_ERR_INVALID, "bad return type");
+		if (ret == PST_RET_IDS && tree->t.idtype != PST_ID_U32)
+			fail(PST_ERR_UNSUPPORTED, "an id-less tree can only return points");
+		*count = 0;
+		if (tree->t.n == 0)
+			return;
+		if (!out_d && capacity)
+			fail(PST_ERR_INVALID, "null output buffer");
+		total = search_noalloc(tree->t, *query, ret, out_d, capacity, reinterpret_cast<cudaStream_t>(stream));
+		*count = total;
+	});
+	if (st == PST_OK && total > capacity) {
+		g_last_error = "result of " + std::to_string(total) + " records exceeds capacity " + std::to_string(capacity);
+		return PST_ERR_CAPACITY;
+	}
+	return st;
+}
+
 pst_status pst_batch_create(pst_batch **out, pst_tree *tree, const pst_batch_opts *opts)
 {
 	return guarded([&] {

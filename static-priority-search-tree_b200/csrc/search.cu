@@ -17,6 +17,8 @@
 // the pass; an exclusive scan gives each query's exact output offset and a flat
 // emit kernel writes ids (or points) from the recorded masks.
 #include <algorithm>
+#include <mutex>
+#include <string>
 #include <type_traits>
 #include <vector>
 
@@ -583,6 +585,152 @@ void Batch::count_sync(cudaStream_t s, uint64_t *total)
 uint64_t Batch::record_size(pst_ret ret) const
 {
 	return ret == PST_RET_IDS ? 4 : point_size(tree->dtype, tree->idtype);
+}
+
+// ---------------------------------------------------------------------------
+// Single query with no allocation at all (pst_search_noalloc).
+//
+// For callers that cannot allocate device memory during a search: code whose
+// device memory is all owned by its own allocator (so a cudaMalloc here would fail
+// or compete with it), and latency-critical loops that cannot take the implicit
+// device-wide synchronisation of cudaMalloc/cudaFree.  The search's working memory
+// (control block, the query, its boundary paths and its frontier) lives in the
+// file-scope array below, which every GPU that loads this library holds until the
+// process exits.
+
+namespace {
+
+constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(8) << 20;  // 8 MiB per device
+constexpr uint32_t NOALLOC_MAX_LEVELS = 22;                  // trees of up to 2^22 - 1 points
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+// Sub-buffers of the scratch array, 256-byte aligned, in bytes.
+constexpr size_t NA_CTL = 0;
+constexpr size_t NA_QRAW = 512;
+constexpr size_t NA_KIND = NA_QRAW + 256;
+constexpr size_t NA_MIN1 = NA_KIND + 256;
+constexpr size_t NA_MAX1 = NA_MIN1 + 256;
+constexpr size_t NA_MIN2 = NA_MAX1 + 256;
+constexpr size_t NA_PATH0 = NA_MIN2 + 256;
+constexpr size_t NA_PATH1 = NA_PATH0 + 256;
+constexpr size_t NA_COUNTS = NA_PATH1 + 256;
+constexpr size_t NA_CURSOR = NA_COUNTS + 256;
+constexpr size_t NA_OFFSETS = NA_CURSOR + 256;
+constexpr size_t NA_SCAN = NA_OFFSETS + 256;
+constexpr size_t NA_TASKS = NA_SCAN + 256;
+// tasks (16 B) and survivor masks (4 B) share the rest
+constexpr uint64_t NA_TASK_CAP = (NOALLOC_SCRATCH_BYTES - NA_TASKS) / (sizeof(uint4) + 4);
+constexpr size_t NA_AMASK = NA_TASKS + NA_TASK_CAP * sizeof(uint4);
+static_assert(sizeof(BatchCtl) <= NA_QRAW, "control block");
+static_assert(NA_AMASK + NA_TASK_CAP * 4 <= NOALLOC_SCRATCH_BYTES, "scratch layout");
+// One query's frontier holds at most one task per 32-slot chunk of every level,
+// plus per level at most two report-above seeds and two boundary results:
+// 2^L/16 + 4L + 32 tasks for a tree of L levels.
+static_assert((1ull << NOALLOC_MAX_LEVELS) / 16 + 4 * NOALLOC_MAX_LEVELS + 32 <= NA_TASK_CAP, "frontier bound");
+
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_ptr[64] = {};
+
+// Device address of the scratch array for the current device, looked up once per
+// device with that device current (the host-side name of a __device__ array is only
+// a stand-in for it).
+unsigned char *noalloc_scratch(int dev)
+{
+	if (dev < 0 || dev >= 64)
+		fail(PST_ERR_CUDA, "device index out of range");
+	if (!g_noalloc_ptr[dev]) {
+		void *p = nullptr;
+		check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(no-alloc scratch)");
+		g_noalloc_ptr[dev] = static_cast<unsigned char *>(p);
+	}
+	return g_noalloc_ptr[dev];
+}
+
+template <typename T>
+uint64_t noalloc_run(TreeStorage &t, const pst_query &q, pst_ret ret, void *out, uint64_t capacity, cudaStream_t s,
+                     unsigned char *base)
+{
+	BatchCtl *ctl = reinterpret_cast<BatchCtl *>(base + NA_CTL);
+	pst_query *qraw = reinterpret_cast<pst_query *>(base + NA_QRAW);
+	uint32_t *kind = reinterpret_cast<uint32_t *>(base + NA_KIND);
+	T *min1 = reinterpret_cast<T *>(base + NA_MIN1);
+	T *max1 = reinterpret_cast<T *>(base + NA_MAX1);
+	T *min2 = reinterpret_cast<T *>(base + NA_MIN2);
+	uint4 *path0 = reinterpret_cast<uint4 *>(base + NA_PATH0);
+	uint4 *path1 = reinterpret_cast<uint4 *>(base + NA_PATH1);
+	uint64_t *counts = reinterpret_cast<uint64_t *>(base + NA_COUNTS);
+	uint64_t *cursor = reinterpret_cast<uint64_t *>(base + NA_CURSOR);
+	uint64_t *offsets = reinterpret_cast<uint64_t *>(base + NA_OFFSETS);
+	uint64_t *scan = reinterpret_cast<uint64_t *>(base + NA_SCAN);
+	uint4 *tasks = reinterpret_cast<uint4 *>(base + NA_TASKS);
+	uint32_t *amask = reinterpret_cast<uint32_t *>(base + NA_AMASK);
+
+	// The array keeps the previous call's contents: reset everything that must
+	// start at zero (control block with nq = 1, count, output cursor).
+	BatchCtl h{};
+	h.nq = 1;
+	PST_CUDA(cudaMemcpyAsync(ctl, &h, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
+	PST_CUDA(cudaMemcpyAsync(qraw, &q, sizeof(pst_query), cudaMemcpyHostToDevice, s));
+	PST_CUDA(cudaMemsetAsync(counts, 0, 8, s));
+	PST_CUDA(cudaMemsetAsync(cursor, 0, 8, s));
+
+	int occ = 0;
+	PST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bfs_kernel_ptr<T>(), BFS_THREADS, 0));
+	const unsigned grid = (unsigned) device_info().sms * (unsigned) std::max(occ, 1);
+	TreeDev<T> tv = t.view<T>();
+	QDev<T> qd{kind, min1, max1, min2};
+	WorkDev w{tasks, amask, NA_TASK_CAP, path0, path1, 2u, counts, cursor, offsets, ctl};
+	k_check_kinds<<<1, 32, 0, s>>>(qraw, ctl);
+	k_unpack_queries<T><<<1, 32, 0, s>>>(qraw, ctl, kind, min1, max1, min2, path0);
+	for (uint32_t d = 0; d < tv.levels; d++)
+		k_bfs_level<T><<<grid, BFS_THREADS, 0, s>>>(tv, qd, w, d);
+	exclusive_scan<uint64_t>(counts, offsets, 1, scan, &ctl->total, s);
+	PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
+	PST_CUDA(cudaStreamSynchronize(s));
+	if (h.flags & BATCH_FLAG_BAD_QUERY)
+		fail(PST_ERR_INVALID, "query kind must be PST_Q_THREE, PST_Q_LEFT or PST_Q_RIGHT");
+	if (h.flags & (BATCH_FLAG_TASK_OVERFLOW | BATCH_FLAG_INTERNAL))
+		fail(PST_ERR_INTERNAL, "no-alloc search: frontier consistency check failed");
+	if (h.total == 0 || h.total > capacity)
+		return h.total;
+	const bool has_id = t.idtype == PST_ID_U32;
+	if (ret == PST_RET_IDS)
+		k_emit<T, true, false><<<grid, BFS_THREADS, 0, s>>>(tv, w, out, capacity);
+	else if (has_id)
+		k_emit<T, true, true><<<grid, BFS_THREADS, 0, s>>>(tv, w, out, capacity);
+	else
+		k_emit<T, false, true><<<grid, BFS_THREADS, 0, s>>>(tv, w, out, capacity);
+	PST_CUDA(cudaGetLastError());
+	PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
+	PST_CUDA(cudaStreamSynchronize(s));
+	if (h.flags & (BATCH_FLAG_OUT_OVERFLOW | BATCH_FLAG_INTERNAL))
+		fail(PST_ERR_INTERNAL, "no-alloc search: emit consistency check failed");
+	return h.total;
+}
+
+}  // namespace
+
+uint64_t search_noalloc(TreeStorage &t, const pst_query &q, pst_ret ret, void *out, uint64_t capacity, cudaStream_t s)
+{
+	if (t.levels > NOALLOC_MAX_LEVELS)
+		fail(PST_ERR_CAPACITY, "pst_search_noalloc handles trees of at most " +
+		                           std::to_string((1ull << NOALLOC_MAX_LEVELS) - 1) + " points (" +
+		                           std::to_string(NOALLOC_SCRATCH_BYTES >> 20) + " MiB static scratch); this tree has " +
+		                           std::to_string(t.n));
+	int dev = 0;
+	PST_CUDA(cudaGetDevice(&dev));
+	// Every call on a device shares the one array, so two calls whose GPU work
+	// overlapped would race on it; within this process the lock, held until the
+	// call's work has completed, keeps calls from overlapping.
+	std::lock_guard<std::mutex> lk(g_noalloc_mu);
+	unsigned char *base = noalloc_scratch(dev);
+	switch (t.dtype) {
+	case PST_F32: return noalloc_run<float>(t, q, ret, out, capacity, s, base);
+	case PST_F64: return noalloc_run<double>(t, q, ret, out, capacity, s, base);
+	case PST_I32: return noalloc_run<int32_t>(t, q, ret, out, capacity, s, base);
+	}
+	fail(PST_ERR_INVALID, "bad dtype");
 }
 
 }  // namespace pst

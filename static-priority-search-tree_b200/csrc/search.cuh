@@ -70,4 +70,8 @@ struct Batch {
 	void enqueue_emit_t(void *out, uint64_t capacity, cudaStream_t s);
 };
 
+// One query into a caller buffer using only the library's static device scratch
+// (no allocation); see pst_search_noalloc in include/pst_c.h.
+uint64_t search_noalloc(TreeStorage &t, const pst_query &q, pst_ret ret, void *out, uint64_t capacity, cudaStream_t s);
+
 }  // namespace pst
