@@ -144,6 +144,82 @@ def calibrate(count_fn, kinds, sel, anchor, n, iters=24, domain=float(1 << 24)):
     return bounds(best)
 
 
+def blob_volume_device(px, py, pz, seed, torch, nblobs=32, noise=0.01):
+    """Sum of 32 isotropic Gaussian blobs (centres uniform over the grid, sigma
+    ~U[8,40] voxels, amplitude ~U[0.5,1]) + N(0, noise), float32 (pz, py, px) on
+    the device; each blob is evaluated separably over its 4-sigma box."""
+    rng = np.random.default_rng(seed)
+    vol = torch.zeros((pz, py, px), dtype=torch.float32, device="cuda")
+    for _ in range(nblobs):
+        c = rng.uniform([0, 0, 0], [px, py, pz])
+        s = rng.uniform(8.0, 40.0)
+        a = float(rng.uniform(0.5, 1.0))
+        lo = np.maximum(np.floor(c - 4 * s).astype(int), 0)
+        hi = np.minimum(np.ceil(c + 4 * s).astype(int) + 1, [px, py, pz])
+        g = [torch.exp(-0.5 * ((torch.arange(int(lo[i]), int(hi[i]), device="cuda", dtype=torch.float32)
+                                 - float(c[i])) / s) ** 2) for i in range(3)]
+        vol[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]] += a * (g[2][:, None, None] * g[1][None, :, None]
+                                                           * g[0][None, None, :])
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    vol += noise * torch.randn(vol.shape, generator=gen, device="cuda", dtype=torch.float32)
+    return vol
+
+
+SERVING_VOLUMES = [(64, 64, 64), (128, 128, 128), (192, 192, 192), (256, 256, 256), (384, 384, 384),
+                   (512, 512, 512), (768, 768, 512), (1024, 1024, 512)]
+
+
+def serving_bench(pst, torch, rates=(1000, 10000, 100000), seconds=1.5, seed=11):
+    """8 resident trees of 4^3 metacells (2^12 .. 2^23 points) from Gaussian-blob
+    volumes; Poisson arrivals; 90% isovalue queries (iso, iso) with iso ~ U[0,1] and
+    10% 3-sided range queries [a, a + w], w ~ U[0, 0.1], min2 = a; results copied to
+    host memory.  Latency runs from the scheduled arrival to the result in host
+    memory (open loop)."""
+    trees = []
+    for i, (px, py, pz) in enumerate(SERVING_VOLUMES):
+        vol = blob_volume_device(px, py, pz, seed + i, torch)
+        mc, n = pst.formMetacellTags(vol.reshape(-1), (px, py, pz), (4, 4, 4), "f32", True)
+        trees.append(pst.StaticPSTGPU(mc, n, "f32", True))
+        del vol, mc
+    torch.cuda.empty_cache()
+    srv = pst.Server(max_batch=1024, slots_per_tree=2, out_budget_bytes=2 << 30, keep_results=2)
+    idx = [srv.add_tree(t) for t in trees]
+    rng = np.random.default_rng(seed)
+    out = {"trees_points": [t.n for t in trees]}
+    for rate in rates:
+        n = int(rate * seconds)
+        gaps = rng.exponential(1.0 / rate, n)
+        tree_of = rng.integers(0, len(trees), n).astype(np.uint32)
+        three = rng.random(n) < 0.1
+        a = rng.uniform(0, 1, n).astype(np.float32)
+        w = rng.uniform(0, 0.1, n).astype(np.float32)
+        kinds = np.where(three, 0, 1).astype(np.int32)
+        q = pst.make_queries(kinds, np.where(three, a, 0), np.where(three, a + w, a), a, "f32")
+        srv.reset_stats()
+        t0 = time.monotonic_ns() + 2_000_000
+        arrive = t0 + np.cumsum(gaps * 1e9).astype(np.uint64)
+        k = 0
+        while k < n:
+            now = time.monotonic_ns()
+            j = int(np.searchsorted(arrive, now, side="right"))
+            if j > k:
+                srv.submit(tree_of[k:j], q[k:j], arrival_ns=arrive[k:j])
+                k = j
+            else:
+                time.sleep(20e-6)
+        srv.drain(120000)
+        st = srv.stats()
+        out[f"{rate}qps"] = {"p50_ms": st["p50_ms"], "p90_ms": st["p90_ms"], "p99_ms": st["p99_ms"],
+                             "mean_ms": st["mean_ms"], "completed": st["completed"], "failed": st["failed"],
+                             "batches": st["batches"], "points": st["points"],
+                             "throughput_qps": st["completed"] / st["busy_s"] if st["busy_s"] else None}
+    srv.close()
+    for t in trees:
+        t.close()
+    return out
+
+
 # ---------------------------------------------------------------------------
 # clocks
 
@@ -160,7 +236,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -294,11 +370,12 @@ def run_reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200")
     ap.add_argument("--points-log2", type=int, default=28)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--plain-queries", type=int, default=256)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -323,7 +400,9 @@ def main():
     pts_d = gen_points_device(n, seed=1 + rank, torch=torch)
     torch.cuda.synchronize()
     c0 = time.perf_counter()
+    torch.cuda.nvtx.range_push("construct")
     tree = pst.StaticPSTGPU(pts_d, n, "f32", True)
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     construct_ms = 1000 * (time.perf_counter() - c0)
     log(f"constructed 2^{args.points_log2} points in {construct_ms:.1f} ms")
@@ -347,6 +426,9 @@ def main():
     offs = torch.empty(NQ + 1, dtype=torch.int64, device="cuda")
     st, tot = eng.run(q_dev, out, offs, queries_on_device=True, sync=True)
     assert st == 0 and tot == total
+    frontier = eng.last_stats()
+    log(f"frontier: {frontier['records']} alive records ({total / max(frontier['records'], 1):.1f} points each), "
+        f"{frontier['seeds']} seeds, {frontier['boundary']} boundary nodes; per level {frontier['per_level']}")
 
     # ---- device-resident timing (value)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
@@ -427,6 +509,15 @@ def main():
         except Exception:
             pass
 
+    serving = None
+    if rank == 0 and not args.no_serving:
+        try:
+            serving = serving_bench(pst, torch)
+            log("serving: " + ", ".join(f"{k} p50 {v['p50_ms']:.2f} p99 {v['p99_ms']:.2f} ms"
+                                        for k, v in serving.items() if k.endswith("qps")))
+        except Exception as e:
+            serving = {"error": str(e)}
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         try:
@@ -448,11 +539,13 @@ def main():
                            "selectivity": [SEL_LO, SEL_HI], "results": "ids",
                            "l2": "inputs larger than L2 (tree ~9 GB)", "parallelism": f"{world} independent shards"},
                 "queries_per_s": qps, "points_per_step": total,
+                "frontier": {k: frontier[k] for k in ("records", "seeds", "boundary")},
                 "plain_queries_per_s": plain_qps, "batched_vs_plain_qps": qps / world / plain_qps,
                 "construct_ms": construct_ms, "construct_pts_per_s": n / (construct_ms / 1000.0),
                 "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(q_host.nbytes),
                         "d2h_bytes_per_step": int(total * 4 + (NQ + 1) * 8)},
-                "gpu_launches": None, "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary()}
+                "gpu_launches": None, "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
+                "serving": serving}
         levels = tree.info()["levels"]
         line["gpu_launches"] = (levels + 6) * args.steps  # unpack+check + levels + 3 scan + emit per step
         print(json.dumps(line))

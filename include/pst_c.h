@@ -194,6 +194,16 @@ pst_status pst_batch_count(pst_batch *batch, const pst_query *queries, uint32_t 
 /* After an asynchronous run: PST_OK, PST_ERR_CAPACITY or PST_ERR_INTERNAL. */
 pst_status pst_batch_status(pst_batch *batch, uint64_t *total);
 
+/* Frontier statistics of the last synchronised pass (for profiling and byte
+ * accounting): alive 32-slot chunk records over all levels, report-above seeds,
+ * reported boundary nodes, points reported, and the records per level (up to 40
+ * entries written to per_level when it is non-null). */
+typedef struct pst_batch_stats {
+	uint64_t records, seeds, boundary, points;
+	uint32_t levels;
+} pst_batch_stats;
+pst_status pst_batch_last_stats(pst_batch *batch, pst_batch_stats *stats, uint32_t *per_level);
+
 /* ------------------------------------------------------------------------- */
 /* Serving: a request loop over several resident trees with continuous batching.
  * Requests that arrive while other batches are on the device join the next free

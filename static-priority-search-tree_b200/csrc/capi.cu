@@ -451,6 +451,26 @@ pst_status pst_batch_status(pst_batch *batch, uint64_t *total)
 	return st != PST_OK ? st : result;
 }
 
+pst_status pst_batch_last_stats(pst_batch *batch, pst_batch_stats *stats, uint32_t *per_level)
+{
+	return guarded([&] {
+		if (!batch || !stats)
+			fail(PST_ERR_INVALID, "null argument");
+		const BatchCtl &c = batch->b.last;
+		pst_batch_stats st{};
+		st.levels = batch->b.tree->levels;
+		for (uint32_t d = 0; d < 40; d++) {
+			st.records += c.lvl_cnt[d];
+			st.seeds += c.seed_cnt[d];
+			if (per_level)
+				per_level[d] = c.lvl_cnt[d];
+		}
+		st.boundary = c.rec_cnt;
+		st.points = c.total;
+		*stats = st;
+	});
+}
+
 static uint64_t ips_common(pst_dtype dtype, pst_idtype idtype, const void *pts_d, uint64_t n, pst_value v, pst_ret ret,
                            void *out, uint64_t cap, uint32_t blocks, cudaStream_t s)
 {

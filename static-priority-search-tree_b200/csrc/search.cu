@@ -4,18 +4,20 @@
 // The reference walks the tree with one thread block per query, handing subtrees
 // to idle threads through shared memory and to child grids when none are idle
 // (pst/static-pst-gpu-search-functions.tu:12-722, pst/static-pst-gpu.tu:819-1148).
-// Here every query of a batch advances one tree level per kernel:
+// Here every query of a batch advances one tree level per kernel (k_bfs_level):
 //   - "path" tasks follow the O(log n) boundary nodes of a query with the
 //     reference's delegation rules (do3SidedSearchDelegation, doLeftSearchDelegation,
 //     doRightSearchDelegation: pst/static-pst-cpu-iter.tpp:602-714);
-//   - every subtree the reference would "report above" becomes chunk tasks.  In a
-//     max-heap on dim2 a node is reported exactly when its own dim2 passes
-//     (its ancestors' dim2 are at least as large), so a chunk task is just the
-//     32 consecutive slots of one level, tested by one warp with one coalesced
-//     load; the survivors' 32 children fill two chunks of the next level.
-// Chunk tasks record their survivor masks.  A count of every query falls out of
-// the pass; an exclusive scan gives each query's exact output offset and a flat
-// emit kernel writes ids (or points) from the recorded masks.
+//   - every subtree the reference would "report above" is scanned by level.  In a
+//     max-heap on dim2 a node of such a subtree is reported exactly when its own
+//     dim2 passes (its ancestors' dim2 are at least as large), so the work unit is a
+//     chunk: 32 consecutive slots of one level, tested by one warp with one coalesced
+//     load.  The frontier is kept as "alive records" only — (chunk, query, mask of
+//     reported slots) — and the next level expands each record into its two child
+//     chunks (spread16), masked by occupancy before anything is loaded.
+// A count of every query falls out of the pass; an exclusive scan gives each
+// query's exact output offset, and a flat emit kernel writes ids (or points) from
+// the alive records.
 #include <algorithm>
 #include <mutex>
 #include <string>
@@ -29,8 +31,9 @@ namespace pst {
 
 namespace {
 
-constexpr uint32_t TASK_RECORD = 1u;  // task holds an already-tested result (no expansion)
 constexpr uint32_t MODE_THREE = 3, MODE_LEFT = 1, MODE_RIGHT = 2;
+constexpr uint32_t FULL = 0xFFFFFFFFu;
+constexpr int LOADS_IN_FLIGHT = 8;  // chunk tests (or emit rows) batched per warp before their results are used
 
 __device__ __forceinline__ bool occ_bit(const uint32_t *occ, uint32_t h) { return (occ[h >> 5] >> (h & 31)) & 1u; }
 
@@ -43,35 +46,23 @@ struct QDev {
 };
 
 struct WorkDev {
-	uint4 *tasks;
-	uint32_t *amask;
-	uint64_t task_cap;
-	uint4 *path0;
-	uint4 *path1;
-	uint32_t path_cap;
+	uint2 *rec_pq;      // alive records: (chunk base position, query)
+	uint32_t *rec_am;   // ... and their masks of reported slots
+	uint64_t rec_cap;
+	uint4 *path0, *path1;  // boundary-path tasks (position, query, mode), double-buffered by level parity
+	uint4 *seed0, *seed1;  // report-above seeds (chunk base, query, candidate mask), idem
+	uint32_t path_cap;     // entries of each path / seed buffer (2 per query)
+	uint2 *ro_pq;          // reported boundary nodes: (chunk base, query) ...
+	uint32_t *ro_bit;      // ... and the node's bit (never expanded)
+	uint32_t ro_cap;
 	uint64_t *counts;
 	uint64_t *cursor;
 	const uint64_t *offsets;
 	BatchCtl *ctl;
 };
 
-// Appends k consecutive task slots to the region of level `lvl`; returns the first
-// slot index or ~0 when the buffer is full (the overflow is recorded).
-__device__ __forceinline__ uint64_t reserve_tasks(const WorkDev &w, uint64_t region_base, uint32_t lvl, uint32_t k)
-{
-	const uint32_t off = atomicAdd(&w.ctl->lvl_cnt[lvl], k);
-	const uint64_t slot = region_base + off;
-	if (slot + k > w.task_cap) {
-		atomicMax((unsigned long long *) &w.ctl->need_tasks, (unsigned long long) (slot + k));
-		atomicOr(&w.ctl->flags, BATCH_FLAG_TASK_OVERFLOW);
-		return ~0ull;
-	}
-	return slot;
-}
-
 template <typename T>
-__device__ void path_step(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev &w, uint32_t d, uint64_t base_next,
-                          uint4 task)
+__device__ void path_step(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev &w, uint32_t d, uint4 task)
 {
 	const uint32_t h = task.x, q = task.y, mode = task.z;
 	const T min2 = qd.min2[q];
@@ -83,10 +74,12 @@ __device__ void path_step(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev 
 	const T v1 = t.dim1[h];
 	const bool rep = kind == PST_Q_THREE ? (min1 <= v1 && v1 <= max1) : kind == PST_Q_LEFT ? (v1 <= max1) : (v1 >= min1);
 	if (rep) {
-		const uint64_t slot = reserve_tasks(w, base_next, d + 1, 1);
-		if (slot != ~0ull) {
-			w.tasks[slot] = make_uint4(h & ~31u, q, 1u << (h & 31), TASK_RECORD);
-			w.amask[slot] = 1u << (h & 31);
+		const uint32_t i = atomicAdd(&w.ctl->rec_cnt, 1u);
+		if (i < w.ro_cap) {
+			w.ro_pq[i] = make_uint2(h & ~31u, q);
+			w.ro_bit[i] = 1u << (h & 31);
+		} else {
+			atomicOr(&w.ctl->flags, BATCH_FLAG_INTERNAL);
 		}
 		atomicAdd((unsigned long long *) &w.counts[q], 1ull);
 	}
@@ -97,7 +90,7 @@ __device__ void path_step(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev 
 	if (!hl && !hr)
 		return;
 	const T m = t.med[h];
-	uint32_t pl = 0, pr = 0;  // continue as path task with this mode (0 = no)
+	uint32_t pl = 0, pr = 0;      // continue as a path task with this mode (0 = no)
 	bool rl = false, rr = false;  // report-above subtree
 	if (mode == MODE_THREE) {
 		if (min1 <= m && m <= max1) {
@@ -123,8 +116,9 @@ __device__ void path_step(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev 
 			pr = MODE_RIGHT;
 		}
 	}
+	// at most two boundary paths per query and level, each leaving at most one seed,
+	// so path_cap = 2 * max_q holds every list
 	uint4 *pout = ((d + 1) & 1) ? w.path1 : w.path0;
-	// at most two boundary paths per query and level, so path_cap = 2 * max_q holds them
 	if (pl) {
 		const uint32_t i = atomicAdd(&w.ctl->path_cnt[d + 1], 1u);
 		if (i < w.path_cap)
@@ -140,96 +134,170 @@ __device__ void path_step(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev 
 			atomicOr(&w.ctl->flags, BATCH_FLAG_INTERNAL);
 	}
 	if (rl || rr) {
-		// l and r share a chunk; both seeds fit one task
+		// l and r share a chunk
 		const uint32_t bits = (rl ? 1u << (l & 31) : 0u) | (rr ? 1u << (r & 31) : 0u);
-		const uint64_t slot = reserve_tasks(w, base_next, d + 1, 1);
-		if (slot != ~0ull)
-			w.tasks[slot] = make_uint4(l & ~31u, q, bits, 0u);
+		uint4 *sout = ((d + 1) & 1) ? w.seed1 : w.seed0;
+		const uint32_t i = atomicAdd(&w.ctl->seed_cnt[d + 1], 1u);
+		if (i < w.path_cap)
+			sout[i] = make_uint4(l & ~31u, q, bits, 0u);
+		else
+			atomicOr(&w.ctl->flags, BATCH_FLAG_INTERNAL);
+	}
+}
+
+// Tests the 32*K chunk tasks held by a warp (lane l owns tasks (l, 0..K-1): chunk
+// base p[k], candidate lanes cand[k], the query's min2) and returns each task's
+// mask of reported slots in am[k].  LOADS_IN_FLIGHT masked row loads are issued
+// before their ballots.
+template <typename T, int K>
+__device__ __forceinline__ void test_chunks(const T *__restrict__ dim2, const uint32_t (&p)[K],
+                                            const uint32_t (&cand)[K], T m2, uint32_t (&am)[K])
+{
+	const uint32_t lane = lane_id();
+	uint32_t any = 0;
+#pragma unroll
+	for (int k = 0; k < K; k++) {
+		am[k] = 0;
+		any |= cand[k];
+	}
+	const uint32_t busy = __ballot_sync(FULL, any != 0);
+	if (!busy)
+		return;
+#pragma unroll
+	for (int g = 0; g < 32 * K; g += LOADS_IN_FLIGHT) {
+		// skip a group whose owning lanes have nothing to test
+		const uint32_t owners = ((1u << (LOADS_IN_FLIGHT / K)) - 1u) << (g / K);
+		if (!(busy & owners))
+			continue;
+		T v[LOADS_IN_FLIGHT], mm[LOADS_IN_FLIGHT];
+		bool ld[LOADS_IN_FLIGHT];
+#pragma unroll
+		for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
+			const int src = (g + u) / K, k = (g + u) % K;
+			const uint32_t c = __shfl_sync(FULL, cand[k], src);
+			const uint32_t pp = __shfl_sync(FULL, p[k], src);
+			mm[u] = __shfl_sync(FULL, m2, src);
+			ld[u] = (c >> lane) & 1u;
+			v[u] = ld[u] ? dim2[pp + lane] : T(0);
+		}
+#pragma unroll
+		for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
+			const int src = (g + u) / K, k = (g + u) % K;
+			const uint32_t a = __ballot_sync(FULL, ld[u] && (mm[u] <= v[u]));
+			if (lane == (uint32_t) src)
+				am[k] = a;
+		}
+	}
+}
+
+// Appends the warp's non-empty masks as alive records of level `lvl` (one atomic
+// per warp) and adds their sizes to the queries' counts (one atomic per run of
+// equal query ids).
+template <int K>
+__device__ __forceinline__ void append_records(const WorkDev &w, uint32_t lvl, uint64_t region_base,
+                                               const uint32_t (&p)[K], const uint32_t (&am)[K], uint32_t q,
+                                               bool valid)
+{
+	const uint32_t lane = lane_id();
+	uint32_t nrec = 0, pts = 0;
+#pragma unroll
+	for (int k = 0; k < K; k++) {
+		nrec += am[k] ? 1u : 0u;
+		pts += __popc(am[k]);
+	}
+	bool last;
+	const uint64_t run = warp_run_sum(valid ? q : 0xFFFFFFFFu, pts, &last);
+	if (valid && last && run)
+		atomicAdd((unsigned long long *) &w.counts[q], (unsigned long long) run);
+	const uint32_t inc = warp_incl_scan(nrec);
+	const uint32_t tot = __shfl_sync(FULL, inc, 31);
+	if (!tot)
+		return;
+	uint64_t slot0 = 0;
+	if (lane == 31) {
+		const uint32_t off = atomicAdd(&w.ctl->lvl_cnt[lvl], tot);
+		slot0 = region_base + off;
+		if (slot0 + tot > w.rec_cap) {
+			atomicMax((unsigned long long *) &w.ctl->need_tasks, (unsigned long long) (slot0 + tot));
+			atomicOr(&w.ctl->flags, BATCH_FLAG_TASK_OVERFLOW);
+			slot0 = ~0ull;
+		}
+	}
+	slot0 = __shfl_sync(FULL, slot0, 31);
+	if (slot0 == ~0ull)
+		return;
+	uint64_t s = slot0 + inc - nrec;
+#pragma unroll
+	for (int k = 0; k < K; k++) {
+		if (am[k]) {
+			w.rec_pq[s] = make_uint2(p[k], q);
+			w.rec_am[s] = am[k];
+			s++;
+		}
 	}
 }
 
 template <typename T>
 __global__ void __launch_bounds__(BFS_THREADS) k_bfs_level(TreeDev<T> t, QDev<T> qd, WorkDev w, uint32_t d)
 {
+	// Once the frontier has overflowed, the reservation that crossed the capacity
+	// left some slots below it unwritten, so nothing of the previous level may be
+	// read: the pass stops here and the host repeats it with a larger buffer.
+	if (w.ctl->flags & BATCH_FLAG_TASK_OVERFLOW)
+		return;
 	__shared__ uint64_t s_base[2];
 	if (threadIdx.x == 0) {
-		uint64_t b = 0;
-		for (uint32_t e = 0; e < d; e++)
+		uint64_t b = 0;  // start of the previous level's records
+		for (uint32_t e = 0; e + 1 < d; e++)
 			b += w.ctl->lvl_cnt[e];
 		s_base[0] = b;
-		s_base[1] = b + w.ctl->lvl_cnt[d];
+		s_base[1] = b + (d ? w.ctl->lvl_cnt[d - 1] : 0u);
 	}
 	__syncthreads();
-	const uint64_t base_d = s_base[0], base_next = s_base[1];
+	const uint64_t base_prev = s_base[0], base_cur = s_base[1];
 	// after a frontier overflow the counters run past what was stored: never read beyond it
-	const uint64_t n_d = base_next <= w.task_cap ? base_next - base_d : (base_d < w.task_cap ? w.task_cap - base_d : 0);
+	const uint64_t end_prev = min(base_cur, w.rec_cap);
+	const uint64_t n_prev = end_prev > base_prev ? end_prev - base_prev : 0;
 	const uint64_t gthreads = (uint64_t) gridDim.x * blockDim.x;
 	const uint64_t gtid = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
-	const bool more = d + 1 < t.levels;
+	const uint64_t gwarps = gthreads / 32, gwarp = gtid / 32;
+	const uint32_t lane = lane_id();
+	const T *__restrict__ dim2 = t.dim2;
 
 	// boundary paths
 	const uint32_t np = min(w.ctl->path_cnt[d], w.path_cap);
 	const uint4 *pin = (d & 1) ? w.path1 : w.path0;
 	for (uint64_t i = gtid; i < np; i += gthreads)
-		path_step<T>(t, qd, w, d, base_next, pin[i]);
+		path_step<T>(t, qd, w, d, pin[i]);
 	__syncwarp();
 
-	// report-above chunks, 32 tasks per warp iteration
-	const uint32_t lane = lane_id();
-	const uint64_t gwarps = gthreads / 32, gwarp = gtid / 32;
-	for (uint64_t wb = gwarp * 32; wb < n_d; wb += gwarps * 32) {
-		const uint64_t idx = base_d + wb + lane;
-		const bool valid = wb + lane < n_d;
-		uint4 tk = valid ? w.tasks[idx] : make_uint4(0, 0, 0, TASK_RECORD);
-		const bool rec = tk.w & TASK_RECORD;
-		uint32_t cand = (!rec) ? (tk.z & t.occ[tk.x >> 5]) : 0u;
-		const T m2 = cand ? qd.min2[tk.y] : T(0);
-		uint32_t my_am = 0;
-#pragma unroll
-		for (int g = 0; g < 32; g += 4) {
-			T v[4];
-			bool ld[4];
-			T mm[4];
-#pragma unroll
-			for (int u = 0; u < 4; u++) {
-				const uint32_t c = __shfl_sync(0xFFFFFFFFu, cand, g + u);
-				const uint32_t p = __shfl_sync(0xFFFFFFFFu, tk.x, g + u);
-				mm[u] = __shfl_sync(0xFFFFFFFFu, m2, g + u);
-				ld[u] = (c >> lane) & 1u;
-				v[u] = ld[u] ? t.dim2[p + lane] : T(0);
-			}
-#pragma unroll
-			for (int u = 0; u < 4; u++) {
-				const uint32_t am = __ballot_sync(0xFFFFFFFFu, ld[u] && (mm[u] <= v[u]));
-				if (lane == (uint32_t) (g + u))
-					my_am = am;
-			}
-		}
-		if (valid && !rec)
-			w.amask[idx] = my_am;
-		// per-query counts: one atomic per run of equal query ids
-		bool last;
-		const uint64_t run = warp_run_sum(tk.y, (uint64_t) __popc(my_am), &last);
-		if (last && run)
-			atomicAdd((unsigned long long *) &w.counts[tk.y], (unsigned long long) run);
-		if (more) {
-			const uint32_t lo = spread16(my_am), hi = spread16(my_am >> 16);
-			const uint32_t nc = (lo ? 1u : 0u) + (hi ? 1u : 0u);
-			const uint32_t inc = warp_incl_scan(nc);
-			const uint32_t tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
-			uint64_t slot0 = 0;
-			if (lane == 31 && tot)
-				slot0 = reserve_tasks(w, base_next, d + 1, tot);
-			slot0 = __shfl_sync(0xFFFFFFFFu, slot0, 31);
-			if (tot && slot0 != ~0ull) {
-				uint64_t s = slot0 + inc - nc;
-				const uint32_t p2 = 2 * tk.x;
-				if (lo)
-					w.tasks[s++] = make_uint4(p2, tk.y, lo, 0u);
-				if (hi)
-					w.tasks[s] = make_uint4(p2 + 32, tk.y, hi, 0u);
-			}
-		}
+	// report-above seeds of this level (one chunk task each)
+	const uint32_t ns = min(w.ctl->seed_cnt[d], w.path_cap);
+	const uint4 *sin = (d & 1) ? w.seed1 : w.seed0;
+	for (uint64_t wb = gwarp * 32; wb < ns; wb += gwarps * 32) {
+		const bool valid = wb + lane < ns;
+		const uint4 sd = valid ? sin[wb + lane] : make_uint4(0, 0, 0, 0);
+		const uint32_t p[1] = {sd.x};
+		const uint32_t cand[1] = {valid ? (sd.z & t.occ[sd.x >> 5]) : 0u};
+		const T m2 = cand[0] ? qd.min2[sd.y] : T(0);
+		uint32_t am[1];
+		test_chunks<T, 1>(dim2, p, cand, m2, am);
+		append_records<1>(w, d, base_cur, p, am, sd.y, valid);
+	}
+
+	// expansion of the previous level's alive records into their two child chunks
+	for (uint64_t wb = gwarp * 32; wb < n_prev; wb += gwarps * 32) {
+		const bool valid = wb + lane < n_prev;
+		const uint64_t idx = base_prev + wb + lane;
+		const uint2 pq = valid ? w.rec_pq[idx] : make_uint2(0, 0);
+		const uint32_t pam = valid ? w.rec_am[idx] : 0u;
+		const uint32_t lo = spread16(pam), hi = spread16(pam >> 16);
+		const uint32_t p[2] = {2 * pq.x, 2 * pq.x + 32};
+		const uint32_t cand[2] = {lo ? (lo & t.occ[p[0] >> 5]) : 0u, hi ? (hi & t.occ[p[1] >> 5]) : 0u};
+		const T m2 = (cand[0] | cand[1]) ? qd.min2[pq.y] : T(0);
+		uint32_t am[2];
+		test_chunks<T, 2>(dim2, p, cand, m2, am);
+		append_records<2>(w, d, base_cur, p, am, pq.y, valid);
 	}
 }
 
@@ -270,14 +338,84 @@ __global__ void k_check_kinds(const pst_query *raw, BatchCtl *ctl)
 	}
 }
 
+// Writes the results of up to 32 records (lane r owns record (p, am) whose results
+// start at out_base) in batches of LOADS_IN_FLIGHT rows: loads first, then stores.
+template <typename T, bool HAS_ID, bool POINTS>
+__device__ __forceinline__ void emit_rows(const TreeDev<T> &t, uint32_t p, uint32_t am, uint64_t out_base,
+                                          void *__restrict__ out, uint64_t capacity)
+{
+	using Pt = Point<T, HAS_ID>;
+	const uint32_t lane = lane_id();
+	const uint32_t busy = __ballot_sync(FULL, am != 0);
+	const uint32_t *__restrict__ ids = t.id;
+	const T *__restrict__ d1 = t.dim1;
+	const T *__restrict__ d2 = t.dim2;
+#pragma unroll
+	for (int g = 0; g < 32; g += LOADS_IN_FLIGHT) {
+		if (!(busy & (((1u << LOADS_IN_FLIGHT) - 1u) << g)))
+			continue;
+		uint32_t a[LOADS_IN_FLIGHT];
+		uint64_t ob[LOADS_IN_FLIGHT];
+		uint32_t vid[LOADS_IN_FLIGHT];
+		T v1[LOADS_IN_FLIGHT], v2[LOADS_IN_FLIGHT];
+#pragma unroll
+		for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
+			a[u] = __shfl_sync(FULL, am, g + u);
+			const uint32_t pp = __shfl_sync(FULL, p, g + u);
+			ob[u] = __shfl_sync(FULL, out_base, g + u);
+			const bool on = (a[u] >> lane) & 1u;
+			const uint32_t h = pp + lane;
+			if constexpr (HAS_ID)
+				vid[u] = on ? ids[h] : 0u;
+			if constexpr (POINTS) {
+				v1[u] = on ? d1[h] : T(0);
+				v2[u] = on ? d2[h] : T(0);
+			}
+		}
+#pragma unroll
+		for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
+			if (!((a[u] >> lane) & 1u))
+				continue;
+			const uint64_t o = ob[u] + __popc(a[u] & lanemask_lt());
+			if (o >= capacity)
+				continue;
+			if constexpr (POINTS) {
+				Pt rec;
+				rec.dim1 = v1[u];
+				rec.dim2 = v2[u];
+				if constexpr (HAS_ID)
+					rec.id = vid[u];
+				static_cast<Pt *>(out)[o] = rec;
+			} else {
+				static_cast<uint32_t *>(out)[o] = vid[u];
+			}
+		}
+	}
+}
+
+// Output slot of this lane's record inside its query's result: one atomic per run
+// of equal query ids on the query's cursor.
+__device__ __forceinline__ uint64_t claim_output(const WorkDev &w, uint32_t q, uint32_t am, bool valid)
+{
+	const uint32_t pc = __popc(am);
+	bool last;
+	const uint64_t run = warp_run_sum(valid ? q : 0xFFFFFFFFu, pc, &last);
+	const uint32_t lastmask = __ballot_sync(FULL, last);
+	const uint32_t run_last = (uint32_t) (__ffs(lastmask & (FULL << lane_id())) - 1);
+	uint64_t rb = 0;
+	if (valid && last && run)
+		rb = atomicAdd((unsigned long long *) &w.cursor[q], (unsigned long long) run);
+	rb = __shfl_sync(FULL, rb, run_last);
+	return (valid && am) ? w.offsets[q] + rb + run - pc : 0;
+}
+
 template <typename T, bool HAS_ID, bool POINTS>
 __global__ void __launch_bounds__(BFS_THREADS) k_emit(TreeDev<T> t, WorkDev w, void *out, uint64_t capacity)
 {
-	using Pt = Point<T, HAS_ID>;
 	__shared__ uint64_t s_total;
 	if (threadIdx.x == 0) {
 		uint64_t b = 0;
-		for (uint32_t e = 0; e <= t.levels; e++)
+		for (uint32_t e = 0; e < t.levels; e++)
 			b += w.ctl->lvl_cnt[e];
 		s_total = b;
 	}
@@ -287,49 +425,26 @@ __global__ void __launch_bounds__(BFS_THREADS) k_emit(TreeDev<T> t, WorkDev w, v
 			atomicOr(&w.ctl->flags, BATCH_FLAG_OUT_OVERFLOW);
 		return;
 	}
-	const uint64_t total = s_total < w.task_cap ? s_total : w.task_cap;
+	const uint64_t total = s_total < w.rec_cap ? s_total : w.rec_cap;
+	const uint32_t nro = min(w.ctl->rec_cnt, w.ro_cap);
 	const uint32_t lane = lane_id();
 	const uint64_t gtid = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	const uint64_t gwarps = (uint64_t) gridDim.x * blockDim.x / 32, gwarp = gtid / 32;
 	for (uint64_t wb = gwarp * 32; wb < total; wb += gwarps * 32) {
 		const uint64_t idx = wb + lane;
 		const bool valid = idx < total;
-		const uint32_t am = valid ? w.amask[idx] : 0u;
-		const uint4 tk = valid ? w.tasks[idx] : make_uint4(0, 0, 0, 0);
-		const uint32_t pc = __popc(am);
-		bool last;
-		const uint64_t run = warp_run_sum(tk.y, pc, &last);
-		// first slot of this lane's results inside its query's output
-		const uint32_t lastmask = __ballot_sync(0xFFFFFFFFu, last);
-		const uint32_t run_last = (uint32_t) (__ffs(lastmask & (0xFFFFFFFFu << lane)) - 1);
-		uint64_t rb = 0;
-		if (last && run)
-			rb = atomicAdd((unsigned long long *) &w.cursor[tk.y], (unsigned long long) run);
-		rb = __shfl_sync(0xFFFFFFFFu, rb, run_last);
-		const uint64_t my_base = am ? w.offsets[tk.y] + rb + run - pc : 0;
-		for (uint32_t tt = 0; tt < 32; tt++) {
-			const uint32_t a = __shfl_sync(0xFFFFFFFFu, am, tt);
-			if (!a)
-				continue;
-			const uint32_t p = __shfl_sync(0xFFFFFFFFu, tk.x, tt);
-			const uint64_t ob = __shfl_sync(0xFFFFFFFFu, my_base, tt);
-			if ((a >> lane) & 1u) {
-				const uint32_t h = p + lane;
-				const uint64_t o = ob + __popc(a & lanemask_lt());
-				if (o >= capacity)
-					continue;
-				if constexpr (POINTS) {
-					Pt rec;
-					rec.dim1 = t.dim1[h];
-					rec.dim2 = t.dim2[h];
-					if constexpr (HAS_ID)
-						rec.id = t.id[h];
-					static_cast<Pt *>(out)[o] = rec;
-				} else {
-					static_cast<uint32_t *>(out)[o] = t.id[h];
-				}
-			}
-		}
+		const uint2 pq = valid ? w.rec_pq[idx] : make_uint2(0, 0);
+		const uint32_t am = valid ? w.rec_am[idx] : 0u;
+		const uint64_t ob = claim_output(w, pq.y, am, valid);
+		emit_rows<T, HAS_ID, POINTS>(t, pq.x, am, ob, out, capacity);
+	}
+	for (uint64_t wb = gwarp * 32; wb < nro; wb += gwarps * 32) {
+		const uint64_t idx = wb + lane;
+		const bool valid = idx < nro;
+		const uint2 pq = valid ? w.ro_pq[idx] : make_uint2(0, 0);
+		const uint32_t am = valid ? w.ro_bit[idx] : 0u;
+		const uint64_t ob = claim_output(w, pq.y, am, valid);
+		emit_rows<T, HAS_ID, POINTS>(t, pq.x, am, ob, out, capacity);
 	}
 }
 
@@ -351,8 +466,9 @@ void Batch::release()
 	if (graph_exec)
 		cudaGraphExecDestroy(graph_exec);
 	graph_exec = nullptr;
-	for (void *p : {(void *) q_raw, (void *) kind, min1, max1, min2, (void *) path0, (void *) path1, (void *) counts,
-	                (void *) cursor, (void *) offsets, (void *) scan_tmp, (void *) ctl, (void *) tasks, (void *) amask})
+	for (void *p : {(void *) q_raw, (void *) kind, min1, max1, min2, (void *) path0, (void *) path1, (void *) seed0,
+	                (void *) seed1, (void *) ro_pq, (void *) ro_bit, (void *) counts, (void *) cursor, (void *) offsets,
+	                (void *) scan_tmp, (void *) ctl, (void *) rec_pq, (void *) rec_am})
 		if (p)
 			cudaFree(p);
 	if (ctl_host)
@@ -362,6 +478,8 @@ void Batch::release()
 	q_raw = nullptr;
 	ctl_host = nullptr;
 	q_stage = nullptr;
+	rec_pq = nullptr;
+	rec_am = nullptr;
 }
 
 static void dmalloc(void **p, size_t bytes)
@@ -394,13 +512,19 @@ void Batch::init(TreeStorage *t, const pst_batch_opts &o)
 	                                : (uint32_t) std::max(occ, 1);
 	grid = (uint32_t) device_info().sms * blocks_per_sm;
 	const size_t vs = value_size(t->dtype);
+	path_cap = 2 * max_q;
+	ro_cap = 2 * max_q * 32;
 	dmalloc((void **) &q_raw, (size_t) max_q * sizeof(pst_query));
 	dmalloc((void **) &kind, (size_t) max_q * 4);
 	dmalloc(&min1, (size_t) max_q * vs);
 	dmalloc(&max1, (size_t) max_q * vs);
 	dmalloc(&min2, (size_t) max_q * vs);
-	dmalloc((void **) &path0, (size_t) max_q * 2 * sizeof(uint4));
-	dmalloc((void **) &path1, (size_t) max_q * 2 * sizeof(uint4));
+	dmalloc((void **) &path0, (size_t) path_cap * sizeof(uint4));
+	dmalloc((void **) &path1, (size_t) path_cap * sizeof(uint4));
+	dmalloc((void **) &seed0, (size_t) path_cap * sizeof(uint4));
+	dmalloc((void **) &seed1, (size_t) path_cap * sizeof(uint4));
+	dmalloc((void **) &ro_pq, (size_t) ro_cap * sizeof(uint2));
+	dmalloc((void **) &ro_bit, (size_t) ro_cap * 4);
 	dmalloc((void **) &counts, (size_t) max_q * 8);
 	dmalloc((void **) &cursor, (size_t) max_q * 8);
 	dmalloc((void **) &offsets, ((size_t) max_q + 1) * 8);
@@ -415,14 +539,14 @@ void Batch::init(TreeStorage *t, const pst_batch_opts &o)
 
 void Batch::grow_tasks(uint64_t cap)
 {
-	if (tasks)
-		cudaFree(tasks);
-	if (amask)
-		cudaFree(amask);
-	tasks = nullptr;
-	amask = nullptr;
-	dmalloc((void **) &tasks, cap * sizeof(uint4));
-	dmalloc((void **) &amask, cap * 4);
+	if (rec_pq)
+		cudaFree(rec_pq);
+	if (rec_am)
+		cudaFree(rec_am);
+	rec_pq = nullptr;
+	rec_am = nullptr;
+	dmalloc((void **) &rec_pq, cap * sizeof(uint2));
+	dmalloc((void **) &rec_am, cap * 4);
 	task_cap = cap;
 	if (graph_exec) {
 		cudaGraphExecDestroy(graph_exec);
@@ -430,12 +554,16 @@ void Batch::grow_tasks(uint64_t cap)
 	}
 }
 
+#define PST_WORKDEV                                                                                                   \
+	WorkDev w{rec_pq, rec_am, task_cap, path0, path1, seed0, seed1, path_cap, ro_pq, ro_bit, ro_cap, counts, cursor, \
+	          offsets, ctl}
+
 template <typename T>
 void Batch::enqueue_count(cudaStream_t s)
 {
 	TreeDev<T> tv = tree->view<T>();
 	QDev<T> qd{kind, static_cast<const T *>(min1), static_cast<const T *>(max1), static_cast<const T *>(min2)};
-	WorkDev w{tasks, amask, task_cap, path0, path1, 2 * max_q, counts, cursor, offsets, ctl};
+	PST_WORKDEV;
 	PST_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
 	PST_CUDA(cudaMemsetAsync(counts, 0, (size_t) max_q * 8, s));
 	PST_CUDA(cudaMemsetAsync(cursor, 0, (size_t) max_q * 8, s));
@@ -454,7 +582,7 @@ template <typename T, bool HAS_ID, bool POINTS>
 void Batch::enqueue_emit_t(void *out, uint64_t capacity, cudaStream_t s)
 {
 	TreeDev<T> tv = tree->view<T>();
-	WorkDev w{tasks, amask, task_cap, path0, path1, 2 * max_q, counts, cursor, offsets, ctl};
+	PST_WORKDEV;
 	k_emit<T, HAS_ID, POINTS><<<grid, threads, 0, s>>>(tv, w, out, capacity);
 	PST_CUDA(cudaGetLastError());
 }
@@ -614,20 +742,28 @@ constexpr size_t NA_MAX1 = NA_MIN1 + 256;
 constexpr size_t NA_MIN2 = NA_MAX1 + 256;
 constexpr size_t NA_PATH0 = NA_MIN2 + 256;
 constexpr size_t NA_PATH1 = NA_PATH0 + 256;
-constexpr size_t NA_COUNTS = NA_PATH1 + 256;
+constexpr size_t NA_SEED0 = NA_PATH1 + 256;
+constexpr size_t NA_SEED1 = NA_SEED0 + 256;
+constexpr uint32_t NA_RO_CAP = 2 * 32;  // two boundary results per level
+constexpr size_t NA_RO_PQ = NA_SEED1 + 256;
+constexpr size_t NA_RO_BIT = NA_RO_PQ + NA_RO_CAP * sizeof(uint2);
+constexpr size_t NA_COUNTS = NA_RO_BIT + 256;
 constexpr size_t NA_CURSOR = NA_COUNTS + 256;
 constexpr size_t NA_OFFSETS = NA_CURSOR + 256;
 constexpr size_t NA_SCAN = NA_OFFSETS + 256;
-constexpr size_t NA_TASKS = NA_SCAN + 256;
-// tasks (16 B) and survivor masks (4 B) share the rest
-constexpr uint64_t NA_TASK_CAP = (NOALLOC_SCRATCH_BYTES - NA_TASKS) / (sizeof(uint4) + 4);
-constexpr size_t NA_AMASK = NA_TASKS + NA_TASK_CAP * sizeof(uint4);
+constexpr size_t NA_RECS = NA_SCAN + 256;
+// alive records (8 B position/query + 4 B mask) share the rest
+constexpr uint64_t NA_REC_CAP = (NOALLOC_SCRATCH_BYTES - NA_RECS) / (sizeof(uint2) + 4) / 64 * 64;
+constexpr size_t NA_REC_AM = NA_RECS + NA_REC_CAP * sizeof(uint2);
 static_assert(sizeof(BatchCtl) <= NA_QRAW, "control block");
-static_assert(NA_AMASK + NA_TASK_CAP * 4 <= NOALLOC_SCRATCH_BYTES, "scratch layout");
-// One query's frontier holds at most one task per 32-slot chunk of every level,
-// plus per level at most two report-above seeds and two boundary results:
-// 2^L/16 + 4L + 32 tasks for a tree of L levels.
-static_assert((1ull << NOALLOC_MAX_LEVELS) / 16 + 4 * NOALLOC_MAX_LEVELS + 32 <= NA_TASK_CAP, "frontier bound");
+static_assert(NA_RO_CAP * 4 <= 256, "boundary-result bits");
+static_assert(NA_REC_AM + NA_REC_CAP * 4 <= NOALLOC_SCRATCH_BYTES, "scratch layout");
+// One query has at most one alive record per 32-slot chunk of every level, plus the
+// records of report-above subtrees that still share a chunk with another subtree:
+// a seed's subtree shares chunks for its first five levels and a query leaves at
+// most two seeds per level, so at most 10 more per level: 2^L/16 + 12L + 32 records
+// for a tree of L levels.
+static_assert((1ull << NOALLOC_MAX_LEVELS) / 16 + 12 * NOALLOC_MAX_LEVELS + 32 <= NA_REC_CAP, "frontier bound");
 
 std::mutex g_noalloc_mu;
 unsigned char *g_noalloc_ptr[64] = {};
@@ -659,12 +795,16 @@ uint64_t noalloc_run(TreeStorage &t, const pst_query &q, pst_ret ret, void *out,
 	T *min2 = reinterpret_cast<T *>(base + NA_MIN2);
 	uint4 *path0 = reinterpret_cast<uint4 *>(base + NA_PATH0);
 	uint4 *path1 = reinterpret_cast<uint4 *>(base + NA_PATH1);
+	uint4 *seed0 = reinterpret_cast<uint4 *>(base + NA_SEED0);
+	uint4 *seed1 = reinterpret_cast<uint4 *>(base + NA_SEED1);
+	uint2 *ro_pq = reinterpret_cast<uint2 *>(base + NA_RO_PQ);
+	uint32_t *ro_bit = reinterpret_cast<uint32_t *>(base + NA_RO_BIT);
 	uint64_t *counts = reinterpret_cast<uint64_t *>(base + NA_COUNTS);
 	uint64_t *cursor = reinterpret_cast<uint64_t *>(base + NA_CURSOR);
 	uint64_t *offsets = reinterpret_cast<uint64_t *>(base + NA_OFFSETS);
 	uint64_t *scan = reinterpret_cast<uint64_t *>(base + NA_SCAN);
-	uint4 *tasks = reinterpret_cast<uint4 *>(base + NA_TASKS);
-	uint32_t *amask = reinterpret_cast<uint32_t *>(base + NA_AMASK);
+	uint2 *rec_pq = reinterpret_cast<uint2 *>(base + NA_RECS);
+	uint32_t *rec_am = reinterpret_cast<uint32_t *>(base + NA_REC_AM);
 
 	// The array keeps the previous call's contents: reset everything that must
 	// start at zero (control block with nq = 1, count, output cursor).
@@ -680,7 +820,8 @@ uint64_t noalloc_run(TreeStorage &t, const pst_query &q, pst_ret ret, void *out,
 	const unsigned grid = (unsigned) device_info().sms * (unsigned) std::max(occ, 1);
 	TreeDev<T> tv = t.view<T>();
 	QDev<T> qd{kind, min1, max1, min2};
-	WorkDev w{tasks, amask, NA_TASK_CAP, path0, path1, 2u, counts, cursor, offsets, ctl};
+	WorkDev w{rec_pq, rec_am, NA_REC_CAP, path0, path1, seed0, seed1, 2u, ro_pq, ro_bit, NA_RO_CAP,
+	          counts, cursor, offsets, ctl};
 	k_check_kinds<<<1, 32, 0, s>>>(qraw, ctl);
 	k_unpack_queries<T><<<1, 32, 0, s>>>(qraw, ctl, kind, min1, max1, min2, path0);
 	for (uint32_t d = 0; d < tv.levels; d++)

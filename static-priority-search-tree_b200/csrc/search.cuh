@@ -17,10 +17,13 @@ enum : uint32_t {
 // Device control block of one pass; the host uploads a zeroed copy (with nq set)
 // at the start of every pass.
 struct BatchCtl {
-	uint32_t lvl_cnt[40];   // chunk tasks appended per level region
+	uint32_t lvl_cnt[40];   // alive records appended per level region
 	uint32_t path_cnt[40];  // boundary-path tasks per level
+	uint32_t seed_cnt[40];  // report-above seeds per level
+	uint32_t rec_cnt;       // reported boundary nodes
 	uint32_t nq;
 	uint32_t flags;
+	uint32_t pad;
 	uint64_t need_tasks;
 	uint64_t total;
 };
@@ -38,10 +41,15 @@ struct Batch {
 	uint32_t *kind = nullptr;
 	void *min1 = nullptr, *max1 = nullptr, *min2 = nullptr;
 	// frontier and results
-	uint4 *tasks = nullptr;
-	uint32_t *amask = nullptr;
-	uint64_t task_cap = 0;
+	uint2 *rec_pq = nullptr;   // alive records: (chunk base position, query)
+	uint32_t *rec_am = nullptr; // ... and their masks of reported slots
+	uint64_t task_cap = 0;      // alive-record capacity
 	uint4 *path0 = nullptr, *path1 = nullptr;
+	uint4 *seed0 = nullptr, *seed1 = nullptr;
+	uint32_t path_cap = 0;
+	uint2 *ro_pq = nullptr;     // reported boundary nodes
+	uint32_t *ro_bit = nullptr;
+	uint32_t ro_cap = 0;
 	uint64_t *counts = nullptr, *cursor = nullptr, *offsets = nullptr, *scan_tmp = nullptr;
 	BatchCtl *ctl = nullptr;
 	BatchCtl *ctl_host = nullptr;  // pinned, zeroed except nq

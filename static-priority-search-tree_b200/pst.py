@@ -50,6 +50,11 @@ class ServerStats(C.Structure):
                 ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double), ("busy_s", C.c_double)]
 
 
+class BatchStats(C.Structure):
+    _fields_ = [("records", C.c_uint64), ("seeds", C.c_uint64), ("boundary", C.c_uint64), ("points", C.c_uint64),
+                ("levels", C.c_uint32)]
+
+
 QUERY_NP = np.dtype([("kind", "<i4"), ("reserved", "<i4"), ("min1", "<u8"), ("max1", "<u8"), ("min2", "<u8")])
 
 _lib = None
@@ -85,6 +90,7 @@ def lib():
         "pst_batch_run": (i32, [vp, vp, u32, i32, i32, vp, u64, vp, P(u64), i32, vp]),
         "pst_batch_count": (i32, [vp, vp, u32, i32, vp, P(u64), vp]),
         "pst_batch_status": (i32, [vp, P(u64)]),
+        "pst_batch_last_stats": (i32, [vp, P(BatchStats), vp]),
         "pst_ips_search": (i32, [i32, i32, vp, u64, u64, i32, P(vp), P(u64), u32, u32, vp]),
         "pst_ips_search_into": (i32, [i32, i32, vp, u64, u64, i32, vp, u64, P(u64), vp]),
         "pst_num_metacells": (i32, [P(u32), P(u32), P(u32), P(u64)]),
@@ -325,6 +331,14 @@ class BatchEngine:
             self.close()
         except Exception:
             pass
+
+    def last_stats(self) -> dict:
+        st = BatchStats()
+        per = (C.c_uint32 * 40)()
+        _check(lib().pst_batch_last_stats(self._h, C.byref(st), per))
+        d = {f: getattr(st, f) for f, _ in BatchStats._fields_}
+        d["per_level"] = list(per)[: st.levels]
+        return d
 
     def count(self, queries: np.ndarray, stream=None):
         torch = _torch()
