@@ -147,45 +147,70 @@ __device__ void path_step(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev 
 
 // Tests the 32*K chunk tasks held by a warp (lane l owns tasks (l, 0..K-1): chunk
 // base p[k], candidate lanes cand[k], the query's min2) and returns each task's
-// mask of reported slots in am[k].  LOADS_IN_FLIGHT masked row loads are issued
-// before their ballots.
+// mask of reported slots in am[k].  A task with at most SPARSE_BITS candidates is
+// tested by its own lane, bit by bit; the others are tested by the whole warp, one
+// coalesced row each, LOADS_IN_FLIGHT rows issued before their ballots.
+constexpr int SPARSE_BITS = 6;
+
 template <typename T, int K>
 __device__ __forceinline__ void test_chunks(const T *__restrict__ dim2, const uint32_t (&p)[K],
                                             const uint32_t (&cand)[K], T m2, uint32_t (&am)[K])
 {
 	const uint32_t lane = lane_id();
-	uint32_t any = 0;
+	uint32_t dense_mask[K];
 #pragma unroll
 	for (int k = 0; k < K; k++) {
 		am[k] = 0;
-		any |= cand[k];
-	}
-	const uint32_t busy = __ballot_sync(FULL, any != 0);
-	if (!busy)
-		return;
-#pragma unroll
-	for (int g = 0; g < 32 * K; g += LOADS_IN_FLIGHT) {
-		// skip a group whose owning lanes have nothing to test
-		const uint32_t owners = ((1u << (LOADS_IN_FLIGHT / K)) - 1u) << (g / K);
-		if (!(busy & owners))
-			continue;
-		T v[LOADS_IN_FLIGHT], mm[LOADS_IN_FLIGHT];
-		bool ld[LOADS_IN_FLIGHT];
-#pragma unroll
-		for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
-			const int src = (g + u) / K, k = (g + u) % K;
-			const uint32_t c = __shfl_sync(FULL, cand[k], src);
-			const uint32_t pp = __shfl_sync(FULL, p[k], src);
-			mm[u] = __shfl_sync(FULL, m2, src);
-			ld[u] = (c >> lane) & 1u;
-			v[u] = ld[u] ? dim2[pp + lane] : T(0);
+		const uint32_t c = cand[k];
+		const bool dense = __popc(c) > SPARSE_BITS;
+		dense_mask[k] = __ballot_sync(FULL, dense);
+		if (!dense && c) {
+			// lane mode: a handful of slots of one 128-byte row
+			uint32_t bits = c, a = 0;
+			while (bits) {
+				const uint32_t b0 = __ffs(bits) - 1;
+				bits &= bits - 1;
+				if (bits) {
+					const uint32_t b1 = __ffs(bits) - 1;
+					bits &= bits - 1;
+					const T v0 = dim2[p[k] + b0], v1 = dim2[p[k] + b1];
+					a |= (m2 <= v0 ? 1u << b0 : 0u) | (m2 <= v1 ? 1u << b1 : 0u);
+				} else {
+					const T v0 = dim2[p[k] + b0];
+					a |= m2 <= v0 ? 1u << b0 : 0u;
+				}
+			}
+			am[k] = a;
 		}
+	}
 #pragma unroll
-		for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
-			const int src = (g + u) / K, k = (g + u) % K;
-			const uint32_t a = __ballot_sync(FULL, ld[u] && (mm[u] <= v[u]));
-			if (lane == (uint32_t) src)
-				am[k] = a;
+	for (int k = 0; k < K; k++) {
+		uint32_t dm = dense_mask[k];
+		while (dm) {
+			// up to LOADS_IN_FLIGHT dense tasks, lowest lanes first (warp-uniform)
+			int src[LOADS_IN_FLIGHT];
+#pragma unroll
+			for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
+				src[u] = dm ? __ffs(dm) - 1 : -1;
+				dm &= dm ? dm - 1 : 0u;
+			}
+			T v[LOADS_IN_FLIGHT], mm[LOADS_IN_FLIGHT];
+			bool ld[LOADS_IN_FLIGHT];
+#pragma unroll
+			for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
+				const int sl = src[u] < 0 ? 0 : src[u];
+				const uint32_t c = __shfl_sync(FULL, cand[k], sl);
+				const uint32_t pp = __shfl_sync(FULL, p[k], sl);
+				mm[u] = __shfl_sync(FULL, m2, sl);
+				ld[u] = src[u] >= 0 && ((c >> lane) & 1u);
+				v[u] = ld[u] ? dim2[pp + lane] : T(0);
+			}
+#pragma unroll
+			for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
+				const uint32_t a = __ballot_sync(FULL, ld[u] && (mm[u] <= v[u]));
+				if (src[u] >= 0 && lane == (uint32_t) src[u])
+					am[k] = a;
+			}
 		}
 	}
 }
@@ -339,30 +364,78 @@ __global__ void k_check_kinds(const pst_query *raw, BatchCtl *ctl)
 }
 
 // Writes the results of up to 32 records (lane r owns record (p, am) whose results
-// start at out_base) in batches of LOADS_IN_FLIGHT rows: loads first, then stores.
+// start at out_base).  A record of at most SPARSE_BITS points is written by its own
+// lane; the others by the whole warp, one row each, LOADS_IN_FLIGHT rows loaded
+// before they are stored.
+template <typename T, bool HAS_ID, bool POINTS>
+__device__ __forceinline__ void emit_one(const TreeDev<T> &t, uint32_t h, uint64_t o, void *__restrict__ out)
+{
+	using Pt = Point<T, HAS_ID>;
+	if constexpr (POINTS) {
+		Pt rec;
+		rec.dim1 = t.dim1[h];
+		rec.dim2 = t.dim2[h];
+		if constexpr (HAS_ID)
+			rec.id = t.id[h];
+		static_cast<Pt *>(out)[o] = rec;
+	} else {
+		static_cast<uint32_t *>(out)[o] = t.id[h];
+	}
+}
+
 template <typename T, bool HAS_ID, bool POINTS>
 __device__ __forceinline__ void emit_rows(const TreeDev<T> &t, uint32_t p, uint32_t am, uint64_t out_base,
                                           void *__restrict__ out, uint64_t capacity)
 {
 	using Pt = Point<T, HAS_ID>;
 	const uint32_t lane = lane_id();
-	const uint32_t busy = __ballot_sync(FULL, am != 0);
+	const bool dense = __popc(am) > SPARSE_BITS;
+	if (!dense && am && out_base + __popc(am) <= capacity) {
+		uint32_t bits = am;
+		uint64_t o = out_base;
+		while (bits) {
+			const uint32_t b0 = __ffs(bits) - 1;
+			bits &= bits - 1;
+			if (bits) {
+				const uint32_t b1 = __ffs(bits) - 1;
+				bits &= bits - 1;
+				if constexpr (POINTS) {
+					emit_one<T, HAS_ID, POINTS>(t, p + b0, o, out);
+					emit_one<T, HAS_ID, POINTS>(t, p + b1, o + 1, out);
+				} else {
+					const uint32_t i0 = t.id[p + b0], i1 = t.id[p + b1];
+					static_cast<uint32_t *>(out)[o] = i0;
+					static_cast<uint32_t *>(out)[o + 1] = i1;
+				}
+				o += 2;
+			} else {
+				emit_one<T, HAS_ID, POINTS>(t, p + b0, o, out);
+				o += 1;
+			}
+		}
+	}
 	const uint32_t *__restrict__ ids = t.id;
 	const T *__restrict__ d1 = t.dim1;
 	const T *__restrict__ d2 = t.dim2;
+	uint32_t dm = __ballot_sync(FULL, dense);
+	while (dm) {
+		int src[LOADS_IN_FLIGHT];
 #pragma unroll
-	for (int g = 0; g < 32; g += LOADS_IN_FLIGHT) {
-		if (!(busy & (((1u << LOADS_IN_FLIGHT) - 1u) << g)))
-			continue;
+		for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
+			src[u] = dm ? __ffs(dm) - 1 : -1;
+			dm &= dm ? dm - 1 : 0u;
+		}
 		uint32_t a[LOADS_IN_FLIGHT];
 		uint64_t ob[LOADS_IN_FLIGHT];
 		uint32_t vid[LOADS_IN_FLIGHT];
 		T v1[LOADS_IN_FLIGHT], v2[LOADS_IN_FLIGHT];
 #pragma unroll
 		for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
-			a[u] = __shfl_sync(FULL, am, g + u);
-			const uint32_t pp = __shfl_sync(FULL, p, g + u);
-			ob[u] = __shfl_sync(FULL, out_base, g + u);
+			const int sl = src[u] < 0 ? 0 : src[u];
+			const uint32_t av = __shfl_sync(FULL, am, sl);
+			a[u] = src[u] >= 0 ? av : 0u;
+			const uint32_t pp = __shfl_sync(FULL, p, sl);
+			ob[u] = __shfl_sync(FULL, out_base, sl);
 			const bool on = (a[u] >> lane) & 1u;
 			const uint32_t h = pp + lane;
 			if constexpr (HAS_ID)

@@ -230,7 +230,9 @@ struct Server {
 		if (sl.phase == SLOT_COUNTING) {
 			const BatchCtl &c = *sl.ctl_h;
 			if (c.flags & BATCH_FLAG_TASK_OVERFLOW) {
-				sl.eng.grow_tasks(std::max<uint64_t>(c.need_tasks + c.need_tasks / 4, sl.eng.task_cap * 2));
+				// the pass stopped at the first level that overflowed, so deeper
+				// levels will want more: grow generously
+				sl.eng.grow_tasks(std::max<uint64_t>(c.need_tasks * 2, sl.eng.task_cap * 2));
 				launch_count(sl);
 				return true;
 			}
@@ -428,8 +430,30 @@ uint32_t server_add_tree(Server *s, TreeStorage *t)
 		pst_batch_opts bo{};
 		bo.max_queries = s->opts.max_batch;
 		bo.use_graph = s->opts.use_graph;
+		// frontier sized from the tree (a quarter record per point) so that batches
+		// rarely grow it while requests wait
+		bo.task_capacity = std::max<uint64_t>(1ull << 16, t->n / 4);
 		sl->eng.init(t, bo);
 		check_cuda(cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+		// warm-up pass: captures the slot's graph now rather than under the first request
+		{
+			// an inverted 3-sided range walks one path and reports nothing
+			pst_query q{};
+			q.kind = PST_Q_THREE;
+			if (t->dtype == PST_F32) {
+				q.min1.f32 = 1.0f;
+				q.max1.f32 = 0.0f;
+			} else if (t->dtype == PST_F64) {
+				q.min1.f64 = 1.0;
+				q.max1.f64 = 0.0;
+			} else {
+				q.min1.i32 = 1;
+				q.max1.i32 = 0;
+			}
+			sl->eng.stage_queries(&q, 1, false, sl->stream);
+			uint64_t total = 0;
+			sl->eng.count_sync(sl->stream, &total);
+		}
 		check_cuda(cudaEventCreateWithFlags(&sl->ev, cudaEventDisableTiming), "cudaEventCreate");
 		check_cuda(cudaMallocHost((void **) &sl->ctl_h, sizeof(BatchCtl)), "cudaMallocHost");
 		check_cuda(cudaMallocHost((void **) &sl->counts_h, (size_t) s->opts.max_batch * 8), "cudaMallocHost");
