@@ -12,11 +12,17 @@
 // partitions index arrays one node at a time (pst/static-pst-gpu.tu:678-806; one
 // thread per node, one block, dynamic parallelism).  This build works level by level
 // instead:
-//   1. one radix sort ranks the points in dim1 order and one in dim2 order;
-//   2. for the wide top levels, a streaming segmented arg-max over the dim1-ordered
-//      dim2 ranks picks every node's point of the level at once, and a per-node
-//      kernel places the median.  Points already taken by ancestors are zeroed
-//      and so drop out of later maxima;
+//   1. every point gets a tiebreak rank tb (its place in (id, input index) order) and
+//      a 64-bit dim2 key whose order is the dim2 order: (dim2 key << 32 | tb + 1) for
+//      4-byte values, (dim2 rank << 32 | tb + 1) for doubles (one extra sort finds
+//      the ranks).  One radix sort by dim1 key carries these keys along, so position
+//      i of the sorted arrays is the i-th point in dim1 order;
+//   2. for the wide top levels, a segmented arg-max over the sorted dim2 keys picks
+//      every node's point of the level at once.  It reads a maximum per 512-position
+//      tile and scans only the tiles cut by a node boundary; points taken by
+//      ancestors are marked in a bitmap, and only the tiles that lost a point are
+//      re-reduced.  A per-node kernel then finds the taken point's position (binary
+//      search on (dim1 key, tb)) and places the median;
 //   3. once every node of a level holds at most ST_CAP points, one CTA per node
 //      builds the whole remaining subtree in shared memory.
 #include <algorithm>
@@ -76,12 +82,12 @@ TreeLayout tree_layout(pst_dtype dt, pst_idtype it, uint64_t n)
 // Subtree builder capacity: nodes of at most ST_CAP points are finished by one CTA.
 constexpr uint32_t ST_CAP = 2048;
 constexpr int ST_THREADS = 256;
-// Arg-max tile: every segment of a level before the subtree level spans at least
-// ST_CAP >= AM_TILE positions, so a tile meets at most two segments.
+// Arg-max tiles: every segment of a level before the subtree level spans at least
+// ST_CAP >= TM_TILE positions, so a tile is cut by at most one segment boundary.
+constexpr uint32_t TM_TILE = 512;
 constexpr int AM_THREADS = 256;
-constexpr int AM_ITEMS = 8;
-constexpr uint32_t AM_TILE = AM_THREADS * AM_ITEMS;
-static_assert(ST_CAP >= AM_TILE, "tile/segment invariant");
+static_assert(ST_CAP >= TM_TILE, "tile/segment invariant");
+static_assert(TM_TILE % 32 == 0, "tiles are whole bitmap words");
 
 // First level whose largest node holds at most ST_CAP points.  Counts within a
 // level take at most two consecutive values (m, m+1).
@@ -96,28 +102,32 @@ uint32_t subtree_level(uint64_t n)
 	return d;
 }
 
+// Sorted arrays, position i = i-th point in dim1 order:
+//   k1s[i]  dim1 key, c2s[i] 64-bit dim2 key (never 0; low 32 bits = tb + 1),
+//   taken   one bit per position, set once the point is stored in a node.
 template <typename T, bool HAS_ID>
 struct BuildCtx {
+	using K = typename KeyOf<T>::K;
 	const Point<T, HAS_ID> *pts;
-	const uint32_t *P;       // tiebreak rank -> input index (null: identity)
-	const uint32_t *S1;      // dim1-sorted position -> tiebreak rank
-	uint32_t *r2p1;          // dim1-sorted position -> dim2 rank + 1 (0 once taken)
-	const uint32_t *pos_of_rank2;
+	const uint32_t *P;  // tiebreak rank -> input index (null: identity)
+	const K *k1s;
+	const uint64_t *c2s;
+	uint32_t *taken;
+	uint64_t *tmax;     // per TM_TILE tile: max c2s over positions not taken (0 if none)
 	T *dim1;
 	T *dim2;
 	T *med;
 	uint32_t *id;
 	uint32_t *occ;
-	uint32_t *top_pos;       // heap position -> dim1-sorted position of its point (levels < L0)
+	uint32_t *top_pos;  // heap position -> dim1-sorted position of its point (levels < L0)
 	uint32_t *err;
 	uint64_t n;
 	uint32_t D;
 
-	__device__ __forceinline__ Point<T, HAS_ID> point_at(uint32_t pos) const
-	{
-		const uint32_t tb = S1[pos];
-		return pts[P ? P[tb] : tb];
-	}
+	__device__ __forceinline__ Point<T, HAS_ID> point_of_tb(uint32_t tb) const { return pts[P ? P[tb] : tb]; }
+	__device__ __forceinline__ static uint32_t tb_of(uint64_t key2) { return (uint32_t) key2 - 1u; }
+	__device__ __forceinline__ Point<T, HAS_ID> point_at(uint32_t pos) const { return point_of_tb(tb_of(c2s[pos])); }
+	__device__ __forceinline__ bool is_taken(uint64_t pos) const { return (taken[pos >> 5] >> (pos & 31)) & 1u; }
 
 	__device__ __forceinline__ void write_node(uint32_t h, const Point<T, HAS_ID> &p) const
 	{
@@ -128,19 +138,82 @@ struct BuildCtx {
 	}
 };
 
+__device__ __forceinline__ uint64_t warp_max_u64(uint64_t v)
+{
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		const uint64_t t = __shfl_xor_sync(0xFFFFFFFFu, v, o);
+		v = t > v ? t : v;
+	}
+	return v;
+}
+
+template <typename K>
+__device__ __forceinline__ void atomic_min_key(K *p, K v)
+{
+	if constexpr (sizeof(K) == 4)
+		atomicMin(reinterpret_cast<unsigned int *>(p), (unsigned int) v);
+	else
+		atomicMin(reinterpret_cast<unsigned long long *>(p), (unsigned long long) v);
+}
+
+template <typename K>
+__device__ __forceinline__ void atomic_max_key(K *p, K v)
+{
+	if constexpr (sizeof(K) == 4)
+		atomicMax(reinterpret_cast<unsigned int *>(p), (unsigned int) v);
+	else
+		atomicMax(reinterpret_cast<unsigned long long *>(p), (unsigned long long) v);
+}
+
+// Block-wide min and max of (lo, hi), folded into range[0] / range[1] with atomics.
+template <typename K>
+__device__ void block_range_fold(K lo, K hi, K *range)
+{
+	__shared__ K s_lo[32], s_hi[32];
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1) {
+		const K a = __shfl_xor_sync(0xFFFFFFFFu, lo, o), b = __shfl_xor_sync(0xFFFFFFFFu, hi, o);
+		lo = a < lo ? a : lo;
+		hi = b > hi ? b : hi;
+	}
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+	if (lane == 0) {
+		s_lo[warp] = lo;
+		s_hi[warp] = hi;
+	}
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		for (int w = 1; w < nw; w++) {
+			lo = s_lo[w] < lo ? s_lo[w] : lo;
+			hi = s_hi[w] > hi ? s_hi[w] : hi;
+		}
+		atomic_min_key<K>(&range[0], lo);
+		atomic_max_key<K>(&range[1], hi);
+	}
+}
+
 // ---------------------------------------------------------------------------
 // Preparation kernels.
 
+// flag |= 1 when ids decrease somewhere; id_range = [min id, max id].
 template <typename T, bool HAS_ID>
-__global__ void k_ids_monotone(const Point<T, HAS_ID> *pts, uint64_t n, uint32_t *flag)
+__global__ void k_ids_scan(const Point<T, HAS_ID> *pts, uint64_t n, uint32_t *flag, uint32_t *id_range)
 {
 	if constexpr (HAS_ID) {
-		for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i + 1 < n;
-		     i += (uint64_t) gridDim.x * blockDim.x)
-			if (pts[i].id > pts[i + 1].id) {
-				atomicOr(flag, 1u);
-				return;
-			}
+		uint32_t lo = 0xFFFFFFFFu, hi = 0;
+		bool dec = false;
+		for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+		     i += (uint64_t) gridDim.x * blockDim.x) {
+			const uint32_t v = pts[i].id;
+			lo = min(lo, v);
+			hi = max(hi, v);
+			if (i + 1 < n && v > pts[i + 1].id)
+				dec = true;
+		}
+		if (__any_sync(0xFFFFFFFFu, dec) && (threadIdx.x & 31) == 0)
+			atomicOr(flag, 1u);
+		block_range_fold<uint32_t>(lo, hi, id_range);
 	}
 }
 
@@ -153,154 +226,230 @@ __global__ void k_id_keys(const Point<T, HAS_ID> *pts, uint64_t n, uint32_t *key
 	}
 }
 
-// Keys of both dimensions in tiebreak-rank order r (input index P[r]).
+// Keys in tiebreak-rank order r (input index P[r]): k1[r] = dim1 key and either the
+// final 64-bit dim2 key (4-byte values) or the raw dim2 key k2[r] (doubles).
+// range = [min k1, max k1, min k2, max k2].
 template <typename T, bool HAS_ID>
-__global__ void k_value_keys(const Point<T, HAS_ID> *pts, const uint32_t *P, uint64_t n, typename KeyOf<T>::K *k1,
-                             typename KeyOf<T>::K *k2)
+__global__ void k_prep_keys(const Point<T, HAS_ID> *pts, const uint32_t *P, uint64_t n,
+                            typename KeyOf<T>::K *k1, uint64_t *c2, typename KeyOf<T>::K *k2,
+                            typename KeyOf<T>::K *range)
 {
+	using K = typename KeyOf<T>::K;
+	K lo1 = ~K(0), hi1 = 0, lo2 = ~K(0), hi2 = 0;
 	for (uint64_t r = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (uint64_t) gridDim.x * blockDim.x) {
 		const Point<T, HAS_ID> p = pts[P ? P[r] : r];
-		k1[r] = KeyOf<T>::key(p.dim1);
-		k2[r] = KeyOf<T>::key(p.dim2);
+		const K a = KeyOf<T>::key(p.dim1), b = KeyOf<T>::key(p.dim2);
+		k1[r] = a;
+		if constexpr (sizeof(K) == 4)
+			c2[r] = ((uint64_t) b << 32) | (uint64_t) (r + 1);
+		else
+			k2[r] = b;
+		lo1 = a < lo1 ? a : lo1;
+		hi1 = a > hi1 ? a : hi1;
+		lo2 = b < lo2 ? b : lo2;
+		hi2 = b > hi2 ? b : hi2;
 	}
+	block_range_fold<K>(lo1, hi1, range);
+	__syncthreads();
+	block_range_fold<K>(lo2, hi2, range + 2);
 }
 
-__global__ void k_iota(uint32_t *v, uint64_t n)
+// Doubles: S2 = dim2-sorted position -> tb (null: identity); c2[tb] = rank << 32 | tb + 1.
+__global__ void k_rank_keys(const uint32_t *S2, uint64_t n, uint64_t *c2)
 {
-	for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t) gridDim.x * blockDim.x)
-		v[i] = (uint32_t) i;
-}
-
-__global__ void k_rank_scatter(const uint32_t *S2, uint64_t n, uint32_t *rank2_of_tb)
-{
-	for (uint64_t j = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t) gridDim.x * blockDim.x)
-		rank2_of_tb[S2[j]] = (uint32_t) j;
-}
-
-__global__ void k_sorted_ranks(const uint32_t *S1, const uint32_t *rank2_of_tb, uint64_t n, uint32_t *r2p1,
-                               uint32_t *pos_of_rank2)
-{
-	for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t) gridDim.x * blockDim.x) {
-		const uint32_t rk = rank2_of_tb[S1[i]];
-		r2p1[i] = rk + 1;
-		pos_of_rank2[rk] = (uint32_t) i;
+	for (uint64_t j = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t) gridDim.x * blockDim.x) {
+		const uint32_t tb = S2 ? S2[j] : (uint32_t) j;
+		c2[tb] = (j << 32) | (uint64_t) (tb + 1);
 	}
 }
 
 // ---------------------------------------------------------------------------
 // Wide levels.
 
-// best[s] = max r2p1 over positions [B[s], B[s+1]).  Each CTA walks a contiguous
-// run of tiles and keeps the open segment's running maximum, so a segment costs
-// one global atomic per CTA that touches it.
-__global__ void __launch_bounds__(AM_THREADS) k_level_argmax(const uint32_t *__restrict__ r2p1, uint64_t n,
-                                                             const uint32_t *__restrict__ B, uint32_t nseg,
-                                                             uint32_t *best, uint64_t tiles_per_cta)
+// Maximum of c2s over the positions of tile t that are not taken; one warp per tile.
+__device__ __forceinline__ uint64_t tile_max(const uint64_t *__restrict__ c2s, const uint32_t *__restrict__ taken,
+                                             uint64_t n, uint64_t t)
 {
-	__shared__ uint32_t s_red[2][AM_THREADS / 32];
-	__shared__ uint32_t s_seg;
-	const uint64_t num_tiles = (n + AM_TILE - 1) / AM_TILE;
-	const uint64_t tb = (uint64_t) blockIdx.x * tiles_per_cta;
-	const uint64_t te = min(tb + tiles_per_cta, num_tiles);
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	uint32_t run_seg = 0xFFFFFFFFu, run_max = 0;  // thread 0 only
-	for (uint64_t tile = tb; tile < te; tile++) {
-		const uint64_t t0 = tile * AM_TILE;
-		if (threadIdx.x == 0) {
-			uint32_t lo = 0, hi = nseg;  // largest s in [0, nseg) with B[s] <= t0
+	const uint32_t lane = lane_id();
+	const uint64_t t0 = t * TM_TILE;
+	uint64_t m = 0;
+#pragma unroll 4
+	for (uint32_t k = 0; k < TM_TILE / 32; k++) {
+		const uint64_t i = t0 + k * 32 + lane;
+		if (i < n) {
+			const uint32_t w = taken[i >> 5];  // one word per k, the same for the whole warp
+			if (!((w >> lane) & 1u))
+				m = max(m, c2s[i]);
+		}
+	}
+	return warp_max_u64(m);
+}
+
+__global__ void __launch_bounds__(AM_THREADS) k_tile_max_all(const uint64_t *__restrict__ c2s,
+                                                             const uint32_t *__restrict__ taken, uint64_t n,
+                                                             uint64_t *tmax)
+{
+	const uint64_t ntiles = (n + TM_TILE - 1) / TM_TILE;
+	const uint64_t gw = ((uint64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t nw = ((uint64_t) gridDim.x * blockDim.x) >> 5;
+	for (uint64_t t = gw; t < ntiles; t += nw) {
+		const uint64_t m = tile_max(c2s, taken, n, t);
+		if (lane_id() == 0)
+			tmax[t] = m;
+	}
+}
+
+// Re-reduces the tiles that lost a point at level d (one warp per node).
+__global__ void __launch_bounds__(AM_THREADS) k_tile_refresh(const uint64_t *__restrict__ c2s,
+                                                             const uint32_t *__restrict__ taken, uint64_t n,
+                                                             const uint32_t *__restrict__ top_pos, uint32_t d,
+                                                             uint64_t *tmax, const uint32_t *err)
+{
+	const uint32_t nseg = 1u << d;
+	const uint64_t gw = ((uint64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	if (gw >= nseg || *err)  // after an error top_pos may hold unwritten entries
+		return;
+	const uint64_t t = top_pos[nseg + gw] / TM_TILE;
+	if (t >= (n + TM_TILE - 1) / TM_TILE)
+		return;
+	const uint64_t m = tile_max(c2s, taken, n, t);
+	if (lane_id() == 0)
+		tmax[t] = m;  // tiles shared by two nodes get the same value twice
+}
+
+// best[s] = max c2s over the positions of [B[s], B[s+1]) not taken.  A thread owns a
+// tile: tiles inside one segment contribute their tmax (one atomic per run of equal
+// segments in a warp); a tile cut by a boundary is scanned by the whole warp.
+__global__ void __launch_bounds__(AM_THREADS) k_level_argmax(const uint64_t *__restrict__ c2s,
+                                                             const uint32_t *__restrict__ taken,
+                                                             const uint64_t *__restrict__ tmax, uint64_t n,
+                                                             const uint32_t *__restrict__ B, uint32_t nseg,
+                                                             unsigned long long *best, const uint32_t *err)
+{
+	if (*err)  // after an error the bounds may hold unwritten entries
+		return;
+	const uint64_t ntiles = (n + TM_TILE - 1) / TM_TILE;
+	const uint32_t lane = lane_id();
+	const uint64_t gw = ((uint64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t nw = ((uint64_t) gridDim.x * blockDim.x) >> 5;
+	for (uint64_t wb = gw * 32; wb < ntiles; wb += nw * 32) {
+		const uint64_t t = wb + lane;
+		const bool valid = t < ntiles;
+		const uint64_t t0 = t * TM_TILE;
+		const uint64_t t1 = valid ? min(t0 + TM_TILE, n) : 0;
+		uint32_t seg = 0xFFFFFFFFu;
+		uint64_t seg_end = 0;
+		if (valid) {
+			uint32_t lo = 0, hi = nseg;  // largest s with B[s] <= t0
 			while (hi - lo > 1) {
-				uint32_t mid = (lo + hi) / 2;
+				const uint32_t mid = (lo + hi) / 2;
 				if (B[mid] <= t0)
 					lo = mid;
 				else
 					hi = mid;
 			}
-			s_seg = lo;
+			seg = lo;
+			seg_end = B[lo + 1];
 		}
-		__syncthreads();
-		const uint32_t sa = s_seg;
-		const uint64_t bnd = sa + 1 < nseg ? B[sa + 1] : n;
-		uint32_t ma = 0, mb = 0;
-		const uint64_t base = t0 + (uint64_t) threadIdx.x * AM_ITEMS;
-		uint32_t v[AM_ITEMS];
-		if (base + AM_ITEMS <= n && (reinterpret_cast<uintptr_t>(r2p1 + base) & 15) == 0) {
-			const uint4 a = *reinterpret_cast<const uint4 *>(r2p1 + base);
-			const uint4 b = *reinterpret_cast<const uint4 *>(r2p1 + base + 4);
-			v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-			v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-		} else {
+		const bool whole = valid && t1 <= seg_end;
+		uint64_t v = whole ? tmax[t] : 0;
+		// max over runs of equal segments (segments do not decrease along the lanes)
+		const uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, seg, 1);
+		const uint32_t heads = __ballot_sync(0xFFFFFFFFu, lane == 0 || prev != seg);
+		const uint32_t start = 31 - __clz(heads & (0xFFFFFFFFu >> (31 - lane)));
 #pragma unroll
-			for (int e = 0; e < AM_ITEMS; e++)
-				v[e] = base + e < n ? r2p1[base + e] : 0u;
+		for (int o = 1; o < 32; o <<= 1) {
+			const uint64_t u = __shfl_up_sync(0xFFFFFFFFu, v, o);
+			if (lane >= start + o)
+				v = u > v ? u : v;
 		}
-#pragma unroll
-		for (int e = 0; e < AM_ITEMS; e++) {
-			if (base + e < bnd)
-				ma = max(ma, v[e]);
-			else
-				mb = max(mb, v[e]);
-		}
-		ma = __reduce_max_sync(0xFFFFFFFFu, ma);
-		mb = __reduce_max_sync(0xFFFFFFFFu, mb);
-		if (lane == 0) {
-			s_red[0][warp] = ma;
-			s_red[1][warp] = mb;
-		}
-		__syncthreads();
-		if (threadIdx.x == 0) {
-			uint32_t MA = 0, MB = 0;
-			for (int w = 0; w < AM_THREADS / 32; w++) {
-				MA = max(MA, s_red[0][w]);
-				MB = max(MB, s_red[1][w]);
+		const uint32_t next = __shfl_down_sync(0xFFFFFFFFu, seg, 1);
+		if (valid && (lane == 31 || next != seg) && v)
+			atomicMax(&best[seg], (unsigned long long) v);
+		// tiles cut by a boundary: positions below seg_end belong to seg, the rest to seg + 1
+		uint32_t cut = __ballot_sync(0xFFFFFFFFu, valid && !whole);
+		while (cut) {
+			const int src = __ffs(cut) - 1;
+			cut &= cut - 1;
+			const uint64_t c0 = __shfl_sync(0xFFFFFFFFu, t0, src);
+			const uint64_t c1 = __shfl_sync(0xFFFFFFFFu, t1, src);
+			const uint64_t ce = __shfl_sync(0xFFFFFFFFu, seg_end, src);
+			const uint32_t cs = __shfl_sync(0xFFFFFFFFu, seg, src);
+			uint64_t ma = 0, mb = 0;
+#pragma unroll 4
+			for (uint32_t k = 0; k < TM_TILE / 32; k++) {
+				const uint64_t i = c0 + k * 32 + lane;
+				if (i < c1) {
+					const uint32_t w = taken[i >> 5];
+					if (!((w >> lane) & 1u)) {
+						const uint64_t x = c2s[i];
+						if (i < ce)
+							ma = max(ma, x);
+						else
+							mb = max(mb, x);
+					}
+				}
 			}
-			if (run_seg == sa) {
-				run_max = max(run_max, MA);
-			} else {
-				if (run_seg != 0xFFFFFFFFu)
-					atomicMax(&best[run_seg], run_max);
-				run_seg = sa;
-				run_max = MA;
-			}
-			if (bnd < (t0 + AM_TILE < n ? t0 + AM_TILE : n)) {  // the tile reaches segment sa + 1
-				atomicMax(&best[run_seg], run_max);
-				run_seg = sa + 1;
-				run_max = MB;
+			ma = warp_max_u64(ma);
+			mb = warp_max_u64(mb);
+			if (lane == 0) {
+				if (ma)
+					atomicMax(&best[cs], (unsigned long long) ma);
+				if (mb)
+					atomicMax(&best[cs + 1], (unsigned long long) mb);
 			}
 		}
-		__syncthreads();
 	}
-	if (threadIdx.x == 0 && run_seg != 0xFFFFFFFFu)
-		atomicMax(&best[run_seg], run_max);
 }
 
-// One thread per node of level d: take the arg-max point, place the median, write
+// One thread per node of level d: locate the arg-max point, place the median, write
 // the node and the next level's segment bounds.  Bounds are dim1-sorted positions
 // that still include points taken by ancestors; those (at most d of them inside a
 // segment, each the point of one ancestor) are skipped when counting to the median.
 template <typename T, bool HAS_ID>
 __global__ void k_level_nodes(BuildCtx<T, HAS_ID> c, uint32_t d, const uint32_t *__restrict__ B,
-                              uint32_t *__restrict__ Bn, const uint32_t *__restrict__ best)
+                              uint32_t *__restrict__ Bn, const unsigned long long *__restrict__ best)
 {
+	using K = typename KeyOf<T>::K;
 	const uint32_t nseg = 1u << d;
 	const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
 	if (j >= nseg)
 		return;
+	if (*c.err)
+		return;
 	const uint32_t h = nseg + j;
 	const uint64_t cnt = node_count(c.n, d, j);
 	const uint32_t lo = B[j], hi = B[j + 1];
-	const uint32_t bj = best[j];
-	if (bj == 0 || cnt < 2) {
+	const uint64_t bj = best[j];
+	if (bj == 0 || cnt < 2 || lo >= hi || hi > c.n) {
 		atomicOr(c.err, 1u);
 		return;
 	}
-	const uint32_t tp = c.pos_of_rank2[bj - 1];
-	c.r2p1[tp] = 0;
+	// position of the point: first position in [lo, hi) at or after (its dim1 key, tb)
+	const uint32_t tb = BuildCtx<T, HAS_ID>::tb_of(bj);
+	const Point<T, HAS_ID> top = c.point_of_tb(tb);
+	const K key1 = KeyOf<T>::key(top.dim1);
+	uint32_t a = lo, b = hi;
+	while (a < b) {
+		const uint32_t mid = a + (b - a) / 2;
+		const K km = c.k1s[mid];
+		if (km < key1 || (km == key1 && BuildCtx<T, HAS_ID>::tb_of(c.c2s[mid]) < tb))
+			a = mid + 1;
+		else
+			b = mid;
+	}
+	const uint32_t tp = a;
+	if (tp >= hi || c.c2s[tp] != bj) {
+		atomicOr(c.err, 8u);
+		return;
+	}
+	atomicOr(&c.taken[tp >> 5], 1u << (tp & 31));
 	c.top_pos[h] = tp;
 	uint32_t rem[33];
 	uint32_t nr = 0;
 	rem[nr++] = tp;
-	for (uint32_t a = h >> 1; a >= 1; a >>= 1) {
-		const uint32_t ta = c.top_pos[a];
+	for (uint32_t an = h >> 1; an >= 1; an >>= 1) {
+		const uint32_t ta = c.top_pos[an];
 		if (ta >= lo && ta < hi)
 			rem[nr++] = ta;
 	}
@@ -325,20 +474,20 @@ __global__ void k_level_nodes(BuildCtx<T, HAS_ID> c, uint32_t d, const uint32_t 
 	Bn[2 * j + 1] = pos + 1;
 	if (j == nseg - 1)
 		Bn[2 * nseg] = hi;
-	c.write_node(h, c.point_at(tp));
+	c.write_node(h, top);
 	c.med[h] = c.point_at(pos).dim1;
 	atomicOr(&c.occ[h >> 5], 1u << (h & 31));
 }
 
 // ---------------------------------------------------------------------------
-// Subtree builder: one CTA per node of level L0 finishes its whole subtree.
+// Subtree builder: one CTA per node of level L0 finishes its whole subtree.  The
+// CTA holds the 64-bit dim2 keys of its points in dim1 order; a key names its point
+// (tb), so no positions are carried.
 
 // Shared-memory carve-up of k_subtree, in 32-bit words.
-constexpr uint32_t ST_OFF_KEYA = 0;
-constexpr uint32_t ST_OFF_POSA = ST_OFF_KEYA + ST_CAP;
-constexpr uint32_t ST_OFF_KEYB = ST_OFF_POSA + ST_CAP;
-constexpr uint32_t ST_OFF_POSB = ST_OFF_KEYB + ST_CAP;
-constexpr uint32_t ST_OFF_CNT = ST_OFF_POSB + ST_CAP;
+constexpr uint32_t ST_OFF_KEYA = 0;                      // [ST_CAP] u64
+constexpr uint32_t ST_OFF_KEYB = ST_OFF_KEYA + 2 * ST_CAP;  // [ST_CAP] u64
+constexpr uint32_t ST_OFF_CNT = ST_OFF_KEYB + 2 * ST_CAP;
 constexpr uint32_t ST_OFF_CNT2 = ST_OFF_CNT + ST_CAP;
 constexpr uint32_t ST_OFF_START = ST_OFF_CNT2 + ST_CAP;
 constexpr uint32_t ST_OFF_TOPI = ST_OFF_START + ST_CAP + 1;
@@ -371,10 +520,8 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
                                                        const uint32_t *__restrict__ B)
 {
 	extern __shared__ __align__(16) uint32_t st_smem[];
-	uint32_t *keyA = st_smem + ST_OFF_KEYA;
-	uint32_t *posA = st_smem + ST_OFF_POSA;
-	uint32_t *keyB = st_smem + ST_OFF_KEYB;
-	uint32_t *posB = st_smem + ST_OFF_POSB;
+	uint64_t *keyA = reinterpret_cast<uint64_t *>(st_smem + ST_OFF_KEYA);
+	uint64_t *keyB = reinterpret_cast<uint64_t *>(st_smem + ST_OFF_KEYB);
 	uint32_t *cnt = st_smem + ST_OFF_CNT;     // [ST_CAP] counts of the current sub-level
 	uint32_t *cnt2 = st_smem + ST_OFF_CNT2;   // [ST_CAP] counts of the next sub-level
 	uint32_t *start = st_smem + ST_OFF_START; // [ST_CAP + 1]
@@ -384,27 +531,30 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 
 	const uint32_t j = blockIdx.x;
 	const uint64_t cN = node_count(c.n, L0, j);
-	if (cN == 0)
+	if (cN == 0 || *c.err)
 		return;
 	const uint32_t lo = L0 ? B[j] : 0u;
 	const uint32_t hi = L0 ? B[j + 1] : (uint32_t) c.n;
+	if (lo >= hi || hi > c.n) {
+		if (threadIdx.x == 0)
+			atomicOr(c.err, 16u);
+		return;
+	}
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = ST_THREADS / 32;
 
-	// Gather the points still free in [lo, hi), in dim1 order.
+	// Gather the keys of the points still free in [lo, hi), in dim1 order.
 	if (threadIdx.x == 0)
 		s_n = 0;
 	__syncthreads();
 	for (uint32_t b = lo; b < hi; b += ST_THREADS) {
 		const uint32_t i = b + threadIdx.x;
-		const uint32_t v = i < hi ? c.r2p1[i] : 0u;
-		const uint32_t keep = v != 0;
+		const bool keep = i < hi && !c.is_taken(i);
+		const uint64_t v = keep ? c.c2s[i] : 0;
 		uint32_t tot;
-		const uint32_t off = block_excl_scan<uint32_t>(keep, &tot, ws);
+		const uint32_t off = block_excl_scan<uint32_t>(keep ? 1u : 0u, &tot, ws);
 		const uint32_t base = s_n;
-		if (keep && base + off < ST_CAP) {
+		if (keep && base + off < ST_CAP)
 			keyA[base + off] = v;
-			posA[base + off] = i;
-		}
 		__syncthreads();
 		if (threadIdx.x == 0)
 			s_n = base + tot;
@@ -418,7 +568,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 	const uint32_t h0 = (1u << L0) + j;
 	const uint32_t last_s = c.D - 1 - L0;
 	const uint32_t half = 1u << (c.D - 1);  // med exists for positions < half
-	uint32_t *kc = keyA, *pc = posA, *kn = keyB, *pn = posB;
+	uint64_t *kc = keyA, *kn = keyB;
 	uint32_t nsub = 1;
 	uint32_t present = (uint32_t) cN;
 	if (threadIdx.x == 0)
@@ -427,23 +577,32 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 	for (uint32_t s = 0;; s++) {
 		block_scan_array<uint32_t>(cnt, start, nsub, ws);
 		const bool wide = present / nsub >= 64;
-		// arg-max of every sub-node (keys are distinct dim2 ranks)
+		// arg-max of every sub-node (keys are distinct)
 		if (wide) {
 			for (uint32_t t = warp; t < nsub; t += nwarps) {
-				uint64_t bestv = 0;
+				uint64_t bk = 0;
+				uint32_t bi = 0;
 				for (uint32_t i = start[t] + lane; i < start[t + 1]; i += 32)
-					bestv = max(bestv, ((uint64_t) kc[i] << 32) | i);
+					if (kc[i] > bk) {
+						bk = kc[i];
+						bi = i;
+					}
 #pragma unroll
 				for (int o = 16; o > 0; o >>= 1) {
-					const uint64_t other = __shfl_xor_sync(0xFFFFFFFFu, bestv, o);
-					bestv = max(bestv, other);
+					const uint64_t ok = __shfl_xor_sync(0xFFFFFFFFu, bk, o);
+					const uint32_t oi = __shfl_xor_sync(0xFFFFFFFFu, bi, o);
+					if (ok > bk) {
+						bk = ok;
+						bi = oi;
+					}
 				}
 				if (lane == 0)
-					topi[t] = (uint32_t) bestv;
+					topi[t] = bi;
 			}
 		} else {
 			for (uint32_t t = threadIdx.x; t < nsub; t += ST_THREADS) {
-				uint32_t bk = 0, bi = 0;
+				uint64_t bk = 0;
+				uint32_t bi = 0;
 				for (uint32_t i = start[t]; i < start[t + 1]; i++)
 					if (kc[i] > bk) {
 						bk = kc[i];
@@ -464,7 +623,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 				if (ct > 0) {
 					occupied = true;
 					const uint32_t ti = topi[t];
-					const Point<T, HAS_ID> p = c.point_at(pc[ti]);
+					const Point<T, HAS_ID> p = c.point_of_tb(BuildCtx<T, HAS_ID>::tb_of(kc[ti]));
 					c.write_node(h, p);
 					if (h < half) {
 						T m = p.dim1;
@@ -472,7 +631,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 							uint32_t mi = start[t] + ct / 2 - 1;
 							if (ti <= mi)
 								mi++;
-							m = c.point_at(pc[mi]).dim1;
+							m = c.point_of_tb(BuildCtx<T, HAS_ID>::tb_of(kc[mi])).dim1;
 						}
 						c.med[h] = m;
 					}
@@ -502,21 +661,15 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 			for (uint32_t t = warp; t < nsub; t += nwarps) {
 				const uint32_t ti = topi[t];
 				for (uint32_t i = start[t] + lane; i < start[t + 1]; i += 32)
-					if (i != ti) {
-						const uint32_t ni = i - t - (i > ti ? 1u : 0u);
-						kn[ni] = kc[i];
-						pn[ni] = pc[i];
-					}
+					if (i != ti)
+						kn[i - t - (i > ti ? 1u : 0u)] = kc[i];
 			}
 		} else {
 			for (uint32_t t = threadIdx.x; t < nsub; t += ST_THREADS) {
 				const uint32_t ti = topi[t];
 				for (uint32_t i = start[t]; i < start[t + 1]; i++)
-					if (i != ti) {
-						const uint32_t ni = i - t - (i > ti ? 1u : 0u);
-						kn[ni] = kc[i];
-						pn[ni] = pc[i];
-					}
+					if (i != ti)
+						kn[i - t - (i > ti ? 1u : 0u)] = kc[i];
 			}
 		}
 		__syncthreads();
@@ -524,11 +677,9 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 			cnt[t] = cnt2[t];
 		present -= nsub;
 		nsub *= 2;
-		uint32_t *tk = kc, *tp = pc;
+		uint64_t *tk = kc;
 		kc = kn;
-		pc = pn;
 		kn = tk;
-		pn = tp;
 		__syncthreads();
 	}
 }
@@ -576,96 +727,116 @@ inline unsigned grid_for(uint64_t n, int threads)
 	return (unsigned) std::max<uint64_t>(1, std::min(want, cap));
 }
 
+// Scratch bytes of build_impl beyond the tree itself (kept next to build_impl so the
+// two stay in step).
+uint64_t build_scratch_bytes(pst_dtype dt, pst_idtype it, uint64_t n)
+{
+	const uint64_t ks = value_size(dt);
+	const uint64_t tiles = rs_num_tiles(n);
+	const uint64_t wide = 1ull << subtree_level(n);
+	// k1, keys_alt (ks each); c2, vals_alt (8 each); doubles: k2 (8) and the rank
+	// sort's u32 payloads (2 x 4); P (4) for non-monotone ids
+	uint64_t per_pt = 2 * ks + 16 + (dt == PST_F64 ? 16 : 0) + (it == PST_ID_U32 ? 4 : 0);
+	return n * per_pt + n / 8 + (n / TM_TILE + 1) * 8 + 256 * tiles * 4 + scan_tmp_elems(256 * tiles) * 4 +
+	       wide * 24 + (1 << 20);
+}
+
 template <typename T, bool HAS_ID>
 void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 {
 	using K = typename KeyOf<T>::K;
 	using Pt = Point<T, HAS_ID>;
+	constexpr bool WIDE_KEY = sizeof(K) == 8;  // doubles: dim2 ranks from their own sort
 	const Pt *pts = static_cast<const Pt *>(pts_d);
 	const uint32_t D = t.levels;
 
 	// ---- scratch
 	const uint64_t rs_tiles = rs_num_tiles(n);
-	DevBuf k1(n * sizeof(K), s), k2(n * sizeof(K), s), kalt(n * sizeof(K), s);
-	DevBuf valt(n * 4, s), vtmp(n * 4, s), S1b(n * 4, s), Pb(HAS_ID ? n * 4 : 0, s);
+	DevBuf k1(n * sizeof(K), s), kalt(n * sizeof(K), s), c2(n * 8, s), valt(n * 8, s);
+	DevBuf k2(WIDE_KEY ? n * 8 : 0, s), v32a(WIDE_KEY ? n * 4 : 0, s), v32b(WIDE_KEY ? n * 4 : 0, s);
+	DevBuf Pb(HAS_ID ? n * 4 : 0, s);
 	DevBuf tile_hist(256 * rs_tiles * 4, s), scan_tmp(scan_tmp_elems(256 * rs_tiles) * 4, s);
-	DevBuf hist_all(8 * 256 * 4, s), flags(64, s);
-	uint32_t *hist_host = nullptr;
-	PST_CUDA(cudaMallocHost(&hist_host, 8 * 256 * 4));
-	struct HostFree {
-		uint32_t *p;
-		~HostFree() { cudaFreeHost(p); }
-	} hf{hist_host};
+	DevBuf flags(256, s);
+	uint32_t *flag = flags.get<uint32_t>();  // [0] ids decrease, [1] error bits, [2..3] id range
+	K *krange = reinterpret_cast<K *>(flags.get<unsigned char>() + 64);  // [k1 min, k1 max, k2 min, k2 max]
+	{
+		unsigned char init[256];
+		memset(init, 0, sizeof(init));
+		const uint32_t id_init[2] = {0xFFFFFFFFu, 0u};
+		memcpy(init + 8, id_init, 8);
+		const K kinit[4] = {~K(0), K(0), ~K(0), K(0)};
+		memcpy(init + 64, kinit, sizeof(kinit));
+		PST_CUDA(cudaMemcpyAsync(flag, init, sizeof(init), cudaMemcpyHostToDevice, s));
+	}
 	SortScratch sc;
-	sc.keys_alt = kalt.p;
-	sc.vals_alt = valt.get<uint32_t>();
-	sc.vals_tmp = vtmp.get<uint32_t>();
 	sc.tile_hist = tile_hist.get<uint32_t>();
 	sc.scan_tmp = scan_tmp.get<uint32_t>();
-	sc.hist_all = hist_all.get<uint32_t>();
-	sc.hist_host = hist_host;
-	uint32_t *flag = flags.get<uint32_t>();
-	PST_CUDA(cudaMemsetAsync(flag, 0, 64, s));
 
 	const unsigned g = grid_for(n, 256);
 	// ---- tiebreak order: (id, input index) when ids are not already non-decreasing
 	const uint32_t *P = nullptr;
 	if constexpr (HAS_ID) {
-		k_ids_monotone<T, HAS_ID><<<g, 256, 0, s>>>(pts, n, flag);
-		uint32_t mono_flag = 0;
-		PST_CUDA(cudaMemcpyAsync(&mono_flag, flag, 4, cudaMemcpyDeviceToHost, s));
+		k_ids_scan<T, HAS_ID><<<g, 256, 0, s>>>(pts, n, flag, flag + 2);
+		uint32_t host[4];
+		PST_CUDA(cudaMemcpyAsync(host, flag, 16, cudaMemcpyDeviceToHost, s));
 		PST_CUDA(cudaStreamSynchronize(s));
-		if (mono_flag) {
-			uint32_t *idk = reinterpret_cast<uint32_t *>(k1.p);  // k1 is at least n*4 bytes
+		if (host[0]) {
+			uint32_t *idk = k1.get<uint32_t>();  // k1 holds at least n u32
 			k_id_keys<T, HAS_ID><<<g, 256, 0, s>>>(pts, n, idk);
-			SortScratch sc32 = sc;
+			SortScratch s32 = sc;
+			s32.keys_alt = kalt.p;
+			s32.vals_alt = valt.p;           // n u32 fit in the u64 buffers
+			s32.vals_tmp = c2.p;
 			uint32_t *kres, *vres;
-			radix_sort<uint32_t>(idk, nullptr, n, sc32, &kres, &vres, s);
-			// vres == null: every digit pass was trivial, i.e. all ids equal; then
-			// (id, index) order is index order and P stays the identity.
-			if (vres) {
-				PST_CUDA(cudaMemcpyAsync(Pb.p, vres, n * 4, cudaMemcpyDeviceToDevice, s));
-				P = Pb.get<uint32_t>();
-			}
+			radix_sort<uint32_t, uint32_t>(idk, nullptr, n, rs_passes<uint32_t>(host[2], host[3]), s32, &kres, &vres, s);
+			// ids decrease somewhere, so they are not all equal and the sort ran
+			PST_CUDA(cudaMemcpyAsync(Pb.p, vres, n * 4, cudaMemcpyDeviceToDevice, s));
+			P = Pb.get<uint32_t>();
 		}
 	}
-	// ---- dim1 and dim2 orders
-	k_value_keys<T, HAS_ID><<<g, 256, 0, s>>>(pts, P, n, k1.get<K>(), k2.get<K>());
+	// ---- keys in tiebreak order
+	k_prep_keys<T, HAS_ID><<<g, 256, 0, s>>>(pts, P, n, k1.get<K>(), c2.get<uint64_t>(), k2.get<K>(), krange);
 	PST_CUDA(cudaGetLastError());
-	K *kres;
-	uint32_t *vres;
-	radix_sort<K>(k1.get<K>(), nullptr, n, sc, &kres, &vres, s);
-	// A null payload result means all keys were equal: the order is the identity.
-	uint32_t *S1 = S1b.get<uint32_t>();
-	if (vres)
-		PST_CUDA(cudaMemcpyAsync(S1, vres, n * 4, cudaMemcpyDeviceToDevice, s));
-	else
-		k_iota<<<g, 256, 0, s>>>(S1, n);
-	radix_sort<K>(k2.get<K>(), nullptr, n, sc, &kres, &vres, s);
-	if (!vres) {
-		vres = valt.get<uint32_t>();
-		k_iota<<<g, 256, 0, s>>>(vres, n);
+	K range[4];
+	PST_CUDA(cudaMemcpyAsync(range, krange, sizeof(range), cudaMemcpyDeviceToHost, s));
+	PST_CUDA(cudaStreamSynchronize(s));
+	if constexpr (WIDE_KEY) {
+		// dim2 ranks: stable sort of the dim2 keys in tiebreak order
+		SortScratch s2 = sc;
+		s2.keys_alt = kalt.p;
+		s2.vals_alt = v32a.p;
+		s2.vals_tmp = v32b.p;
+		K *kres;
+		uint32_t *S2;
+		radix_sort<K, uint32_t>(k2.get<K>(), nullptr, n, rs_passes<K>(range[2], range[3]), s2, &kres, &S2, s);
+		k_rank_keys<<<g, 256, 0, s>>>(S2, n, c2.get<uint64_t>());
+		PST_CUDA(cudaGetLastError());
 	}
-	// vres: dim2-sorted position -> tiebreak rank (S2).  k1's storage is free now.
-	uint32_t *rank2_of_tb = reinterpret_cast<uint32_t *>(k1.p);
-	k_rank_scatter<<<g, 256, 0, s>>>(vres, n, rank2_of_tb);
-	uint32_t *r2p1 = reinterpret_cast<uint32_t *>(kalt.p);
-	if (reinterpret_cast<void *>(vres) == kalt.p)
-		fail(PST_ERR_INTERNAL, "scratch aliasing");
-	uint32_t *pos_of_rank2 = vres == valt.get<uint32_t>() ? vtmp.get<uint32_t>() : valt.get<uint32_t>();
-	k_sorted_ranks<<<g, 256, 0, s>>>(S1, rank2_of_tb, n, r2p1, pos_of_rank2);
-	PST_CUDA(cudaGetLastError());
+	// ---- dim1 order, carrying the dim2 keys
+	K *k1s;
+	uint64_t *c2s;
+	{
+		SortScratch s1 = sc;
+		s1.keys_alt = kalt.p;
+		s1.vals_alt = valt.p;
+		radix_sort<K, uint64_t>(k1.get<K>(), c2.get<uint64_t>(), n, rs_passes<K>(range[0], range[1]), s1, &k1s, &c2s,
+		                        s);
+	}
 
 	// ---- levels
 	const uint32_t L0 = std::min(subtree_level(n), D - 1);
 	const uint64_t nodes_wide = 1ull << L0;
-	DevBuf Ba((nodes_wide + 1) * 4, s), Bb((nodes_wide + 1) * 4, s), bestb(nodes_wide * 4, s), topb(nodes_wide * 4, s);
+	const uint64_t ntiles = (n + TM_TILE - 1) / TM_TILE;
+	DevBuf Ba((nodes_wide + 1) * 4, s), Bb((nodes_wide + 1) * 4, s), bestb(nodes_wide * 8, s),
+	    topb(nodes_wide * 4, s), takenb(((n + 31) / 32) * 4, s), tmaxb(L0 ? ntiles * 8 : 0, s);
+	PST_CUDA(cudaMemsetAsync(takenb.p, 0, ((n + 31) / 32) * 4, s));
 	BuildCtx<T, HAS_ID> c;
 	c.pts = pts;
 	c.P = P;
-	c.S1 = S1;
-	c.r2p1 = r2p1;
-	c.pos_of_rank2 = pos_of_rank2;
+	c.k1s = k1s;
+	c.c2s = c2s;
+	c.taken = takenb.get<uint32_t>();
+	c.tmax = tmaxb.get<uint64_t>();
 	c.dim1 = as<T>(t.dim1);
 	c.dim2 = as<T>(t.dim2);
 	c.med = as<T>(t.med);
@@ -680,17 +851,25 @@ void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 		const uint32_t b0[2] = {0u, (uint32_t) n};
 		PST_CUDA(cudaMemcpyAsync(B, b0, 8, cudaMemcpyHostToDevice, s));
 	}
-	const uint64_t am_tiles = (n + AM_TILE - 1) / AM_TILE;
-	const uint64_t am_ctas_max = (uint64_t) device_info().sms * 8;
-	const uint64_t tiles_per_cta = (am_tiles + am_ctas_max - 1) / am_ctas_max;
-	const unsigned am_grid = (unsigned) ((am_tiles + tiles_per_cta - 1) / tiles_per_cta);
-	for (uint32_t d = 0; d < L0; d++) {
-		const uint32_t nseg = 1u << d;
-		PST_CUDA(cudaMemsetAsync(bestb.p, 0, nseg * 4, s));
-		k_level_argmax<<<am_grid, AM_THREADS, 0, s>>>(r2p1, n, B, nseg, bestb.get<uint32_t>(), tiles_per_cta);
-		k_level_nodes<T, HAS_ID><<<(nseg + 127) / 128, 128, 0, s>>>(c, d, B, Bn, bestb.get<uint32_t>());
-		PST_CUDA(cudaGetLastError());
-		std::swap(B, Bn);
+	if (L0) {
+		const unsigned tgrid = (unsigned) std::max<uint64_t>(
+		    1, std::min<uint64_t>((ntiles + AM_THREADS / 32 - 1) / (AM_THREADS / 32), (uint64_t) device_info().sms * 8));
+		k_tile_max_all<<<tgrid, AM_THREADS, 0, s>>>(c2s, c.taken, n, c.tmax);
+		const unsigned am_grid = (unsigned) std::max<uint64_t>(
+		    1, std::min<uint64_t>((ntiles + AM_THREADS - 1) / AM_THREADS, (uint64_t) device_info().sms * 8));
+		for (uint32_t d = 0; d < L0; d++) {
+			const uint32_t nseg = 1u << d;
+			PST_CUDA(cudaMemsetAsync(bestb.p, 0, (size_t) nseg * 8, s));
+			k_level_argmax<<<am_grid, AM_THREADS, 0, s>>>(c2s, c.taken, c.tmax, n, B, nseg,
+			                                              bestb.get<unsigned long long>(), c.err);
+			k_level_nodes<T, HAS_ID><<<(nseg + 127) / 128, 128, 0, s>>>(c, d, B, Bn,
+			                                                            bestb.get<unsigned long long>());
+			if (d + 1 < L0)
+				k_tile_refresh<<<(unsigned) ((nseg * 32 + AM_THREADS - 1) / AM_THREADS), AM_THREADS, 0, s>>>(
+				    c2s, c.taken, n, c.top_pos, d, c.tmax, c.err);
+			PST_CUDA(cudaGetLastError());
+			std::swap(B, Bn);
+		}
 	}
 	PST_CUDA(cudaFuncSetAttribute(k_subtree<T, HAS_ID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 	                              (int) st_smem_bytes()));
@@ -709,12 +888,7 @@ uint64_t tree_bytes(pst_dtype dt, pst_idtype it, uint64_t n) { return tree_layou
 
 uint64_t build_bytes_needed(pst_dtype dt, pst_idtype it, uint64_t n)
 {
-	const uint64_t ks = value_size(dt);
-	const uint64_t tiles = rs_num_tiles(n);
-	const uint64_t wide = 1ull << subtree_level(n);
-	const uint64_t scratch = n * (3 * ks + 3 * 4 + (it == PST_ID_U32 ? 4 : 0)) + 256 * tiles * 4 +
-	                         scan_tmp_elems(256 * tiles) * 4 + wide * 16 + (1 << 20);
-	return tree_bytes(dt, it, n) + scratch;
+	return tree_bytes(dt, it, n) + build_scratch_bytes(dt, it, n);
 }
 
 void build_tree(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)

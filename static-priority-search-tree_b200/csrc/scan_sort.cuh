@@ -129,46 +129,32 @@ void exclusive_scan(const T *in, U *out, uint64_t n, T *tmp, T *total_d, cudaStr
 
 // ---------------------------------------------------------------------------
 // LSD radix sort, 8-bit digits, 4096-key tiles.  Stable: within a tile keys are
-// ranked in input order with __match_any_sync over warp-private digit counters,
-// and tiles take their digit offsets from a digit-major exclusive scan.
+// ranked in input order (warp-private digit counters; the lanes of a warp holding
+// the same digit are found with eight ballots, one per digit bit), and tiles take
+// their digit offsets from a digit-major exclusive scan.  Only the passes that
+// cover bits where the keys differ are run: keys between kmin and kmax share
+// every bit above the highest bit of kmin ^ kmax.
 
 constexpr int RS_THREADS = 256;
 constexpr int RS_ITEMS = 16;
 constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
 constexpr int RS_WARPS = RS_THREADS / 32;
+static_assert(RS_THREADS == 256, "one thread per digit in the digit scans");
 
 template <typename K>
 __device__ __forceinline__ uint32_t rs_digit(K k, int shift) { return (uint32_t) (k >> shift) & 0xFFu; }
 
-// Digit histograms of every pass at once: hist[pass * 256 + digit].
-template <typename K>
-__global__ void __launch_bounds__(256) k_rs_hist_all(const K *keys, uint64_t n, uint32_t *hist)
+// Mask of the valid lanes of this warp that hold the same digit as this lane.
+__device__ __forceinline__ uint32_t rs_peers(uint32_t d, bool valid)
 {
-	constexpr int P = sizeof(K);
-	__shared__ uint32_t sh[P][256];
-	for (int i = threadIdx.x; i < P * 256; i += blockDim.x)
-		(&sh[0][0])[i] = 0;
-	__syncthreads();
-	// The loop bound is uniform across the block so that whole warps stay converged
-	// for __match_any_sync; lanes past the end use the out-of-range digit 256.
-	for (uint64_t b = (uint64_t) blockIdx.x * blockDim.x; b < n; b += (uint64_t) gridDim.x * blockDim.x) {
-		const uint64_t i = b + threadIdx.x;
-		const bool valid = i < n;
-		const K k = valid ? keys[i] : K(0);
+	uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);
 #pragma unroll
-		for (int p = 0; p < P; p++) {
-			const uint32_t d = valid ? rs_digit(k, 8 * p) : 256u;
-			const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-			if (valid && (threadIdx.x & 31) == (uint32_t) (__ffs(peers) - 1))
-				atomicAdd(&sh[p][d], (uint32_t) __popc(peers));
-		}
+	for (int b = 0; b < 8; b++) {
+		const bool bit = (d >> b) & 1u;
+		const uint32_t m = __ballot_sync(0xFFFFFFFFu, bit);
+		peers &= bit ? m : ~m;
 	}
-	__syncthreads();
-	for (int i = threadIdx.x; i < P * 256; i += blockDim.x) {
-		uint32_t v = (&sh[0][0])[i];
-		if (v)
-			atomicAdd(&hist[i], v);
-	}
+	return peers;
 }
 
 // Per-tile digit counts, digit-major: tile_hist[digit * num_tiles + tile].
@@ -185,11 +171,8 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const K *keys, uint64
 #pragma unroll 4
 	for (int i = 0; i < RS_ITEMS; i++) {
 		const uint64_t idx = t0 + (uint64_t) warp * (RS_ITEMS * 32) + i * 32 + lane;
-		const bool valid = idx < n;
-		const uint32_t d = valid ? rs_digit(keys[idx], shift) : 256u;
-		const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-		if (valid && lane == __ffs(peers) - 1)
-			h[warp][d] += __popc(peers);
+		if (idx < n)
+			atomicAdd(&h[warp][rs_digit(keys[idx], shift)], 1u);
 	}
 	__syncthreads();
 	uint32_t s = 0;
@@ -199,19 +182,20 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const K *keys, uint64
 	tile_hist[(uint64_t) threadIdx.x * num_tiles + blockIdx.x] = s;
 }
 
-// vals_in == nullptr means the identity payload (the key's input index).
-template <typename K>
-__global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const K *keys_in, const uint32_t *vals_in, K *keys_out,
-                                                             uint32_t *vals_out, uint64_t n, int shift,
+// One pass.  vals_in == nullptr means the identity payload (the key's input index;
+// 32-bit payloads only).
+template <typename K, typename V>
+__global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const K *keys_in, const V *vals_in, K *keys_out,
+                                                             V *vals_out, uint64_t n, int shift,
                                                              const uint32_t *tile_off, uint32_t num_tiles)
 {
 	extern __shared__ __align__(16) unsigned char rs_smem[];
-	K *sk = reinterpret_cast<K *>(rs_smem);
-	uint32_t *sv = reinterpret_cast<uint32_t *>(sk + RS_TILE);
-	uint32_t *whist = sv + RS_TILE;          // [RS_WARPS][256]
-	uint32_t *dstart = whist + RS_WARPS * 256; // [256] tile-local digit start
-	uint32_t *gbase = dstart + 256;           // [256] global start of the digit for this tile
-	uint32_t *wsum = gbase + 256;             // [33]
+	V *sv = reinterpret_cast<V *>(rs_smem);
+	K *sk = reinterpret_cast<K *>(sv + RS_TILE);
+	uint32_t *whist = reinterpret_cast<uint32_t *>(sk + RS_TILE);  // [RS_WARPS][256]
+	uint32_t *dstart = whist + RS_WARPS * 256;                      // [256] tile-local digit start
+	uint32_t *gbase = dstart + 256;                                 // [256] global start of the digit for this tile
+	uint32_t *wsum = gbase + 256;                                   // [33]
 
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	for (int i = threadIdx.x; i < RS_WARPS * 256; i += RS_THREADS)
@@ -221,17 +205,17 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const K *keys_in, c
 
 	const uint64_t t0 = (uint64_t) blockIdx.x * RS_TILE;
 	K k[RS_ITEMS];
-	uint32_t v[RS_ITEMS];
+	V v[RS_ITEMS];
 	uint32_t loc[RS_ITEMS];
 #pragma unroll
 	for (int i = 0; i < RS_ITEMS; i++) {
 		const uint64_t idx = t0 + (uint64_t) warp * (RS_ITEMS * 32) + i * 32 + lane;
 		const bool valid = idx < n;
 		k[i] = valid ? keys_in[idx] : K(0);
-		v[i] = valid ? (vals_in ? vals_in[idx] : (uint32_t) idx) : 0u;
-		const uint32_t d = valid ? rs_digit(k[i], shift) : 256u;
-		const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-		const int leader = __ffs(peers) - 1;
+		v[i] = valid ? (vals_in ? vals_in[idx] : (V) idx) : V(0);
+		const uint32_t d = rs_digit(k[i], shift);
+		const uint32_t peers = rs_peers(d, valid);
+		const int leader = valid ? __ffs(peers) - 1 : lane;
 		uint32_t old = 0;
 		if (valid && lane == leader) {
 			old = whist[warp * 256 + d];
@@ -239,6 +223,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const K *keys_in, c
 		}
 		old = __shfl_sync(0xFFFFFFFFu, old, leader);
 		loc[i] = old + __popc(peers & lanemask_lt());
+		__syncwarp();  // the next item's leaders read the counters written here
 	}
 	__syncthreads();
 	// Exclusive prefix of each digit over warps, then over digits.
@@ -277,72 +262,64 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const K *keys_in, c
 	}
 }
 
-template <typename K>
+template <typename K, typename V>
 constexpr size_t rs_downsweep_smem()
 {
-	return RS_TILE * (sizeof(K) + 4) + (RS_WARPS * 256 + 256 + 256 + 33) * 4;
+	return RS_TILE * (sizeof(K) + sizeof(V)) + (RS_WARPS * 256 + 256 + 256 + 33) * 4;
 }
-
-// Scratch for radix_sort: key/value ping-pong buffers of n entries plus the
-// tile histogram and its scan temporaries.
-struct SortScratch {
-	void *keys_alt = nullptr;
-	uint32_t *vals_alt = nullptr;
-	uint32_t *vals_tmp = nullptr;  // second payload buffer when the input payload must be kept
-	uint32_t *tile_hist = nullptr;
-	uint32_t *scan_tmp = nullptr;
-	uint32_t *hist_all = nullptr;  // [8 * 256]
-	uint32_t *hist_host = nullptr; // pinned [8 * 256]
-};
 
 inline uint64_t rs_num_tiles(uint64_t n) { return (n + RS_TILE - 1) / RS_TILE; }
 
-// Sorts (keys, vals) ascending by key, stably.  `keys`/`vals` hold the input
-// (vals may be null: identity payload) and on return hold the sorted result in
-// the buffers returned through *keys_res / *vals_res (either the input buffers or
-// the scratch ping-pong buffers).  Passes whose digit is constant are skipped
-// (one host round trip for the all-pass histogram).
+// Scratch for radix_sort: key/value ping-pong buffers of n entries plus the tile
+// histogram and its scan temporaries.
+struct SortScratch {
+	void *keys_alt = nullptr;  // n keys
+	void *vals_alt = nullptr;  // n payloads
+	void *vals_tmp = nullptr;  // n payloads (second buffer for an identity input payload)
+	uint32_t *tile_hist = nullptr;
+	uint32_t *scan_tmp = nullptr;
+};
+
+// Number of 8-bit passes needed to sort keys lying in [kmin, kmax].
 template <typename K>
-void radix_sort(K *keys, uint32_t *vals, uint64_t n, SortScratch &sc, K **keys_res, uint32_t **vals_res,
-                cudaStream_t s)
+inline int rs_passes(K kmin, K kmax)
+{
+	const uint64_t diff = (uint64_t) (kmin ^ kmax);
+	if (!diff)
+		return 0;
+	int bits = 64 - __builtin_clzll(diff);
+	return (bits + 7) / 8;
+}
+
+// Sorts (keys, vals) ascending by key, stably, over the first `passes` digits.
+// vals may be null (identity payload, 32-bit payloads only).  The sorted data is in
+// the buffers returned through *keys_res / *vals_res (the input buffers or the
+// scratch ones; *vals_res stays null when passes == 0 and vals is null).
+template <typename K, typename V>
+void radix_sort(K *keys, V *vals, uint64_t n, int passes, SortScratch &sc, K **keys_res, V **vals_res, cudaStream_t s)
 {
 	*keys_res = keys;
 	*vals_res = vals;
-	if (n == 0)
+	if (n == 0 || passes == 0)
 		return;
-	constexpr int P = sizeof(K);
 	const uint64_t tiles = rs_num_tiles(n);
-	PST_CUDA(cudaMemsetAsync(sc.hist_all, 0, P * 256 * sizeof(uint32_t), s));
-	const int sms = device_info().sms;
-	k_rs_hist_all<K><<<(unsigned) std::min<uint64_t>((n + 255) / 256, (uint64_t) sms * 8), 256, 0, s>>>(keys, n, sc.hist_all);
-	PST_CUDA(cudaGetLastError());
-	PST_CUDA(cudaMemcpyAsync(sc.hist_host, sc.hist_all, P * 256 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-	PST_CUDA(cudaStreamSynchronize(s));
-
-	PST_CUDA(cudaFuncSetAttribute(k_rs_downsweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-	                              (int) rs_downsweep_smem<K>()));
+	PST_CUDA(cudaFuncSetAttribute(k_rs_downsweep<K, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                              (int) rs_downsweep_smem<K, V>()));
 	K *kin = keys, *kout = static_cast<K *>(sc.keys_alt);
-	uint32_t *vin = vals;
-	uint32_t *vout = sc.vals_alt;
-	for (int p = 0; p < P; p++) {
-		bool trivial = false;
-		for (int d = 0; d < 256; d++)
-			if (sc.hist_host[p * 256 + d] == n)
-				trivial = true;
-		if (trivial)
-			continue;
+	V *vin = vals;
+	V *vout = static_cast<V *>(sc.vals_alt);
+	for (int p = 0; p < passes; p++) {
 		k_rs_upsweep<K><<<(unsigned) tiles, RS_THREADS, 0, s>>>(kin, n, 8 * p, sc.tile_hist, (uint32_t) tiles);
 		exclusive_scan<uint32_t>(sc.tile_hist, sc.tile_hist, 256 * tiles, sc.scan_tmp, nullptr, s);
-		k_rs_downsweep<K><<<(unsigned) tiles, RS_THREADS, rs_downsweep_smem<K>(), s>>>(kin, vin, kout, vout, n, 8 * p,
-		                                                                                sc.tile_hist, (uint32_t) tiles);
+		k_rs_downsweep<K, V><<<(unsigned) tiles, RS_THREADS, rs_downsweep_smem<K, V>(), s>>>(
+		    kin, vin, kout, vout, n, 8 * p, sc.tile_hist, (uint32_t) tiles);
 		PST_CUDA(cudaGetLastError());
-		// ping-pong; an identity (null) input payload is replaced by vals_tmp
 		K *kt = kin;
 		kin = kout;
 		kout = kt;
-		uint32_t *vt = vin;
+		V *vt = vin;
 		vin = vout;
-		vout = vt ? vt : sc.vals_tmp;
+		vout = vt ? vt : static_cast<V *>(sc.vals_tmp);
 	}
 	*keys_res = kin;
 	*vals_res = vin;

@@ -607,19 +607,29 @@ void Batch::init(TreeStorage *t, const pst_batch_opts &o)
 	PST_CUDA(cudaMallocHost((void **) &q_stage, (size_t) max_q * sizeof(pst_query)));
 	memset(ctl_host, 0, sizeof(BatchCtl));
 	const uint64_t want = o.task_capacity ? o.task_capacity : std::max<uint64_t>(1ull << 16, (uint64_t) max_q * 64);
-	grow_tasks(want);
+	grow_tasks(want, 0);
+	PST_CUDA(cudaStreamSynchronize(0));
 }
 
-void Batch::grow_tasks(uint64_t cap)
+void Batch::grow_tasks(uint64_t cap, cudaStream_t s)
 {
+	// Stream-ordered on `s` (the stream of every pass that used the old frontier), so
+	// a growth does not wait for work on the device's other streams.
 	if (rec_pq)
-		cudaFree(rec_pq);
+		PST_CUDA(cudaFreeAsync(rec_pq, s));
 	if (rec_am)
-		cudaFree(rec_am);
+		PST_CUDA(cudaFreeAsync(rec_am, s));
 	rec_pq = nullptr;
 	rec_am = nullptr;
-	dmalloc((void **) &rec_pq, cap * sizeof(uint2));
-	dmalloc((void **) &rec_am, cap * 4);
+	for (auto pb : {std::make_pair((void **) &rec_pq, cap * sizeof(uint2)), std::make_pair((void **) &rec_am, cap * 4)}) {
+		cudaError_t e = cudaMallocAsync(pb.first, std::max<size_t>(pb.second, 16), s);
+		if (e == cudaErrorMemoryAllocation) {
+			cudaGetLastError();
+			task_cap = 0;
+			fail(PST_ERR_NOMEM, "frontier allocation of " + std::to_string(pb.second) + " B failed");
+		}
+		check_cuda(e, "cudaMallocAsync(frontier)");
+	}
 	task_cap = cap;
 	if (graph_exec) {
 		cudaGraphExecDestroy(graph_exec);
@@ -779,7 +789,7 @@ void Batch::count_sync(cudaStream_t s, uint64_t *total)
 		}
 		if (attempt > 8)
 			fail(PST_ERR_INTERNAL, "frontier did not fit after growth");
-		grow_tasks(std::max<uint64_t>(h.need_tasks + h.need_tasks / 4, task_cap * 2));
+		grow_tasks(std::max<uint64_t>(h.need_tasks + h.need_tasks / 4, task_cap * 2), s);
 	}
 }
 

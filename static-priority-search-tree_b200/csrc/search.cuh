@@ -60,7 +60,7 @@ struct Batch {
 	~Batch();
 	void init(TreeStorage *t, const pst_batch_opts &o);
 	void release();
-	void grow_tasks(uint64_t cap);
+	void grow_tasks(uint64_t cap, cudaStream_t s);
 	void stage_queries(const pst_query *q, uint32_t nq, bool on_device, cudaStream_t s);
 	void launch_count(cudaStream_t s);
 	void count_sync(cudaStream_t s, uint64_t *total);

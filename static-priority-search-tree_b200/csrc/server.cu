@@ -45,22 +45,30 @@ struct Request {
 	std::vector<unsigned char> result;
 };
 
-// First-fit allocator over one device allocation (offsets, 256-byte granules).
+// First-fit allocator over one device allocation (offsets, 256-byte granules).  When
+// results go to host memory, a pinned host buffer of the same size mirrors it: a
+// batch's results are copied to the same offsets there, so staging never allocates
+// while requests wait.
 struct Arena {
 	char *base = nullptr;
+	unsigned char *host = nullptr;
 	uint64_t size = 0, used = 0, peak = 0;
 	std::map<uint64_t, uint64_t> free_;  // offset -> length
 
-	void init(uint64_t bytes)
+	void init(uint64_t bytes, bool host_mirror)
 	{
 		size = (bytes + 255) / 256 * 256;
 		check_cuda(cudaMalloc(&base, size), "cudaMalloc(result arena)");
+		if (host_mirror)
+			check_cuda(cudaMallocHost((void **) &host, size), "cudaMallocHost(result staging)");
 		free_[0] = size;
 	}
 	~Arena()
 	{
 		if (base)
 			cudaFree(base);
+		if (host)
+			cudaFreeHost(host);
 	}
 	bool alloc(uint64_t bytes, uint64_t *off)
 	{
@@ -112,8 +120,6 @@ struct Slot {
 	BatchCtl *ctl_h = nullptr;
 	uint64_t *counts_h = nullptr;
 	uint64_t *offs_h = nullptr;
-	unsigned char *stage_h = nullptr;
-	uint64_t stage_cap = 0;
 	uint64_t out_off = 0, out_bytes = 0;
 	uint64_t total = 0;
 
@@ -129,8 +135,6 @@ struct Slot {
 			cudaFreeHost(counts_h);
 		if (offs_h)
 			cudaFreeHost(offs_h);
-		if (stage_h)
-			cudaFreeHost(stage_h);
 	}
 };
 
@@ -232,7 +236,7 @@ struct Server {
 			if (c.flags & BATCH_FLAG_TASK_OVERFLOW) {
 				// the pass stopped at the first level that overflowed, so deeper
 				// levels will want more: grow generously
-				sl.eng.grow_tasks(std::max<uint64_t>(c.need_tasks * 2, sl.eng.task_cap * 2));
+				sl.eng.grow_tasks(std::max<uint64_t>(c.need_tasks * 2, sl.eng.task_cap * 2), sl.stream);
 				launch_count(sl);
 				return true;
 			}
@@ -273,18 +277,11 @@ struct Server {
 			}
 			if (!arena.alloc(sl.out_bytes, &sl.out_off))
 				return false;  // admitted once results in flight free up
-			if (opts.keep_results && sl.stage_cap < sl.out_bytes) {
-				if (sl.stage_h)
-					cudaFreeHost(sl.stage_h);
-				sl.stage_h = nullptr;
-				sl.stage_cap = std::max<uint64_t>(sl.out_bytes, sl.stage_cap * 2);
-				check_cuda(cudaMallocHost((void **) &sl.stage_h, sl.stage_cap), "cudaMallocHost(result staging)");
-			}
 			sl.eng.enqueue_emit(sl.ret, arena.base + sl.out_off, sl.total, sl.stream);
 			check_cuda(cudaMemcpyAsync(sl.offs_h, sl.eng.offsets, ((size_t) n + 1) * 8, cudaMemcpyDeviceToHost,
 			                           sl.stream), "copy offsets");
 			if (opts.keep_results)
-				check_cuda(cudaMemcpyAsync(sl.stage_h, arena.base + sl.out_off, sl.out_bytes, cudaMemcpyDeviceToHost,
+				check_cuda(cudaMemcpyAsync(arena.host + sl.out_off, arena.base + sl.out_off, sl.out_bytes, cudaMemcpyDeviceToHost,
 				                           sl.stream), "copy results");
 			check_cuda(cudaMemcpyAsync(sl.ctl_h, sl.eng.ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, sl.stream),
 			           "copy control");
@@ -297,19 +294,21 @@ struct Server {
 			return true;
 		}
 		// SLOT_EMITTING done
-		arena.release(sl.out_off, sl.out_bytes);
 		if (sl.ctl_h->flags & (BATCH_FLAG_OUT_OVERFLOW | BATCH_FLAG_INTERNAL | BATCH_FLAG_TASK_OVERFLOW)) {
+			arena.release(sl.out_off, sl.out_bytes);
 			fail_all(sl, PST_ERR_INTERNAL);
 			return true;
 		}
 		const uint64_t rs = sl.eng.record_size(sl.ret);
+		const unsigned char *staged = arena.host ? arena.host + sl.out_off : nullptr;
 		for (uint32_t i = 0; i < n; i++) {
 			const uint64_t a = sl.offs_h[i], b = sl.offs_h[i + 1];
 			std::vector<unsigned char> res;
 			if (opts.keep_results == 1)
-				res.assign(sl.stage_h + a * rs, sl.stage_h + b * rs);
+				res.assign(staged + a * rs, staged + b * rs);
 			finish(sl.reqs[i], PST_OK, b - a, std::move(res));
 		}
+		arena.release(sl.out_off, sl.out_bytes);
 		{
 			std::lock_guard<std::mutex> lk(mu);
 			st.batches++;
@@ -413,7 +412,7 @@ Server *server_create(const pst_server_opts &o)
 	if (!s->opts.out_budget_bytes)
 		s->opts.out_budget_bytes = 1ull << 30;
 	check_cuda(cudaGetDevice(&s->device), "cudaGetDevice");
-	s->arena.init(s->opts.out_budget_bytes);
+	s->arena.init(s->opts.out_budget_bytes, s->opts.keep_results != 0);
 	s->start();
 	return s.release();
 }
