@@ -166,6 +166,109 @@ def blob_volume_device(px, py, pz, seed, torch, nblobs=32, noise=0.01):
     return vol
 
 
+# ---------------------------------------------------------------------------
+# large random trees: every value type, kind and selectivity (run with --sweep)
+
+SWEEP_TYPES = (("f32", True), ("f64", True), ("i32", True), ("f32", False))
+SWEEP_SEL = (1e-5, 1e-3, 1e-1)
+SWEEP_BATCH = 32
+
+
+def gen_points_typed(n, seed, dt, has_id, torch):
+    """PointStruct records of dim1 ~U[0,2^24), dim2 = dim1 + U[0,2^16) in the value type
+    (integer-valued draws for i32), ids 0..n-1; returned as a byte tensor."""
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    if dt == "i32":
+        d1 = torch.randint(0, 1 << 24, (n,), generator=g, device="cuda", dtype=torch.int32)
+        d2 = d1 + torch.randint(0, 1 << 16, (n,), generator=g, device="cuda", dtype=torch.int32)
+    else:
+        tt = torch.float32 if dt == "f32" else torch.float64
+        d1 = torch.rand(n, generator=g, device="cuda", dtype=tt) * float(1 << 24)
+        d2 = d1 + torch.rand(n, generator=g, device="cuda", dtype=tt) * float(1 << 16)
+    wide = dt == "f64"
+    it = torch.int64 if wide else torch.int32
+    rec = torch.zeros((n, 3 if has_id else 2), dtype=it, device="cuda")
+    rec[:, 0] = d1.view(it)
+    rec[:, 1] = d2.view(it)
+    if has_id:
+        rec[:, 2] = torch.arange(n, device="cuda", dtype=it)  # id in the low word, padding zero
+    del d1, d2
+    return rec
+
+
+def sweep(pst, torch, n, seed=1):
+    """Per value type: build, then for each kind and selectivity a batch of 32 queries
+    calibrated to s * n points each: batched pass time and one plain query."""
+    out = []
+    rng = np.random.default_rng(seed)
+    for dt, has_id in SWEEP_TYPES:
+        vs = 8 if dt == "f64" else 4
+        pts = gen_points_typed(n, seed, dt, has_id, torch)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tree = pst.StaticPSTGPU(pts, n, dt, has_id)
+        torch.cuda.synchronize()
+        build_ms = 1000 * (time.perf_counter() - t0)
+        del pts
+        torch.cuda.empty_cache()
+        ret = "ids" if has_id else "points"
+        rec_bytes = 4 if has_id else 2 * vs
+        # read dim1, dim2 (+ id) per reported point, write the record
+        bpp = 2 * vs + (4 if has_id else 0) + rec_bytes
+        eng = pst.BatchEngine(tree, max_queries=SWEEP_BATCH)
+        for kind in (0, 1, 2):
+            for s in SWEEP_SEL:
+                kinds = np.full(SWEEP_BATCH, kind, np.int32)
+                anchor = rng.uniform(0, (1 << 24) * (1 - 4 * s), SWEEP_BATCH)
+                sel = np.full(SWEEP_BATCH, s)
+
+                def count_fn(k, a, b, c):
+                    if dt == "i32":
+                        a, b, c = (np.round(x).astype(np.int32) for x in (a, b, c))
+                    counts, _ = eng.count(pst.make_queries(k, a, b, c, dt))
+                    return counts.cpu().numpy()
+                a, b, c = calibrate(count_fn, kinds, sel, anchor, n)
+                if dt == "i32":
+                    a, b, c = (np.round(x).astype(np.int32) for x in (a, b, c))
+                q = pst.make_queries(kinds, a, b, c, dt)
+                counts, total = eng.count(q)
+                qd = torch.from_numpy(q.view(np.uint8).copy()).to("cuda")
+                buf = torch.empty(total * rec_bytes + 16, dtype=torch.uint8, device="cuda")
+                offs = torch.empty(SWEEP_BATCH + 1, dtype=torch.int64, device="cuda")
+                for _ in range(3):
+                    eng.run(qd, buf, offs, ret=ret, queries_on_device=True, sync=True)
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+                reps = 5
+                ev[0].record()
+                for _ in range(reps):
+                    eng.run(qd, buf, offs, ret=ret, queries_on_device=True, sync=False)
+                ev[1].record()
+                ev[1].synchronize()
+                ms = ev[0].elapsed_time(ev[1]) / reps
+                # one plain drop-in query (callee-allocated result), wall clock
+                name = {0: "three", 1: "left", 2: "right"}[kind]
+                args = (float(a[0]), float(b[0]), float(c[0])) if dt != "i32" else (int(a[0]), int(b[0]), int(c[0]))
+                tree.search(name, *args, ret=ret)
+                torch.cuda.synchronize()
+                t1 = time.perf_counter()
+                k1 = len(tree.search(name, *args, ret=ret))
+                plain_s = time.perf_counter() - t1
+                row = {"dtype": dt, "ids": has_id, "kind": name, "sel": s, "queries": SWEEP_BATCH,
+                       "mean_points": total / SWEEP_BATCH, "batch_ms": ms, "pts_per_s": total / (ms / 1000),
+                       "gbs": total * bpp / (ms / 1000) / 1e9, "bytes_per_pt": bpp, "build_ms": build_ms,
+                       "plain_query_ms": plain_s * 1000, "plain_pts_per_s": k1 / plain_s if plain_s else None}
+                out.append(row)
+                log(f"sweep {dt}{'' if has_id else '-noid'} {name:5s} s={s:g}: {total / SWEEP_BATCH:.3g} pts/query, "
+                    f"batch {ms:.3f} ms = {row['pts_per_s']:.3g} pts/s ({row['gbs']:.0f} GB/s), "
+                    f"plain {plain_s * 1000:.1f} ms")
+                del buf, qd
+        eng.close()
+        tree.close()
+        torch.cuda.empty_cache()
+    return out
+
+
 SERVING_VOLUMES = [(64, 64, 64), (128, 128, 128), (192, 192, 192), (256, 256, 256), (384, 384, 384),
                    (512, 512, 512), (768, 768, 512), (1024, 1024, 512)]
 
@@ -377,6 +480,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--plain-queries", type=int, default=256)
+    ap.add_argument("--sweep", action="store_true", help="also run every value type x kind x selectivity")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -514,6 +618,15 @@ def main():
         except Exception:
             pass
 
+    sweep_rows = None
+    if rank == 0 and args.sweep:
+        eng.close()
+        tree.close()
+        torch.cuda.empty_cache()
+        sweep_rows = sweep(pst, torch, n)
+        tree = pst.StaticPSTGPU(gen_points_device(n, seed=1 + rank, torch=torch), n, "f32", True)
+        eng = pst.BatchEngine(tree, max_queries=NQ)
+
     serving = None
     if rank == 0 and not args.no_serving:
         try:
@@ -551,6 +664,8 @@ def main():
                         "d2h_bytes_per_step": int(total * 4 + (NQ + 1) * 8)},
                 "gpu_launches": None, "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
                 "serving": serving}
+        if sweep_rows is not None:
+            line["sweep"] = sweep_rows
         levels = tree.info()["levels"]
         line["gpu_launches"] = (levels + 6) * args.steps  # unpack+check + levels + 3 scan + emit per step
         print(json.dumps(line))

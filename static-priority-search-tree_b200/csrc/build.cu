@@ -481,65 +481,72 @@ __global__ void k_level_nodes(BuildCtx<T, HAS_ID> c, uint32_t d, const uint32_t 
 
 // ---------------------------------------------------------------------------
 // Subtree builder: one CTA per node of level L0 finishes its whole subtree.  The
-// CTA holds the 64-bit dim2 keys of its points in dim1 order; a key names its point
-// (tb), so no positions are carried.
+// CTA holds the 64-bit dim2 keys of its points in dim1 order, each with the slot
+// of its point in a shared-memory copy of the subtree's points (gathered once, all
+// reads in flight together), so node writes never wait on global memory.
 
-// Shared-memory carve-up of k_subtree, in 32-bit words.
-constexpr uint32_t ST_OFF_KEYA = 0;                      // [ST_CAP] u64
-constexpr uint32_t ST_OFF_KEYB = ST_OFF_KEYA + 2 * ST_CAP;  // [ST_CAP] u64
-constexpr uint32_t ST_OFF_CNT = ST_OFF_KEYB + 2 * ST_CAP;
-constexpr uint32_t ST_OFF_CNT2 = ST_OFF_CNT + ST_CAP;
-constexpr uint32_t ST_OFF_START = ST_OFF_CNT2 + ST_CAP;
-constexpr uint32_t ST_OFF_TOPI = ST_OFF_START + ST_CAP + 1;
-constexpr uint32_t ST_OFF_WS = ST_OFF_TOPI + ST_CAP;
-constexpr uint32_t ST_WORDS = ST_OFF_WS + 33;
-constexpr size_t st_smem_bytes() { return (size_t) ST_WORDS * 4; }
-static_assert(st_smem_bytes() <= 227 * 1024, "subtree builder shared memory");
+// Shared-memory carve-up of k_subtree, in bytes: points first (8-byte aligned for
+// doubles), then the u64 keys, the u16 point slots and the u16 arg-max per sub-node.
+template <typename T, bool HAS_ID>
+struct SubtreeSmem {
+	static constexpr size_t PTS = 0;
+	static constexpr size_t KEYA = PTS + (size_t) ST_CAP * sizeof(Point<T, HAS_ID>);
+	static constexpr size_t KEYB = KEYA + (size_t) ST_CAP * 8;
+	static constexpr size_t SLOTA = KEYB + (size_t) ST_CAP * 8;
+	static constexpr size_t SLOTB = SLOTA + (size_t) ST_CAP * 2;
+	static constexpr size_t TOPI = SLOTB + (size_t) ST_CAP * 2;
+	static constexpr size_t WS = TOPI + (size_t) ST_CAP * 2;
+	static constexpr size_t BYTES = WS + 33 * 4;
+	static_assert(KEYA % 8 == 0 && BYTES <= 227 * 1024, "subtree builder shared memory");
+};
 
-template <typename U>
-__device__ void block_scan_array(const U *in, U *out, uint32_t n, U *ws)
+// Count and start of sub-node t of sub-level s in that sub-level's compacted key
+// order, from the subtree's count cN alone: going down one level removes each
+// node's point (every node above the last level holds one), the left child keeps
+// the first floor(c/2) of the rest and the right child the others, so
+//   start(2t) = start(t) - t,  start(2t+1) = start(t) - t + floor(c/2).
+__device__ __forceinline__ void subnode_span(uint32_t cN, uint32_t s, uint32_t t, uint32_t &cnt, uint32_t &start)
 {
-	// out[i] = sum in[0..i); out[n] = total.  in may equal out.
-	U carry = 0;
-	for (uint32_t b = 0; b < n; b += blockDim.x) {
-		const uint32_t i = b + threadIdx.x;
-		const U v = i < n ? in[i] : U(0);
-		U tot;
-		const U ex = block_excl_scan<U>(v, &tot, ws);
-		if (i < n)
-			out[i] = carry + ex;
-		carry += tot;
+	uint32_t c = cN, st = 0, ti = 0;
+	for (int e = (int) s - 1; e >= 0; e--) {
+		const uint32_t bit = (t >> e) & 1u;
+		const uint32_t left = c / 2;
+		st = st - ti + (bit ? left : 0u);
+		c = c ? (bit ? c - 1 - left : left) : 0u;
+		ti = 2 * ti + bit;
 	}
-	if (threadIdx.x == 0)
-		out[n] = carry;
-	__syncthreads();
+	cnt = c;
+	start = st;
 }
 
 template <typename T, bool HAS_ID>
 __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, uint32_t L0,
                                                        const uint32_t *__restrict__ B)
 {
-	extern __shared__ __align__(16) uint32_t st_smem[];
-	uint64_t *keyA = reinterpret_cast<uint64_t *>(st_smem + ST_OFF_KEYA);
-	uint64_t *keyB = reinterpret_cast<uint64_t *>(st_smem + ST_OFF_KEYB);
-	uint32_t *cnt = st_smem + ST_OFF_CNT;     // [ST_CAP] counts of the current sub-level
-	uint32_t *cnt2 = st_smem + ST_OFF_CNT2;   // [ST_CAP] counts of the next sub-level
-	uint32_t *start = st_smem + ST_OFF_START; // [ST_CAP + 1]
-	uint32_t *topi = st_smem + ST_OFF_TOPI;   // [ST_CAP]
-	uint32_t *ws = st_smem + ST_OFF_WS;       // [33]
+	using SM = SubtreeSmem<T, HAS_ID>;
+	using Pt = Point<T, HAS_ID>;
+	extern __shared__ __align__(16) unsigned char st_smem[];
+	Pt *spts = reinterpret_cast<Pt *>(st_smem + SM::PTS);
+	uint64_t *kc = reinterpret_cast<uint64_t *>(st_smem + SM::KEYA);
+	uint64_t *kn = reinterpret_cast<uint64_t *>(st_smem + SM::KEYB);
+	uint16_t *sc = reinterpret_cast<uint16_t *>(st_smem + SM::SLOTA);
+	uint16_t *sn = reinterpret_cast<uint16_t *>(st_smem + SM::SLOTB);
+	uint16_t *topi = reinterpret_cast<uint16_t *>(st_smem + SM::TOPI);  // [ST_CAP]
+	uint32_t *ws = reinterpret_cast<uint32_t *>(st_smem + SM::WS);      // [33]
 	__shared__ uint32_t s_n;
 
 	const uint32_t j = blockIdx.x;
-	const uint64_t cN = node_count(c.n, L0, j);
-	if (cN == 0 || *c.err)
+	const uint64_t cN64 = node_count(c.n, L0, j);
+	if (cN64 == 0 || *c.err)
 		return;
 	const uint32_t lo = L0 ? B[j] : 0u;
 	const uint32_t hi = L0 ? B[j + 1] : (uint32_t) c.n;
-	if (lo >= hi || hi > c.n) {
+	if (lo >= hi || hi > c.n || cN64 > ST_CAP) {
 		if (threadIdx.x == 0)
 			atomicOr(c.err, 16u);
 		return;
 	}
+	const uint32_t cN = (uint32_t) cN64;
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = ST_THREADS / 32;
 
 	// Gather the keys of the points still free in [lo, hi), in dim1 order.
@@ -553,36 +560,53 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 		uint32_t tot;
 		const uint32_t off = block_excl_scan<uint32_t>(keep ? 1u : 0u, &tot, ws);
 		const uint32_t base = s_n;
-		if (keep && base + off < ST_CAP)
-			keyA[base + off] = v;
+		if (keep && base + off < ST_CAP) {
+			kc[base + off] = v;
+			sc[base + off] = (uint16_t) (base + off);
+		}
 		__syncthreads();
 		if (threadIdx.x == 0)
 			s_n = base + tot;
 		__syncthreads();
 	}
-	if (s_n != cN || cN > ST_CAP) {
+	if (s_n != cN) {
 		if (threadIdx.x == 0)
 			atomicOr(c.err, 2u);
 		return;
 	}
+	// ... and their points, every read of the CTA in flight at once
+	{
+		constexpr int PER = ST_CAP / ST_THREADS;
+		Pt tmp[PER];
+#pragma unroll
+		for (int u = 0; u < PER; u++) {
+			const uint32_t i = threadIdx.x + u * ST_THREADS;
+			if (i < cN)
+				tmp[u] = c.point_of_tb(BuildCtx<T, HAS_ID>::tb_of(kc[i]));
+		}
+#pragma unroll
+		for (int u = 0; u < PER; u++) {
+			const uint32_t i = threadIdx.x + u * ST_THREADS;
+			if (i < cN)
+				spts[i] = tmp[u];
+		}
+	}
+	__syncthreads();
 	const uint32_t h0 = (1u << L0) + j;
 	const uint32_t last_s = c.D - 1 - L0;
 	const uint32_t half = 1u << (c.D - 1);  // med exists for positions < half
-	uint64_t *kc = keyA, *kn = keyB;
-	uint32_t nsub = 1;
-	uint32_t present = (uint32_t) cN;
-	if (threadIdx.x == 0)
-		cnt[0] = (uint32_t) cN;
-	__syncthreads();
+	uint32_t present = cN;
 	for (uint32_t s = 0;; s++) {
-		block_scan_array<uint32_t>(cnt, start, nsub, ws);
+		const uint32_t nsub = 1u << s;
 		const bool wide = present / nsub >= 64;
 		// arg-max of every sub-node (keys are distinct)
 		if (wide) {
 			for (uint32_t t = warp; t < nsub; t += nwarps) {
+				uint32_t ct, st;
+				subnode_span(cN, s, t, ct, st);
 				uint64_t bk = 0;
 				uint32_t bi = 0;
-				for (uint32_t i = start[t] + lane; i < start[t + 1]; i += 32)
+				for (uint32_t i = st + lane; i < st + ct; i += 32)
 					if (kc[i] > bk) {
 						bk = kc[i];
 						bi = i;
@@ -597,18 +621,20 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 					}
 				}
 				if (lane == 0)
-					topi[t] = bi;
+					topi[t] = (uint16_t) bi;
 			}
 		} else {
 			for (uint32_t t = threadIdx.x; t < nsub; t += ST_THREADS) {
+				uint32_t ct, st;
+				subnode_span(cN, s, t, ct, st);
 				uint64_t bk = 0;
 				uint32_t bi = 0;
-				for (uint32_t i = start[t]; i < start[t + 1]; i++)
+				for (uint32_t i = st; i < st + ct; i++)
 					if (kc[i] > bk) {
 						bk = kc[i];
 						bi = i;
 					}
-				topi[t] = bi;
+				topi[t] = (uint16_t) bi;
 			}
 		}
 		__syncthreads();
@@ -618,20 +644,21 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 			bool occupied = false;
 			uint32_t h = 0;
 			if (t < nsub) {
-				const uint32_t ct = cnt[t];
+				uint32_t ct, st;
+				subnode_span(cN, s, t, ct, st);
 				h = (h0 << s) + t;
 				if (ct > 0) {
 					occupied = true;
 					const uint32_t ti = topi[t];
-					const Point<T, HAS_ID> p = c.point_of_tb(BuildCtx<T, HAS_ID>::tb_of(kc[ti]));
+					const Pt p = spts[sc[ti]];
 					c.write_node(h, p);
 					if (h < half) {
-						T m = p.dim1;
+						T m = p.dim1;  // a node of one point: its own dim1
 						if (ct >= 2) {
-							uint32_t mi = start[t] + ct / 2 - 1;
+							uint32_t mi = st + ct / 2 - 1;
 							if (ti <= mi)
 								mi++;
-							m = c.point_of_tb(BuildCtx<T, HAS_ID>::tb_of(kc[mi])).dim1;
+							m = spts[sc[mi]].dim1;
 						}
 						c.med[h] = m;
 					}
@@ -650,40 +677,42 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 		}
 		if (s == last_s)
 			break;
-		// counts of the next sub-level
-		for (uint32_t t = threadIdx.x; t < nsub; t += ST_THREADS) {
-			const uint32_t ct = cnt[t];
-			cnt2[2 * t] = ct ? ct / 2 : 0u;
-			cnt2[2 * t + 1] = ct ? ct - 1 - ct / 2 : 0u;
-		}
-		// drop each sub-node's point; every segment is non-empty above the last level
+		// drop each sub-node's point; every sub-node above the last level holds one
 		if (wide) {
 			for (uint32_t t = warp; t < nsub; t += nwarps) {
+				uint32_t ct, st;
+				subnode_span(cN, s, t, ct, st);
 				const uint32_t ti = topi[t];
-				for (uint32_t i = start[t] + lane; i < start[t + 1]; i += 32)
-					if (i != ti)
-						kn[i - t - (i > ti ? 1u : 0u)] = kc[i];
+				for (uint32_t i = st + lane; i < st + ct; i += 32)
+					if (i != ti) {
+						const uint32_t ni = i - t - (i > ti ? 1u : 0u);
+						kn[ni] = kc[i];
+						sn[ni] = sc[i];
+					}
 			}
 		} else {
 			for (uint32_t t = threadIdx.x; t < nsub; t += ST_THREADS) {
+				uint32_t ct, st;
+				subnode_span(cN, s, t, ct, st);
 				const uint32_t ti = topi[t];
-				for (uint32_t i = start[t]; i < start[t + 1]; i++)
-					if (i != ti)
-						kn[i - t - (i > ti ? 1u : 0u)] = kc[i];
+				for (uint32_t i = st; i < st + ct; i++)
+					if (i != ti) {
+						const uint32_t ni = i - t - (i > ti ? 1u : 0u);
+						kn[ni] = kc[i];
+						sn[ni] = sc[i];
+					}
 			}
 		}
-		__syncthreads();
-		for (uint32_t t = threadIdx.x; t < 2 * nsub; t += ST_THREADS)
-			cnt[t] = cnt2[t];
 		present -= nsub;
-		nsub *= 2;
 		uint64_t *tk = kc;
 		kc = kn;
 		kn = tk;
+		uint16_t *ts = sc;
+		sc = sn;
+		sn = ts;
 		__syncthreads();
 	}
 }
-
 
 template <typename T>
 T *as(void *p)
@@ -691,32 +720,72 @@ T *as(void *p)
 	return static_cast<T *>(p);
 }
 
-struct DevBuf {
-	void *p = nullptr;
-	cudaStream_t s = nullptr;
-	DevBuf() = default;
-	DevBuf(size_t bytes, cudaStream_t st) : s(st)
+// All construction scratch lives in one device allocation (one cudaMalloc maps it
+// far faster than a dozen stream-ordered allocations that regrow a trimmed pool).
+struct ScratchLayout {
+	size_t k1, kalt, c2, valt, k2, v32a, v32b, P, rs_status, rs_misc, flags, Ba, Bb, best, top, taken, tmax;
+	size_t total;
+};
+
+ScratchLayout scratch_layout(pst_dtype dt, pst_idtype it, uint64_t n)
+{
+	ScratchLayout L{};
+	const size_t ks = value_size(dt);
+	const bool wide_key = dt == PST_F64;
+	const uint32_t D = tree_levels(n);
+	const uint32_t L0 = n ? std::min(subtree_level(n), D - 1) : 0;
+	const uint64_t nodes_wide = 1ull << L0;
+	const uint64_t rs_tiles = rs_num_tiles(n);
+	const uint64_t ntiles = (n + TM_TILE - 1) / TM_TILE;
+	size_t o = 0;
+	auto take = [&](size_t bytes) {
+		const size_t r = o;
+		o = align_up(o + bytes);
+		return r;
+	};
+	L.k1 = take(n * ks);
+	L.kalt = take(n * ks);
+	L.c2 = take(n * 8);
+	L.valt = take(n * 8);
+	L.k2 = take(wide_key ? n * 8 : 0);
+	L.v32a = take(wide_key ? n * 4 : 0);
+	L.v32b = take(wide_key ? n * 4 : 0);
+	L.P = take(it == PST_ID_U32 ? n * 4 : 0);
+	L.rs_status = take(256 * rs_tiles * 8);
+	L.rs_misc = take(rs_misc_words() * 4);
+	L.flags = take(256);
+	L.Ba = take((nodes_wide + 1) * 4);
+	L.Bb = take((nodes_wide + 1) * 4);
+	L.best = take(nodes_wide * 8);
+	L.top = take(nodes_wide * 4);
+	L.taken = take(((n + 31) / 32) * 4);
+	L.tmax = take(L0 ? ntiles * 8 : 0);
+	L.total = o;
+	return L;
+}
+
+struct Scratch {
+	char *base = nullptr;
+	explicit Scratch(size_t bytes)
 	{
-		if (bytes == 0)
-			return;
-		cudaError_t e = cudaMallocAsync(&p, bytes, st);
+		cudaError_t e = cudaMalloc(&base, std::max<size_t>(bytes, 256));
 		if (e == cudaErrorMemoryAllocation) {
 			cudaGetLastError();
-			fail(PST_ERR_NOMEM, "device allocation of " + std::to_string(bytes) + " B failed during construction");
+			fail(PST_ERR_NOMEM, "construction scratch allocation of " + std::to_string(bytes) + " B failed");
 		}
-		check_cuda(e, "cudaMallocAsync");
+		check_cuda(e, "cudaMalloc(construction scratch)");
 	}
-	~DevBuf()
+	~Scratch()
 	{
-		if (p)
-			cudaFreeAsync(p, s);
+		if (base)
+			cudaFree(base);  // waits for the construction's work
 	}
-	DevBuf(const DevBuf &) = delete;
-	DevBuf &operator=(const DevBuf &) = delete;
+	Scratch(const Scratch &) = delete;
+	Scratch &operator=(const Scratch &) = delete;
 	template <typename T>
-	T *get() const
+	T *at(size_t off) const
 	{
-		return static_cast<T *>(p);
+		return reinterpret_cast<T *>(base + off);
 	}
 };
 
@@ -727,19 +796,8 @@ inline unsigned grid_for(uint64_t n, int threads)
 	return (unsigned) std::max<uint64_t>(1, std::min(want, cap));
 }
 
-// Scratch bytes of build_impl beyond the tree itself (kept next to build_impl so the
-// two stay in step).
-uint64_t build_scratch_bytes(pst_dtype dt, pst_idtype it, uint64_t n)
-{
-	const uint64_t ks = value_size(dt);
-	const uint64_t tiles = rs_num_tiles(n);
-	const uint64_t wide = 1ull << subtree_level(n);
-	// k1, keys_alt (ks each); c2, vals_alt (8 each); doubles: k2 (8) and the rank
-	// sort's u32 payloads (2 x 4); P (4) for non-monotone ids
-	uint64_t per_pt = 2 * ks + 16 + (dt == PST_F64 ? 16 : 0) + (it == PST_ID_U32 ? 4 : 0);
-	return n * per_pt + n / 8 + (n / TM_TILE + 1) * 8 + 256 * tiles * 4 + scan_tmp_elems(256 * tiles) * 4 +
-	       wide * 24 + (1 << 20);
-}
+// Scratch bytes of build_impl beyond the tree itself.
+uint64_t build_scratch_bytes(pst_dtype dt, pst_idtype it, uint64_t n) { return scratch_layout(dt, it, n).total; }
 
 template <typename T, bool HAS_ID>
 void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
@@ -751,14 +809,13 @@ void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 	const uint32_t D = t.levels;
 
 	// ---- scratch
-	const uint64_t rs_tiles = rs_num_tiles(n);
-	DevBuf k1(n * sizeof(K), s), kalt(n * sizeof(K), s), c2(n * 8, s), valt(n * 8, s);
-	DevBuf k2(WIDE_KEY ? n * 8 : 0, s), v32a(WIDE_KEY ? n * 4 : 0, s), v32b(WIDE_KEY ? n * 4 : 0, s);
-	DevBuf Pb(HAS_ID ? n * 4 : 0, s);
-	DevBuf tile_hist(256 * rs_tiles * 4, s), scan_tmp(scan_tmp_elems(256 * rs_tiles) * 4, s);
-	DevBuf flags(256, s);
-	uint32_t *flag = flags.get<uint32_t>();  // [0] ids decrease, [1] error bits, [2..3] id range
-	K *krange = reinterpret_cast<K *>(flags.get<unsigned char>() + 64);  // [k1 min, k1 max, k2 min, k2 max]
+	const ScratchLayout SL = scratch_layout(t.dtype, t.idtype, n);
+	Scratch scr(SL.total);
+	void *k1 = scr.at<void>(SL.k1), *kalt = scr.at<void>(SL.kalt);
+	uint64_t *c2 = scr.at<uint64_t>(SL.c2);
+	void *valt = scr.at<void>(SL.valt);
+	uint32_t *flag = scr.at<uint32_t>(SL.flags);  // [0] ids decrease, [1] error bits, [2..3] id range
+	K *krange = reinterpret_cast<K *>(scr.at<unsigned char>(SL.flags) + 64);  // [k1 min, k1 max, k2 min, k2 max]
 	{
 		unsigned char init[256];
 		memset(init, 0, sizeof(init));
@@ -768,9 +825,14 @@ void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 		memcpy(init + 64, kinit, sizeof(kinit));
 		PST_CUDA(cudaMemcpyAsync(flag, init, sizeof(init), cudaMemcpyHostToDevice, s));
 	}
+	// one SortScratch for every sort of this build: its epoch tags the look-back
+	// status of each pass, which is cleared only here
 	SortScratch sc;
-	sc.tile_hist = tile_hist.get<uint32_t>();
-	sc.scan_tmp = scan_tmp.get<uint32_t>();
+	sc.status = scr.at<uint64_t>(SL.rs_status);
+	sc.hist = scr.at<uint32_t>(SL.rs_misc);
+	sc.counters = sc.hist + RS_MAX_PASSES * 256;
+	sc.err = flag + 1;
+	PST_CUDA(cudaMemsetAsync(sc.status, 0, 256 * rs_num_tiles(n) * 8, s));
 
 	const unsigned g = grid_for(n, 256);
 	// ---- tiebreak order: (id, input index) when ids are not already non-decreasing
@@ -781,72 +843,68 @@ void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 		PST_CUDA(cudaMemcpyAsync(host, flag, 16, cudaMemcpyDeviceToHost, s));
 		PST_CUDA(cudaStreamSynchronize(s));
 		if (host[0]) {
-			uint32_t *idk = k1.get<uint32_t>();  // k1 holds at least n u32
+			uint32_t *idk = static_cast<uint32_t *>(k1);  // k1 holds at least n u32
 			k_id_keys<T, HAS_ID><<<g, 256, 0, s>>>(pts, n, idk);
-			SortScratch s32 = sc;
-			s32.keys_alt = kalt.p;
-			s32.vals_alt = valt.p;           // n u32 fit in the u64 buffers
-			s32.vals_tmp = c2.p;
+			sc.keys_alt = kalt;
+			sc.vals_alt = valt;  // n u32 fit in the u64 buffers
+			sc.vals_tmp = c2;
 			uint32_t *kres, *vres;
-			radix_sort<uint32_t, uint32_t>(idk, nullptr, n, rs_passes<uint32_t>(host[2], host[3]), s32, &kres, &vres, s);
+			radix_sort<uint32_t, uint32_t>(idk, nullptr, n, rs_passes<uint32_t>(host[2], host[3]), sc, &kres, &vres, s);
 			// ids decrease somewhere, so they are not all equal and the sort ran
-			PST_CUDA(cudaMemcpyAsync(Pb.p, vres, n * 4, cudaMemcpyDeviceToDevice, s));
-			P = Pb.get<uint32_t>();
+			PST_CUDA(cudaMemcpyAsync(scr.at<uint32_t>(SL.P), vres, n * 4, cudaMemcpyDeviceToDevice, s));
+			P = scr.at<uint32_t>(SL.P);
 		}
 	}
 	// ---- keys in tiebreak order
-	k_prep_keys<T, HAS_ID><<<g, 256, 0, s>>>(pts, P, n, k1.get<K>(), c2.get<uint64_t>(), k2.get<K>(), krange);
+	k_prep_keys<T, HAS_ID><<<g, 256, 0, s>>>(pts, P, n, static_cast<K *>(k1), c2, scr.at<K>(SL.k2), krange);
 	PST_CUDA(cudaGetLastError());
 	K range[4];
 	PST_CUDA(cudaMemcpyAsync(range, krange, sizeof(range), cudaMemcpyDeviceToHost, s));
 	PST_CUDA(cudaStreamSynchronize(s));
 	if constexpr (WIDE_KEY) {
 		// dim2 ranks: stable sort of the dim2 keys in tiebreak order
-		SortScratch s2 = sc;
-		s2.keys_alt = kalt.p;
-		s2.vals_alt = v32a.p;
-		s2.vals_tmp = v32b.p;
+		sc.keys_alt = kalt;
+		sc.vals_alt = scr.at<void>(SL.v32a);
+		sc.vals_tmp = scr.at<void>(SL.v32b);
 		K *kres;
 		uint32_t *S2;
-		radix_sort<K, uint32_t>(k2.get<K>(), nullptr, n, rs_passes<K>(range[2], range[3]), s2, &kres, &S2, s);
-		k_rank_keys<<<g, 256, 0, s>>>(S2, n, c2.get<uint64_t>());
+		radix_sort<K, uint32_t>(scr.at<K>(SL.k2), nullptr, n, rs_passes<K>(range[2], range[3]), sc, &kres, &S2, s);
+		k_rank_keys<<<g, 256, 0, s>>>(S2, n, c2);
 		PST_CUDA(cudaGetLastError());
 	}
 	// ---- dim1 order, carrying the dim2 keys
 	K *k1s;
 	uint64_t *c2s;
 	{
-		SortScratch s1 = sc;
-		s1.keys_alt = kalt.p;
-		s1.vals_alt = valt.p;
-		radix_sort<K, uint64_t>(k1.get<K>(), c2.get<uint64_t>(), n, rs_passes<K>(range[0], range[1]), s1, &k1s, &c2s,
-		                        s);
+		sc.keys_alt = kalt;
+		sc.vals_alt = valt;
+		sc.vals_tmp = nullptr;
+		radix_sort<K, uint64_t>(static_cast<K *>(k1), c2, n, rs_passes<K>(range[0], range[1]), sc, &k1s, &c2s, s);
 	}
 
 	// ---- levels
 	const uint32_t L0 = std::min(subtree_level(n), D - 1);
 	const uint64_t nodes_wide = 1ull << L0;
 	const uint64_t ntiles = (n + TM_TILE - 1) / TM_TILE;
-	DevBuf Ba((nodes_wide + 1) * 4, s), Bb((nodes_wide + 1) * 4, s), bestb(nodes_wide * 8, s),
-	    topb(nodes_wide * 4, s), takenb(((n + 31) / 32) * 4, s), tmaxb(L0 ? ntiles * 8 : 0, s);
-	PST_CUDA(cudaMemsetAsync(takenb.p, 0, ((n + 31) / 32) * 4, s));
+	unsigned long long *best = scr.at<unsigned long long>(SL.best);
+	PST_CUDA(cudaMemsetAsync(scr.at<void>(SL.taken), 0, ((n + 31) / 32) * 4, s));
 	BuildCtx<T, HAS_ID> c;
 	c.pts = pts;
 	c.P = P;
 	c.k1s = k1s;
 	c.c2s = c2s;
-	c.taken = takenb.get<uint32_t>();
-	c.tmax = tmaxb.get<uint64_t>();
+	c.taken = scr.at<uint32_t>(SL.taken);
+	c.tmax = scr.at<uint64_t>(SL.tmax);
 	c.dim1 = as<T>(t.dim1);
 	c.dim2 = as<T>(t.dim2);
 	c.med = as<T>(t.med);
 	c.id = t.id;
 	c.occ = t.occ;
-	c.top_pos = topb.get<uint32_t>();
+	c.top_pos = scr.at<uint32_t>(SL.top);
 	c.err = flag + 1;
 	c.n = n;
 	c.D = D;
-	uint32_t *B = Ba.get<uint32_t>(), *Bn = Bb.get<uint32_t>();
+	uint32_t *B = scr.at<uint32_t>(SL.Ba), *Bn = scr.at<uint32_t>(SL.Bb);
 	{
 		const uint32_t b0[2] = {0u, (uint32_t) n};
 		PST_CUDA(cudaMemcpyAsync(B, b0, 8, cudaMemcpyHostToDevice, s));
@@ -859,11 +917,9 @@ void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 		    1, std::min<uint64_t>((ntiles + AM_THREADS - 1) / AM_THREADS, (uint64_t) device_info().sms * 8));
 		for (uint32_t d = 0; d < L0; d++) {
 			const uint32_t nseg = 1u << d;
-			PST_CUDA(cudaMemsetAsync(bestb.p, 0, (size_t) nseg * 8, s));
-			k_level_argmax<<<am_grid, AM_THREADS, 0, s>>>(c2s, c.taken, c.tmax, n, B, nseg,
-			                                              bestb.get<unsigned long long>(), c.err);
-			k_level_nodes<T, HAS_ID><<<(nseg + 127) / 128, 128, 0, s>>>(c, d, B, Bn,
-			                                                            bestb.get<unsigned long long>());
+			PST_CUDA(cudaMemsetAsync(best, 0, (size_t) nseg * 8, s));
+			k_level_argmax<<<am_grid, AM_THREADS, 0, s>>>(c2s, c.taken, c.tmax, n, B, nseg, best, c.err);
+			k_level_nodes<T, HAS_ID><<<(nseg + 127) / 128, 128, 0, s>>>(c, d, B, Bn, best);
 			if (d + 1 < L0)
 				k_tile_refresh<<<(unsigned) ((nseg * 32 + AM_THREADS - 1) / AM_THREADS), AM_THREADS, 0, s>>>(
 				    c2s, c.taken, n, c.top_pos, d, c.tmax, c.err);
@@ -871,9 +927,9 @@ void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 			std::swap(B, Bn);
 		}
 	}
-	PST_CUDA(cudaFuncSetAttribute(k_subtree<T, HAS_ID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-	                              (int) st_smem_bytes()));
-	k_subtree<T, HAS_ID><<<(unsigned) nodes_wide, ST_THREADS, st_smem_bytes(), s>>>(c, L0, B);
+	constexpr size_t st_bytes = SubtreeSmem<T, HAS_ID>::BYTES;
+	PST_CUDA(cudaFuncSetAttribute(k_subtree<T, HAS_ID>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) st_bytes));
+	k_subtree<T, HAS_ID><<<(unsigned) nodes_wide, ST_THREADS, st_bytes, s>>>(c, L0, B);
 	PST_CUDA(cudaGetLastError());
 	uint32_t errs[2] = {0, 0};
 	PST_CUDA(cudaMemcpyAsync(errs, flag, 8, cudaMemcpyDeviceToHost, s));

@@ -128,18 +128,31 @@ void exclusive_scan(const T *in, U *out, uint64_t n, T *tmp, T *total_d, cudaStr
 }
 
 // ---------------------------------------------------------------------------
-// LSD radix sort, 8-bit digits, 4096-key tiles.  Stable: within a tile keys are
-// ranked in input order (warp-private digit counters; the lanes of a warp holding
-// the same digit are found with eight ballots, one per digit bit), and tiles take
-// their digit offsets from a digit-major exclusive scan.  Only the passes that
-// cover bits where the keys differ are run: keys between kmin and kmax share
-// every bit above the highest bit of kmin ^ kmax.
+// LSD radix sort, 8-bit digits, 4096-key tiles, one kernel per digit pass
+// ("onesweep"): a first kernel histograms the digits of every pass at once; in a
+// pass, each tile ranks its keys stably (warp-private digit counters; the lanes of
+// a warp holding the same digit are found with eight ballots, one per digit bit),
+// publishes its digit counts, and finds the counts of all earlier tiles by walking
+// back over their published aggregates until one carries an inclusive prefix
+// (decoupled look-back).  Tiles take their numbers from an atomic counter in the
+// order they start, so a tile only waits on tiles that are already running; every
+// wait is bounded and a wait that runs out raises an error flag instead of
+// scattering.  Keys move once per pass: read, staged in shared memory in sorted
+// order, written with coalesced runs.  Only the passes that cover bits where the
+// keys differ are run: keys between kmin and kmax share every bit above the
+// highest bit of kmin ^ kmax.
 
 constexpr int RS_THREADS = 256;
 constexpr int RS_ITEMS = 16;
 constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
 constexpr int RS_WARPS = RS_THREADS / 32;
+constexpr int RS_MAX_PASSES = 8;
 static_assert(RS_THREADS == 256, "one thread per digit in the digit scans");
+
+// Look-back status word of (tile, digit): flag (2 bits) | epoch (30 bits) | count.
+constexpr uint64_t RS_AGG = 1ull << 62, RS_PREFIX = 2ull << 62, RS_FLAGS = 3ull << 62;
+constexpr uint32_t RS_SPIN_LIMIT = 1u << 22;
+constexpr uint32_t RS_ERR_LOOKBACK = 32u;  // error bit raised when a look-back wait runs out
 
 template <typename K>
 __device__ __forceinline__ uint32_t rs_digit(K k, int shift) { return (uint32_t) (k >> shift) & 0xFFu; }
@@ -157,37 +170,42 @@ __device__ __forceinline__ uint32_t rs_peers(uint32_t d, bool valid)
 	return peers;
 }
 
-// Per-tile digit counts, digit-major: tile_hist[digit * num_tiles + tile].
+// hist[p * 256 + digit] += count of keys with that digit in pass p, for p < passes.
+// Warps of a block pair up on private shared-memory histograms.
 template <typename K>
-__global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const K *keys, uint64_t n, int shift, uint32_t *tile_hist,
-                                                           uint32_t num_tiles)
+__global__ void __launch_bounds__(RS_THREADS) k_rs_global_hist(const K *__restrict__ keys, uint64_t n, int passes,
+                                                               uint32_t *hist)
 {
-	__shared__ uint32_t h[RS_WARPS][256];
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	for (int i = threadIdx.x; i < RS_WARPS * 256; i += RS_THREADS)
-		(&h[0][0])[i] = 0;
+	constexpr int COPIES = 4;
+	extern __shared__ uint32_t gh_smem[];  // [COPIES][passes * 256]
+	const int words = passes * 256;
+	for (int i = threadIdx.x; i < COPIES * words; i += RS_THREADS)
+		gh_smem[i] = 0;
 	__syncthreads();
-	const uint64_t t0 = (uint64_t) blockIdx.x * RS_TILE;
-#pragma unroll 4
-	for (int i = 0; i < RS_ITEMS; i++) {
-		const uint64_t idx = t0 + (uint64_t) warp * (RS_ITEMS * 32) + i * 32 + lane;
-		if (idx < n)
-			atomicAdd(&h[warp][rs_digit(keys[idx], shift)], 1u);
+	uint32_t *h = gh_smem + ((threadIdx.x >> 5) % COPIES) * words;
+	for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t) gridDim.x * blockDim.x) {
+		const K k = keys[i];
+		for (int p = 0; p < passes; p++)
+			atomicAdd(&h[p * 256 + rs_digit(k, 8 * p)], 1u);
 	}
 	__syncthreads();
-	uint32_t s = 0;
+	for (int i = threadIdx.x; i < words; i += RS_THREADS) {
+		uint32_t t = 0;
 #pragma unroll
-	for (int w = 0; w < RS_WARPS; w++)
-		s += h[w][threadIdx.x];
-	tile_hist[(uint64_t) threadIdx.x * num_tiles + blockIdx.x] = s;
+		for (int c = 0; c < COPIES; c++)
+			t += gh_smem[c * words + i];
+		if (t)
+			atomicAdd(&hist[i], t);
+	}
 }
 
 // One pass.  vals_in == nullptr means the identity payload (the key's input index;
 // 32-bit payloads only).
 template <typename K, typename V>
-__global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const K *keys_in, const V *vals_in, K *keys_out,
-                                                             V *vals_out, uint64_t n, int shift,
-                                                             const uint32_t *tile_off, uint32_t num_tiles)
+__global__ void __launch_bounds__(RS_THREADS, 3) k_rs_onesweep(const K *keys_in, const V *vals_in, K *keys_out,
+                                                            V *vals_out, uint64_t n, int shift,
+                                                            const uint32_t *__restrict__ hist, uint64_t *status,
+                                                            uint32_t *tile_counter, uint32_t epoch, uint32_t *err)
 {
 	extern __shared__ __align__(16) unsigned char rs_smem[];
 	V *sv = reinterpret_cast<V *>(rs_smem);
@@ -196,23 +214,29 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const K *keys_in, c
 	uint32_t *dstart = whist + RS_WARPS * 256;                      // [256] tile-local digit start
 	uint32_t *gbase = dstart + 256;                                 // [256] global start of the digit for this tile
 	uint32_t *wsum = gbase + 256;                                   // [33]
+	__shared__ uint32_t s_tile, s_fail;
 
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	if (threadIdx.x == 0) {
+		s_tile = atomicAdd(tile_counter, 1u);
+		s_fail = 0;
+	}
 	for (int i = threadIdx.x; i < RS_WARPS * 256; i += RS_THREADS)
 		whist[i] = 0;
-	gbase[threadIdx.x] = tile_off[(uint64_t) threadIdx.x * num_tiles + blockIdx.x];
 	__syncthreads();
-
-	const uint64_t t0 = (uint64_t) blockIdx.x * RS_TILE;
+	const uint32_t tile = s_tile;
+	const uint64_t t0 = (uint64_t) tile * RS_TILE;
 	K k[RS_ITEMS];
-	V v[RS_ITEMS];
 	uint32_t loc[RS_ITEMS];
 #pragma unroll
 	for (int i = 0; i < RS_ITEMS; i++) {
 		const uint64_t idx = t0 + (uint64_t) warp * (RS_ITEMS * 32) + i * 32 + lane;
+		k[i] = idx < n ? keys_in[idx] : K(0);
+	}
+#pragma unroll
+	for (int i = 0; i < RS_ITEMS; i++) {
+		const uint64_t idx = t0 + (uint64_t) warp * (RS_ITEMS * 32) + i * 32 + lane;
 		const bool valid = idx < n;
-		k[i] = valid ? keys_in[idx] : K(0);
-		v[i] = valid ? (vals_in ? vals_in[idx] : (V) idx) : V(0);
 		const uint32_t d = rs_digit(k[i], shift);
 		const uint32_t peers = rs_peers(d, valid);
 		const int leader = valid ? __ffs(peers) - 1 : lane;
@@ -226,20 +250,53 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const K *keys_in, c
 		__syncwarp();  // the next item's leaders read the counters written here
 	}
 	__syncthreads();
-	// Exclusive prefix of each digit over warps, then over digits.
 	{
-		const int d = threadIdx.x;
-		uint32_t run = 0;
+		const uint32_t d = threadIdx.x;
+		uint32_t cnt = 0;
 #pragma unroll
 		for (int w = 0; w < RS_WARPS; w++) {
-			uint32_t t = whist[w * 256 + d];
-			whist[w * 256 + d] = run;
-			run += t;
+			const uint32_t t = whist[w * 256 + d];
+			whist[w * 256 + d] = cnt;
+			cnt += t;
+		}
+		// publish this tile's count, then gather the counts of the tiles before it
+		volatile uint64_t *st = reinterpret_cast<volatile uint64_t *>(status);
+		const uint64_t tag = (uint64_t) (epoch & 0x3FFFFFFFu) << 32;
+		uint64_t excl = 0;
+		if (tile == 0) {
+			st[d] = RS_PREFIX | tag | cnt;
+		} else {
+			st[(uint64_t) tile * 256 + d] = RS_AGG | tag | cnt;
+			int64_t t = (int64_t) tile - 1;
+			uint32_t spins = 0;
+			for (;;) {
+				const uint64_t x = st[(uint64_t) t * 256 + d];
+				const uint64_t f = x & RS_FLAGS;
+				if (f == 0 || (x & ~RS_FLAGS & ~0xFFFFFFFFull) != tag) {
+					if (++spins > RS_SPIN_LIMIT) {
+						atomicOr(err, RS_ERR_LOOKBACK);
+						s_fail = 1;
+						break;
+					}
+					__nanosleep(64);
+					continue;
+				}
+				excl += x & 0xFFFFFFFFull;
+				if (f == RS_PREFIX)
+					break;
+				t--;
+			}
+			st[(uint64_t) tile * 256 + d] = RS_PREFIX | tag | (excl + cnt);
 		}
 		uint32_t tot;
-		dstart[d] = block_excl_scan<uint32_t>(run, &tot, wsum);
+		const uint32_t hb = block_excl_scan<uint32_t>(hist[d], &tot, wsum);
+		dstart[d] = block_excl_scan<uint32_t>(cnt, &tot, wsum);
+		gbase[d] = hb + (uint32_t) excl;
 	}
 	__syncthreads();
+	if (s_fail)
+		return;
+	// payloads are read only now, so they hold no registers through the ranking
 #pragma unroll
 	for (int i = 0; i < RS_ITEMS; i++) {
 		const uint64_t idx = t0 + (uint64_t) warp * (RS_ITEMS * 32) + i * 32 + lane;
@@ -247,7 +304,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const K *keys_in, c
 			const uint32_t d = rs_digit(k[i], shift);
 			const uint32_t lp = dstart[d] + whist[warp * 256 + d] + loc[i];
 			sk[lp] = k[i];
-			sv[lp] = v[i];
+			sv[lp] = vals_in ? vals_in[idx] : (V) idx;
 		}
 	}
 	__syncthreads();
@@ -257,28 +314,37 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const K *keys_in, c
 		const K key = sk[j];
 		const uint32_t d = rs_digit(key, shift);
 		const uint64_t g = (uint64_t) gbase[d] + (j - dstart[d]);
-		keys_out[g] = key;
-		vals_out[g] = sv[j];
+		if (g < n) {
+			keys_out[g] = key;
+			vals_out[g] = sv[j];
+		}
 	}
 }
 
 template <typename K, typename V>
-constexpr size_t rs_downsweep_smem()
+constexpr size_t rs_onesweep_smem()
 {
 	return RS_TILE * (sizeof(K) + sizeof(V)) + (RS_WARPS * 256 + 256 + 256 + 33) * 4;
 }
 
 inline uint64_t rs_num_tiles(uint64_t n) { return (n + RS_TILE - 1) / RS_TILE; }
 
-// Scratch for radix_sort: key/value ping-pong buffers of n entries plus the tile
-// histogram and its scan temporaries.
+// Scratch of radix_sort: key/value ping-pong buffers of n entries, the look-back
+// status of every (tile, digit) and the small per-pass counters.  `status` must be
+// zeroed once before the first sort that uses it; `epoch` then tags every pass so
+// later sorts reuse it without clearing.
 struct SortScratch {
 	void *keys_alt = nullptr;  // n keys
 	void *vals_alt = nullptr;  // n payloads
 	void *vals_tmp = nullptr;  // n payloads (second buffer for an identity input payload)
-	uint32_t *tile_hist = nullptr;
-	uint32_t *scan_tmp = nullptr;
+	uint64_t *status = nullptr;  // rs_num_tiles(n) * 256
+	uint32_t *hist = nullptr;    // RS_MAX_PASSES * 256, zeroed by radix_sort
+	uint32_t *counters = nullptr;  // RS_MAX_PASSES tile counters, zeroed by radix_sort
+	uint32_t *err = nullptr;
+	uint32_t epoch = 1;
 };
+
+constexpr size_t rs_misc_words() { return RS_MAX_PASSES * 256 + RS_MAX_PASSES; }
 
 // Number of 8-bit passes needed to sort keys lying in [kmin, kmax].
 template <typename K>
@@ -294,7 +360,8 @@ inline int rs_passes(K kmin, K kmax)
 // Sorts (keys, vals) ascending by key, stably, over the first `passes` digits.
 // vals may be null (identity payload, 32-bit payloads only).  The sorted data is in
 // the buffers returned through *keys_res / *vals_res (the input buffers or the
-// scratch ones; *vals_res stays null when passes == 0 and vals is null).
+// scratch ones; *vals_res stays null when passes == 0 and vals is null).  `hist` and
+// `counters` must be adjacent (rs_misc_words()).
 template <typename K, typename V>
 void radix_sort(K *keys, V *vals, uint64_t n, int passes, SortScratch &sc, K **keys_res, V **vals_res, cudaStream_t s)
 {
@@ -302,17 +369,21 @@ void radix_sort(K *keys, V *vals, uint64_t n, int passes, SortScratch &sc, K **k
 	*vals_res = vals;
 	if (n == 0 || passes == 0)
 		return;
+	if (passes > RS_MAX_PASSES)
+		fail(PST_ERR_INTERNAL, "radix sort: too many passes");
 	const uint64_t tiles = rs_num_tiles(n);
-	PST_CUDA(cudaFuncSetAttribute(k_rs_downsweep<K, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-	                              (int) rs_downsweep_smem<K, V>()));
+	PST_CUDA(cudaFuncSetAttribute(k_rs_onesweep<K, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                              (int) rs_onesweep_smem<K, V>()));
+	PST_CUDA(cudaMemsetAsync(sc.hist, 0, rs_misc_words() * 4, s));
+	const unsigned hg = (unsigned) std::min<uint64_t>((n + RS_THREADS - 1) / RS_THREADS,
+	                                                  (uint64_t) device_info().sms * 4);
+	k_rs_global_hist<K><<<hg, RS_THREADS, 4 * passes * 256 * 4, s>>>(keys, n, passes, sc.hist);
 	K *kin = keys, *kout = static_cast<K *>(sc.keys_alt);
 	V *vin = vals;
 	V *vout = static_cast<V *>(sc.vals_alt);
 	for (int p = 0; p < passes; p++) {
-		k_rs_upsweep<K><<<(unsigned) tiles, RS_THREADS, 0, s>>>(kin, n, 8 * p, sc.tile_hist, (uint32_t) tiles);
-		exclusive_scan<uint32_t>(sc.tile_hist, sc.tile_hist, 256 * tiles, sc.scan_tmp, nullptr, s);
-		k_rs_downsweep<K, V><<<(unsigned) tiles, RS_THREADS, rs_downsweep_smem<K, V>(), s>>>(
-		    kin, vin, kout, vout, n, 8 * p, sc.tile_hist, (uint32_t) tiles);
+		k_rs_onesweep<K, V><<<(unsigned) tiles, RS_THREADS, rs_onesweep_smem<K, V>(), s>>>(
+		    kin, vin, kout, vout, n, 8 * p, sc.hist + 256 * p, sc.status, sc.counters + p, sc.epoch++, sc.err);
 		PST_CUDA(cudaGetLastError());
 		K *kt = kin;
 		kin = kout;

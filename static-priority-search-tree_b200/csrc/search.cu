@@ -145,6 +145,107 @@ __device__ void path_step(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev 
 	}
 }
 
+// Dense tasks over 4-byte values, 16 bytes per lane: a task's ROWS consecutive rows
+// of 32 slots (ROWS * 128 bytes) are read by 8 * ROWS lanes with one vector load
+// each, so one load instruction of the warp covers 32 / (8 * ROWS) tasks and a lane
+// keeps QUAD_GROUPS of them in flight.  Each 8-lane group ORs its nibbles into the
+// row's 32-bit mask, which the task's owner lane then reads.
+constexpr int QUAD_GROUPS = 4;
+
+template <typename T>
+struct Vec4;
+template <>
+struct Vec4<float> {
+	using V = float4;
+};
+template <>
+struct Vec4<int32_t> {
+	using V = int4;
+};
+
+// The owners (lanes of `dm`, lowest first) of the next QUAD_GROUPS * TPG tasks.
+template <int N>
+__device__ __forceinline__ void next_owners(uint32_t &dm, int (&s)[N])
+{
+#pragma unroll
+	for (int i = 0; i < N; i++) {
+		s[i] = dm ? __ffs(dm) - 1 : -1;
+		dm &= dm ? dm - 1 : 0u;
+	}
+}
+
+// Owner lane of the task this lane serves in group u (slot g of TPG), -1 if none.
+template <int TPG, int N>
+__device__ __forceinline__ int group_src(const int (&s)[N], int u, uint32_t g)
+{
+	int src = s[u * TPG];
+#pragma unroll
+	for (int j = 1; j < TPG; j++)
+		src = g == (uint32_t) j ? s[u * TPG + j] : src;
+	return src;
+}
+
+// Slot j of group u owned by this lane, -1 if none.
+template <int TPG, int N>
+__device__ __forceinline__ int owned_slot(const int (&s)[N], int u, uint32_t lane)
+{
+	int myj = -1;
+#pragma unroll
+	for (int j = 0; j < TPG; j++)
+		myj = s[u * TPG + j] == (int) lane ? j : myj;
+	return myj;
+}
+
+template <typename T, int ROWS>
+__device__ __forceinline__ void dense_quads(const T *__restrict__ dim2, uint32_t p, const uint32_t (&cand)[ROWS],
+                                            T m2, uint32_t dm, uint32_t (&am)[ROWS])
+{
+	using V = typename Vec4<T>::V;
+	constexpr int LPT = 8 * ROWS;  // lanes per task
+	constexpr int TPG = 32 / LPT;  // tasks per load instruction
+	const uint32_t lane = lane_id();
+	const uint32_t g = lane / LPT, sub = lane % LPT, r = sub / 8, qd = sub % 8;
+	while (dm) {
+		int s[QUAD_GROUPS * TPG];
+		next_owners(dm, s);
+		V v[QUAD_GROUPS];
+		uint32_t nib[QUAD_GROUPS];
+		T mm[QUAD_GROUPS];
+#pragma unroll
+		for (int u = 0; u < QUAD_GROUPS; u++) {
+			const int src = group_src<TPG>(s, u, g);
+			const int sl = src < 0 ? 0 : src;
+			uint32_t crow = __shfl_sync(FULL, cand[0], sl);
+			if constexpr (ROWS == 2) {
+				const uint32_t c1 = __shfl_sync(FULL, cand[1], sl);
+				crow = r ? c1 : crow;
+			}
+			const uint32_t pp = __shfl_sync(FULL, p, sl);
+			mm[u] = __shfl_sync(FULL, m2, sl);
+			nib[u] = src >= 0 ? (crow >> (4 * qd)) & 0xFu : 0u;
+			v[u] = nib[u] ? *reinterpret_cast<const V *>(dim2 + pp + 32 * r + 4 * qd) : V{};
+		}
+#pragma unroll
+		for (int u = 0; u < QUAD_GROUPS; u++) {
+			const uint32_t b = nib[u];
+			const uint32_t bits = ((b & 1u) && mm[u] <= v[u].x ? 1u : 0u) | ((b & 2u) && mm[u] <= v[u].y ? 2u : 0u) |
+			                      ((b & 4u) && mm[u] <= v[u].z ? 4u : 0u) | ((b & 8u) && mm[u] <= v[u].w ? 8u : 0u);
+			uint32_t row = bits << (4 * qd);
+			row |= __shfl_xor_sync(FULL, row, 1);
+			row |= __shfl_xor_sync(FULL, row, 2);
+			row |= __shfl_xor_sync(FULL, row, 4);
+			const int myj = owned_slot<TPG>(s, u, lane);
+			const int base = myj < 0 ? 0 : myj * LPT;
+#pragma unroll
+			for (int rr = 0; rr < ROWS; rr++) {
+				const uint32_t val = __shfl_sync(FULL, row, base + 8 * rr);
+				if (myj >= 0)
+					am[rr] = val;
+			}
+		}
+	}
+}
+
 // Tests the 32*K chunk tasks held by a warp (lane l owns tasks (l, 0..K-1): chunk
 // base p[k], candidate lanes cand[k], the query's min2) and returns each task's
 // mask of reported slots in am[k].  A task with at most SPARSE_BITS candidates is
@@ -157,12 +258,17 @@ __device__ __forceinline__ void test_chunks(const T *__restrict__ dim2, const ui
                                             const uint32_t (&cand)[K], T m2, uint32_t (&am)[K])
 {
 	const uint32_t lane = lane_id();
+	constexpr bool QUADS = sizeof(T) == 4;
 	uint32_t dense_mask[K];
+	uint32_t total = 0;
+#pragma unroll
+	for (int k = 0; k < K; k++)
+		total += __popc(cand[k]);
 #pragma unroll
 	for (int k = 0; k < K; k++) {
 		am[k] = 0;
 		const uint32_t c = cand[k];
-		const bool dense = __popc(c) > SPARSE_BITS;
+		const bool dense = QUADS ? total > SPARSE_BITS : __popc(c) > SPARSE_BITS;
 		dense_mask[k] = __ballot_sync(FULL, dense);
 		if (!dense && c) {
 			// lane mode: a handful of slots of one 128-byte row
@@ -182,6 +288,12 @@ __device__ __forceinline__ void test_chunks(const T *__restrict__ dim2, const ui
 			}
 			am[k] = a;
 		}
+	}
+	if constexpr (QUADS) {
+		// rows of one task are consecutive: p[k] = p[0] + 32 k
+		if (dense_mask[0])
+			dense_quads<T, K>(dim2, p[0], cand, m2, dense_mask[0], am);
+		return;
 	}
 #pragma unroll
 	for (int k = 0; k < K; k++) {
@@ -383,6 +495,50 @@ __device__ __forceinline__ void emit_one(const TreeDev<T> &t, uint32_t h, uint64
 	}
 }
 
+// Dense id records, 16 bytes per lane: 8 lanes read a record's row of 32 ids with
+// one vector load each and store the reported ones at their compacted offsets.
+__device__ __forceinline__ void emit_id_quads(const uint32_t *__restrict__ ids, uint32_t p, uint32_t am,
+                                              uint64_t out_base, uint32_t dm, uint32_t *__restrict__ out,
+                                              uint64_t capacity)
+{
+	constexpr int TPG = 4;
+	const uint32_t lane = lane_id();
+	const uint32_t g = lane / 8, qd = lane % 8;
+	const uint32_t below = (1u << (4 * qd)) - 1u;
+	while (dm) {
+		int s[QUAD_GROUPS * TPG];
+		next_owners(dm, s);
+		uint4 v[QUAD_GROUPS];
+		uint32_t nib[QUAD_GROUPS];
+		uint64_t o[QUAD_GROUPS];
+#pragma unroll
+		for (int u = 0; u < QUAD_GROUPS; u++) {
+			const int src = group_src<TPG>(s, u, g);
+			const int sl = src < 0 ? 0 : src;
+			const uint32_t a = __shfl_sync(FULL, am, sl);
+			const uint32_t pp = __shfl_sync(FULL, p, sl);
+			const uint64_t ob = __shfl_sync(FULL, out_base, sl);
+			nib[u] = src >= 0 ? (a >> (4 * qd)) & 0xFu : 0u;
+			o[u] = ob + __popc(a & below);
+			v[u] = nib[u] ? *reinterpret_cast<const uint4 *>(ids + pp + 4 * qd) : make_uint4(0, 0, 0, 0);
+		}
+#pragma unroll
+		for (int u = 0; u < QUAD_GROUPS; u++) {
+			uint64_t oo = o[u];
+			const uint32_t b = nib[u];
+			const uint32_t vals[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+#pragma unroll
+			for (int j = 0; j < 4; j++) {
+				if ((b >> j) & 1u) {
+					if (oo < capacity)
+						out[oo] = vals[j];
+					oo++;
+				}
+			}
+		}
+	}
+}
+
 template <typename T, bool HAS_ID, bool POINTS>
 __device__ __forceinline__ void emit_rows(const TreeDev<T> &t, uint32_t p, uint32_t am, uint64_t out_base,
                                           void *__restrict__ out, uint64_t capacity)
@@ -418,6 +574,11 @@ __device__ __forceinline__ void emit_rows(const TreeDev<T> &t, uint32_t p, uint3
 	const T *__restrict__ d1 = t.dim1;
 	const T *__restrict__ d2 = t.dim2;
 	uint32_t dm = __ballot_sync(FULL, dense);
+	if constexpr (!POINTS) {
+		if (dm)
+			emit_id_quads(ids, p, am, out_base, dm, static_cast<uint32_t *>(out), capacity);
+		return;
+	}
 	while (dm) {
 		int src[LOADS_IN_FLIGHT];
 #pragma unroll
