@@ -79,8 +79,12 @@ TreeLayout tree_layout(pst_dtype dt, pst_idtype it, uint64_t n)
 	return L;
 }
 
-// Subtree builder capacity: nodes of at most ST_CAP points are finished by one CTA.
-constexpr uint32_t ST_CAP = 2048;
+// Subtree builder capacity: nodes of at most ST_CAP points are finished by one CTA
+// (a power of two; PST_SUBTREE_CAP overrides it at build time).
+#ifndef PST_SUBTREE_CAP
+#define PST_SUBTREE_CAP 2048
+#endif
+constexpr uint32_t ST_CAP = PST_SUBTREE_CAP;
 constexpr int ST_THREADS = 256;
 // Arg-max tiles: every segment of a level before the subtree level spans at least
 // ST_CAP >= TM_TILE positions, so a tile is cut by at most one segment boundary.
@@ -495,29 +499,19 @@ struct SubtreeSmem {
 	static constexpr size_t SLOTA = KEYB + (size_t) ST_CAP * 8;
 	static constexpr size_t SLOTB = SLOTA + (size_t) ST_CAP * 2;
 	static constexpr size_t TOPI = SLOTB + (size_t) ST_CAP * 2;
-	static constexpr size_t WS = TOPI + (size_t) ST_CAP * 2;
+	static constexpr size_t CNT = TOPI + (size_t) ST_CAP * 2;
+	static constexpr size_t START = CNT + (size_t) ST_CAP * 2;
+	static constexpr size_t WS = START + (size_t) ST_CAP * 2;
 	static constexpr size_t BYTES = WS + 33 * 4;
 	static_assert(KEYA % 8 == 0 && BYTES <= 227 * 1024, "subtree builder shared memory");
 };
 
-// Count and start of sub-node t of sub-level s in that sub-level's compacted key
-// order, from the subtree's count cN alone: going down one level removes each
-// node's point (every node above the last level holds one), the left child keeps
-// the first floor(c/2) of the rest and the right child the others, so
+// Count and start of every sub-node of the current sub-level (in that sub-level's
+// compacted key order) are kept in shared memory and derived level to level
+// without a scan: going down one level removes each node's point (every node
+// above the last level holds one), the left child keeps the first floor(c/2) of
+// the rest and the right child the others, so
 //   start(2t) = start(t) - t,  start(2t+1) = start(t) - t + floor(c/2).
-__device__ __forceinline__ void subnode_span(uint32_t cN, uint32_t s, uint32_t t, uint32_t &cnt, uint32_t &start)
-{
-	uint32_t c = cN, st = 0, ti = 0;
-	for (int e = (int) s - 1; e >= 0; e--) {
-		const uint32_t bit = (t >> e) & 1u;
-		const uint32_t left = c / 2;
-		st = st - ti + (bit ? left : 0u);
-		c = c ? (bit ? c - 1 - left : left) : 0u;
-		ti = 2 * ti + bit;
-	}
-	cnt = c;
-	start = st;
-}
 
 template <typename T, bool HAS_ID>
 __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, uint32_t L0,
@@ -531,8 +525,10 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 	uint64_t *kn = reinterpret_cast<uint64_t *>(st_smem + SM::KEYB);
 	uint16_t *sc = reinterpret_cast<uint16_t *>(st_smem + SM::SLOTA);
 	uint16_t *sn = reinterpret_cast<uint16_t *>(st_smem + SM::SLOTB);
-	uint16_t *topi = reinterpret_cast<uint16_t *>(st_smem + SM::TOPI);  // [ST_CAP]
-	uint32_t *ws = reinterpret_cast<uint32_t *>(st_smem + SM::WS);      // [33]
+	uint16_t *topi = reinterpret_cast<uint16_t *>(st_smem + SM::TOPI);    // [ST_CAP]
+	uint16_t *scnt = reinterpret_cast<uint16_t *>(st_smem + SM::CNT);     // [ST_CAP]
+	uint16_t *sstart = reinterpret_cast<uint16_t *>(st_smem + SM::START); // [ST_CAP]
+	uint32_t *ws = reinterpret_cast<uint32_t *>(st_smem + SM::WS);        // [33]
 	__shared__ uint32_t s_n;
 
 	const uint32_t j = blockIdx.x;
@@ -596,14 +592,18 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 	const uint32_t last_s = c.D - 1 - L0;
 	const uint32_t half = 1u << (c.D - 1);  // med exists for positions < half
 	uint32_t present = cN;
+	if (threadIdx.x == 0) {
+		scnt[0] = (uint16_t) cN;
+		sstart[0] = 0;
+	}
+	__syncthreads();
 	for (uint32_t s = 0;; s++) {
 		const uint32_t nsub = 1u << s;
 		const bool wide = present / nsub >= 64;
 		// arg-max of every sub-node (keys are distinct)
 		if (wide) {
 			for (uint32_t t = warp; t < nsub; t += nwarps) {
-				uint32_t ct, st;
-				subnode_span(cN, s, t, ct, st);
+				const uint32_t ct = scnt[t], st = sstart[t];
 				uint64_t bk = 0;
 				uint32_t bi = 0;
 				for (uint32_t i = st + lane; i < st + ct; i += 32)
@@ -625,8 +625,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 			}
 		} else {
 			for (uint32_t t = threadIdx.x; t < nsub; t += ST_THREADS) {
-				uint32_t ct, st;
-				subnode_span(cN, s, t, ct, st);
+				const uint32_t ct = scnt[t], st = sstart[t];
 				uint64_t bk = 0;
 				uint32_t bi = 0;
 				for (uint32_t i = st; i < st + ct; i++)
@@ -644,8 +643,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 			bool occupied = false;
 			uint32_t h = 0;
 			if (t < nsub) {
-				uint32_t ct, st;
-				subnode_span(cN, s, t, ct, st);
+				const uint32_t ct = scnt[t], st = sstart[t];
 				h = (h0 << s) + t;
 				if (ct > 0) {
 					occupied = true;
@@ -680,8 +678,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 		// drop each sub-node's point; every sub-node above the last level holds one
 		if (wide) {
 			for (uint32_t t = warp; t < nsub; t += nwarps) {
-				uint32_t ct, st;
-				subnode_span(cN, s, t, ct, st);
+				const uint32_t ct = scnt[t], st = sstart[t];
 				const uint32_t ti = topi[t];
 				for (uint32_t i = st + lane; i < st + ct; i += 32)
 					if (i != ti) {
@@ -692,8 +689,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 			}
 		} else {
 			for (uint32_t t = threadIdx.x; t < nsub; t += ST_THREADS) {
-				uint32_t ct, st;
-				subnode_span(cN, s, t, ct, st);
+				const uint32_t ct = scnt[t], st = sstart[t];
 				const uint32_t ti = topi[t];
 				for (uint32_t i = st; i < st + ct; i++)
 					if (i != ti) {
@@ -701,6 +697,27 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 						kn[ni] = kc[i];
 						sn[ni] = sc[i];
 					}
+			}
+		}
+		// spans of the next sub-level, in place: parents to registers, then children
+		constexpr int PMAX = ST_CAP / 2 / ST_THREADS;
+		uint32_t pc[PMAX], ps[PMAX];
+#pragma unroll
+		for (int u = 0; u < PMAX; u++) {
+			const uint32_t t = threadIdx.x + u * ST_THREADS;
+			pc[u] = t < nsub ? scnt[t] : 0u;
+			ps[u] = t < nsub ? sstart[t] : 0u;
+		}
+		__syncthreads();
+#pragma unroll
+		for (int u = 0; u < PMAX; u++) {
+			const uint32_t t = threadIdx.x + u * ST_THREADS;
+			if (t < nsub) {
+				const uint32_t left = pc[u] / 2;
+				scnt[2 * t] = (uint16_t) (pc[u] ? left : 0u);
+				scnt[2 * t + 1] = (uint16_t) (pc[u] ? pc[u] - 1 - left : 0u);
+				sstart[2 * t] = (uint16_t) (ps[u] - t);
+				sstart[2 * t + 1] = (uint16_t) (ps[u] - t + left);
 			}
 		}
 		present -= nsub;

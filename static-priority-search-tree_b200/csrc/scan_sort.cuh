@@ -183,10 +183,21 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_global_hist(const K *__restri
 		gh_smem[i] = 0;
 	__syncthreads();
 	uint32_t *h = gh_smem + ((threadIdx.x >> 5) % COPIES) * words;
-	for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t) gridDim.x * blockDim.x) {
-		const K k = keys[i];
-		for (int p = 0; p < passes; p++)
-			atomicAdd(&h[p * 256 + rs_digit(k, 8 * p)], 1u);
+	constexpr int IT = 8;  // loads issued before their atomics
+	const uint64_t step = (uint64_t) gridDim.x * blockDim.x * IT;
+	for (uint64_t base = (uint64_t) blockIdx.x * blockDim.x * IT + threadIdx.x; base < n; base += step) {
+		K k[IT];
+#pragma unroll
+		for (int u = 0; u < IT; u++) {
+			const uint64_t i = base + (uint64_t) u * blockDim.x;
+			k[u] = i < n ? keys[i] : K(0);
+		}
+#pragma unroll
+		for (int u = 0; u < IT; u++) {
+			if (base + (uint64_t) u * blockDim.x < n)
+				for (int p = 0; p < passes; p++)
+					atomicAdd(&h[p * 256 + rs_digit(k[u], 8 * p)], 1u);
+		}
 	}
 	__syncthreads();
 	for (int i = threadIdx.x; i < words; i += RS_THREADS) {

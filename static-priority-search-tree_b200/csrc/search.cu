@@ -293,35 +293,35 @@ __device__ __forceinline__ void test_chunks(const T *__restrict__ dim2, const ui
 		// rows of one task are consecutive: p[k] = p[0] + 32 k
 		if (dense_mask[0])
 			dense_quads<T, K>(dim2, p[0], cand, m2, dense_mask[0], am);
-		return;
-	}
+	} else {
 #pragma unroll
-	for (int k = 0; k < K; k++) {
-		uint32_t dm = dense_mask[k];
-		while (dm) {
-			// up to LOADS_IN_FLIGHT dense tasks, lowest lanes first (warp-uniform)
-			int src[LOADS_IN_FLIGHT];
+		for (int k = 0; k < K; k++) {
+			uint32_t dm = dense_mask[k];
+			while (dm) {
+				// up to LOADS_IN_FLIGHT dense tasks, lowest lanes first (warp-uniform)
+				int src[LOADS_IN_FLIGHT];
 #pragma unroll
-			for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
-				src[u] = dm ? __ffs(dm) - 1 : -1;
-				dm &= dm ? dm - 1 : 0u;
-			}
-			T v[LOADS_IN_FLIGHT], mm[LOADS_IN_FLIGHT];
-			bool ld[LOADS_IN_FLIGHT];
+				for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
+					src[u] = dm ? __ffs(dm) - 1 : -1;
+					dm &= dm ? dm - 1 : 0u;
+				}
+				T v[LOADS_IN_FLIGHT], mm[LOADS_IN_FLIGHT];
+				bool ld[LOADS_IN_FLIGHT];
 #pragma unroll
-			for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
-				const int sl = src[u] < 0 ? 0 : src[u];
-				const uint32_t c = __shfl_sync(FULL, cand[k], sl);
-				const uint32_t pp = __shfl_sync(FULL, p[k], sl);
-				mm[u] = __shfl_sync(FULL, m2, sl);
-				ld[u] = src[u] >= 0 && ((c >> lane) & 1u);
-				v[u] = ld[u] ? dim2[pp + lane] : T(0);
-			}
+				for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
+					const int sl = src[u] < 0 ? 0 : src[u];
+					const uint32_t c = __shfl_sync(FULL, cand[k], sl);
+					const uint32_t pp = __shfl_sync(FULL, p[k], sl);
+					mm[u] = __shfl_sync(FULL, m2, sl);
+					ld[u] = src[u] >= 0 && ((c >> lane) & 1u);
+					v[u] = ld[u] ? dim2[pp + lane] : T(0);
+				}
 #pragma unroll
-			for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
-				const uint32_t a = __ballot_sync(FULL, ld[u] && (mm[u] <= v[u]));
-				if (src[u] >= 0 && lane == (uint32_t) src[u])
-					am[k] = a;
+				for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
+					const uint32_t a = __ballot_sync(FULL, ld[u] && (mm[u] <= v[u]));
+					if (src[u] >= 0 && lane == (uint32_t) src[u])
+						am[k] = a;
+				}
 			}
 		}
 	}
@@ -577,51 +577,51 @@ __device__ __forceinline__ void emit_rows(const TreeDev<T> &t, uint32_t p, uint3
 	if constexpr (!POINTS) {
 		if (dm)
 			emit_id_quads(ids, p, am, out_base, dm, static_cast<uint32_t *>(out), capacity);
-		return;
-	}
-	while (dm) {
-		int src[LOADS_IN_FLIGHT];
+	} else {
+		while (dm) {
+			int src[LOADS_IN_FLIGHT];
 #pragma unroll
-		for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
-			src[u] = dm ? __ffs(dm) - 1 : -1;
-			dm &= dm ? dm - 1 : 0u;
-		}
-		uint32_t a[LOADS_IN_FLIGHT];
-		uint64_t ob[LOADS_IN_FLIGHT];
-		uint32_t vid[LOADS_IN_FLIGHT];
-		T v1[LOADS_IN_FLIGHT], v2[LOADS_IN_FLIGHT];
-#pragma unroll
-		for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
-			const int sl = src[u] < 0 ? 0 : src[u];
-			const uint32_t av = __shfl_sync(FULL, am, sl);
-			a[u] = src[u] >= 0 ? av : 0u;
-			const uint32_t pp = __shfl_sync(FULL, p, sl);
-			ob[u] = __shfl_sync(FULL, out_base, sl);
-			const bool on = (a[u] >> lane) & 1u;
-			const uint32_t h = pp + lane;
-			if constexpr (HAS_ID)
-				vid[u] = on ? ids[h] : 0u;
-			if constexpr (POINTS) {
-				v1[u] = on ? d1[h] : T(0);
-				v2[u] = on ? d2[h] : T(0);
+			for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
+				src[u] = dm ? __ffs(dm) - 1 : -1;
+				dm &= dm ? dm - 1 : 0u;
 			}
-		}
+			uint32_t a[LOADS_IN_FLIGHT];
+			uint64_t ob[LOADS_IN_FLIGHT];
+			uint32_t vid[LOADS_IN_FLIGHT];
+			T v1[LOADS_IN_FLIGHT], v2[LOADS_IN_FLIGHT];
 #pragma unroll
-		for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
-			if (!((a[u] >> lane) & 1u))
-				continue;
-			const uint64_t o = ob[u] + __popc(a[u] & lanemask_lt());
-			if (o >= capacity)
-				continue;
-			if constexpr (POINTS) {
-				Pt rec;
-				rec.dim1 = v1[u];
-				rec.dim2 = v2[u];
+			for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
+				const int sl = src[u] < 0 ? 0 : src[u];
+				const uint32_t av = __shfl_sync(FULL, am, sl);
+				a[u] = src[u] >= 0 ? av : 0u;
+				const uint32_t pp = __shfl_sync(FULL, p, sl);
+				ob[u] = __shfl_sync(FULL, out_base, sl);
+				const bool on = (a[u] >> lane) & 1u;
+				const uint32_t h = pp + lane;
 				if constexpr (HAS_ID)
-					rec.id = vid[u];
-				static_cast<Pt *>(out)[o] = rec;
-			} else {
-				static_cast<uint32_t *>(out)[o] = vid[u];
+					vid[u] = on ? ids[h] : 0u;
+				if constexpr (POINTS) {
+					v1[u] = on ? d1[h] : T(0);
+					v2[u] = on ? d2[h] : T(0);
+				}
+			}
+#pragma unroll
+			for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
+				if (!((a[u] >> lane) & 1u))
+					continue;
+				const uint64_t o = ob[u] + __popc(a[u] & lanemask_lt());
+				if (o >= capacity)
+					continue;
+				if constexpr (POINTS) {
+					Pt rec;
+					rec.dim1 = v1[u];
+					rec.dim2 = v2[u];
+					if constexpr (HAS_ID)
+						rec.id = vid[u];
+					static_cast<Pt *>(out)[o] = rec;
+				} else {
+					static_cast<uint32_t *>(out)[o] = vid[u];
+				}
 			}
 		}
 	}
