@@ -33,7 +33,6 @@ namespace {
 
 constexpr uint32_t MODE_THREE = 3, MODE_LEFT = 1, MODE_RIGHT = 2;
 constexpr uint32_t FULL = 0xFFFFFFFFu;
-constexpr int LOADS_IN_FLIGHT = 8;  // chunk tests (or emit rows) batched per warp before their results are used
 
 __device__ __forceinline__ bool occ_bit(const uint32_t *occ, uint32_t h) { return (occ[h >> 5] >> (h & 31)) & 1u; }
 
@@ -45,21 +44,29 @@ struct QDev {
 	const T *min2;
 };
 
+// Alive records cover a "block" of 64 consecutive slots of one level (two
+// 128-byte rows of a 4-byte field): (block base position, query, mask of reported
+// slots, low and high word).  Block bases are multiples of 64.
 struct WorkDev {
-	uint2 *rec_pq;      // alive records: (chunk base position, query)
-	uint32_t *rec_am;   // ... and their masks of reported slots
+	uint4 *rec;            // alive records of every level, level regions in order
 	uint64_t rec_cap;
 	uint4 *path0, *path1;  // boundary-path tasks (position, query, mode), double-buffered by level parity
 	uint4 *seed0, *seed1;  // report-above seeds (chunk base, query, candidate mask), idem
 	uint32_t path_cap;     // entries of each path / seed buffer (2 per query)
-	uint2 *ro_pq;          // reported boundary nodes: (chunk base, query) ...
-	uint32_t *ro_bit;      // ... and the node's bit (never expanded)
+	uint4 *ro;             // reported boundary nodes as one-bit block records (never expanded)
 	uint32_t ro_cap;
 	uint64_t *counts;
 	uint64_t *cursor;
 	const uint64_t *offsets;
 	BatchCtl *ctl;
 };
+
+// The block record of a 32-slot chunk (base pos32, a multiple of 32) and its mask.
+__device__ __forceinline__ uint4 block_record(uint32_t pos32, uint32_t q, uint32_t bits32)
+{
+	const bool upper = (pos32 & 32u) != 0;
+	return make_uint4(pos32 & ~63u, q, upper ? 0u : bits32, upper ? bits32 : 0u);
+}
 
 template <typename T>
 __device__ void path_step(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev &w, uint32_t d, uint4 task)
@@ -75,12 +82,10 @@ __device__ void path_step(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev 
 	const bool rep = kind == PST_Q_THREE ? (min1 <= v1 && v1 <= max1) : kind == PST_Q_LEFT ? (v1 <= max1) : (v1 >= min1);
 	if (rep) {
 		const uint32_t i = atomicAdd(&w.ctl->rec_cnt, 1u);
-		if (i < w.ro_cap) {
-			w.ro_pq[i] = make_uint2(h & ~31u, q);
-			w.ro_bit[i] = 1u << (h & 31);
-		} else {
+		if (i < w.ro_cap)
+			w.ro[i] = block_record(h & ~31u, q, 1u << (h & 31));
+		else
 			atomicOr(&w.ctl->flags, BATCH_FLAG_INTERNAL);
-		}
 		atomicAdd((unsigned long long *) &w.counts[q], 1ull);
 	}
 	if (d + 1 >= t.levels)
@@ -145,13 +150,6 @@ __device__ void path_step(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev 
 	}
 }
 
-// Dense tasks over 4-byte values, 16 bytes per lane: a task's ROWS consecutive rows
-// of 32 slots (ROWS * 128 bytes) are read by 8 * ROWS lanes with one vector load
-// each, so one load instruction of the warp covers 32 / (8 * ROWS) tasks and a lane
-// keeps QUAD_GROUPS of them in flight.  Each 8-lane group ORs its nibbles into the
-// row's 32-bit mask, which the task's owner lane then reads.
-constexpr int QUAD_GROUPS = 4;
-
 template <typename T>
 struct Vec4;
 template <>
@@ -163,189 +161,37 @@ struct Vec4<int32_t> {
 	using V = int4;
 };
 
-// The owners (lanes of `dm`, lowest first) of the next QUAD_GROUPS * TPG tasks.
-template <int N>
-__device__ __forceinline__ void next_owners(uint32_t &dm, int (&s)[N])
+// Four consecutive values from a 16-byte aligned address (two loads for doubles).
+template <typename T>
+__device__ __forceinline__ void load_quad(const T *__restrict__ p, T (&v)[4])
 {
-#pragma unroll
-	for (int i = 0; i < N; i++) {
-		s[i] = dm ? __ffs(dm) - 1 : -1;
-		dm &= dm ? dm - 1 : 0u;
+	if constexpr (sizeof(T) == 4) {
+		using V = typename Vec4<T>::V;
+		const V x = *reinterpret_cast<const V *>(p);
+		v[0] = x.x;
+		v[1] = x.y;
+		v[2] = x.z;
+		v[3] = x.w;
+	} else {
+		const double2 a = reinterpret_cast<const double2 *>(p)[0];
+		const double2 b = reinterpret_cast<const double2 *>(p)[1];
+		v[0] = a.x;
+		v[1] = a.y;
+		v[2] = b.x;
+		v[3] = b.y;
 	}
 }
 
-// Owner lane of the task this lane serves in group u (slot g of TPG), -1 if none.
-template <int TPG, int N>
-__device__ __forceinline__ int group_src(const int (&s)[N], int u, uint32_t g)
-{
-	int src = s[u * TPG];
-#pragma unroll
-	for (int j = 1; j < TPG; j++)
-		src = g == (uint32_t) j ? s[u * TPG + j] : src;
-	return src;
-}
-
-// Slot j of group u owned by this lane, -1 if none.
-template <int TPG, int N>
-__device__ __forceinline__ int owned_slot(const int (&s)[N], int u, uint32_t lane)
-{
-	int myj = -1;
-#pragma unroll
-	for (int j = 0; j < TPG; j++)
-		myj = s[u * TPG + j] == (int) lane ? j : myj;
-	return myj;
-}
-
-template <typename T, int ROWS>
-__device__ __forceinline__ void dense_quads(const T *__restrict__ dim2, uint32_t p, const uint32_t (&cand)[ROWS],
-                                            T m2, uint32_t dm, uint32_t (&am)[ROWS])
-{
-	using V = typename Vec4<T>::V;
-	constexpr int LPT = 8 * ROWS;  // lanes per task
-	constexpr int TPG = 32 / LPT;  // tasks per load instruction
-	const uint32_t lane = lane_id();
-	const uint32_t g = lane / LPT, sub = lane % LPT, r = sub / 8, qd = sub % 8;
-	while (dm) {
-		int s[QUAD_GROUPS * TPG];
-		next_owners(dm, s);
-		V v[QUAD_GROUPS];
-		uint32_t nib[QUAD_GROUPS];
-		T mm[QUAD_GROUPS];
-#pragma unroll
-		for (int u = 0; u < QUAD_GROUPS; u++) {
-			const int src = group_src<TPG>(s, u, g);
-			const int sl = src < 0 ? 0 : src;
-			uint32_t crow = __shfl_sync(FULL, cand[0], sl);
-			if constexpr (ROWS == 2) {
-				const uint32_t c1 = __shfl_sync(FULL, cand[1], sl);
-				crow = r ? c1 : crow;
-			}
-			const uint32_t pp = __shfl_sync(FULL, p, sl);
-			mm[u] = __shfl_sync(FULL, m2, sl);
-			nib[u] = src >= 0 ? (crow >> (4 * qd)) & 0xFu : 0u;
-			v[u] = nib[u] ? *reinterpret_cast<const V *>(dim2 + pp + 32 * r + 4 * qd) : V{};
-		}
-#pragma unroll
-		for (int u = 0; u < QUAD_GROUPS; u++) {
-			const uint32_t b = nib[u];
-			const uint32_t bits = ((b & 1u) && mm[u] <= v[u].x ? 1u : 0u) | ((b & 2u) && mm[u] <= v[u].y ? 2u : 0u) |
-			                      ((b & 4u) && mm[u] <= v[u].z ? 4u : 0u) | ((b & 8u) && mm[u] <= v[u].w ? 8u : 0u);
-			uint32_t row = bits << (4 * qd);
-			row |= __shfl_xor_sync(FULL, row, 1);
-			row |= __shfl_xor_sync(FULL, row, 2);
-			row |= __shfl_xor_sync(FULL, row, 4);
-			const int myj = owned_slot<TPG>(s, u, lane);
-			const int base = myj < 0 ? 0 : myj * LPT;
-#pragma unroll
-			for (int rr = 0; rr < ROWS; rr++) {
-				const uint32_t val = __shfl_sync(FULL, row, base + 8 * rr);
-				if (myj >= 0)
-					am[rr] = val;
-			}
-		}
-	}
-}
-
-// Tests the 32*K chunk tasks held by a warp (lane l owns tasks (l, 0..K-1): chunk
-// base p[k], candidate lanes cand[k], the query's min2) and returns each task's
-// mask of reported slots in am[k].  A task with at most SPARSE_BITS candidates is
-// tested by its own lane, bit by bit; the others are tested by the whole warp, one
-// coalesced row each, LOADS_IN_FLIGHT rows issued before their ballots.
-constexpr int SPARSE_BITS = 6;
-
-template <typename T, int K>
-__device__ __forceinline__ void test_chunks(const T *__restrict__ dim2, const uint32_t (&p)[K],
-                                            const uint32_t (&cand)[K], T m2, uint32_t (&am)[K])
+// Appends each lane's non-empty records (at most K) to the level region (one atomic
+// per warp).
+template <int K>
+__device__ __forceinline__ void append_blocks(const WorkDev &w, uint32_t lvl, uint64_t region_base, const uint4 (&r)[K])
 {
 	const uint32_t lane = lane_id();
-	constexpr bool QUADS = sizeof(T) == 4;
-	uint32_t dense_mask[K];
-	uint32_t total = 0;
+	uint32_t nrec = 0;
 #pragma unroll
 	for (int k = 0; k < K; k++)
-		total += __popc(cand[k]);
-#pragma unroll
-	for (int k = 0; k < K; k++) {
-		am[k] = 0;
-		const uint32_t c = cand[k];
-		const bool dense = QUADS ? total > SPARSE_BITS : __popc(c) > SPARSE_BITS;
-		dense_mask[k] = __ballot_sync(FULL, dense);
-		if (!dense && c) {
-			// lane mode: a handful of slots of one 128-byte row
-			uint32_t bits = c, a = 0;
-			while (bits) {
-				const uint32_t b0 = __ffs(bits) - 1;
-				bits &= bits - 1;
-				if (bits) {
-					const uint32_t b1 = __ffs(bits) - 1;
-					bits &= bits - 1;
-					const T v0 = dim2[p[k] + b0], v1 = dim2[p[k] + b1];
-					a |= (m2 <= v0 ? 1u << b0 : 0u) | (m2 <= v1 ? 1u << b1 : 0u);
-				} else {
-					const T v0 = dim2[p[k] + b0];
-					a |= m2 <= v0 ? 1u << b0 : 0u;
-				}
-			}
-			am[k] = a;
-		}
-	}
-	if constexpr (QUADS) {
-		// rows of one task are consecutive: p[k] = p[0] + 32 k
-		if (dense_mask[0])
-			dense_quads<T, K>(dim2, p[0], cand, m2, dense_mask[0], am);
-	} else {
-#pragma unroll
-		for (int k = 0; k < K; k++) {
-			uint32_t dm = dense_mask[k];
-			while (dm) {
-				// up to LOADS_IN_FLIGHT dense tasks, lowest lanes first (warp-uniform)
-				int src[LOADS_IN_FLIGHT];
-#pragma unroll
-				for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
-					src[u] = dm ? __ffs(dm) - 1 : -1;
-					dm &= dm ? dm - 1 : 0u;
-				}
-				T v[LOADS_IN_FLIGHT], mm[LOADS_IN_FLIGHT];
-				bool ld[LOADS_IN_FLIGHT];
-#pragma unroll
-				for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
-					const int sl = src[u] < 0 ? 0 : src[u];
-					const uint32_t c = __shfl_sync(FULL, cand[k], sl);
-					const uint32_t pp = __shfl_sync(FULL, p[k], sl);
-					mm[u] = __shfl_sync(FULL, m2, sl);
-					ld[u] = src[u] >= 0 && ((c >> lane) & 1u);
-					v[u] = ld[u] ? dim2[pp + lane] : T(0);
-				}
-#pragma unroll
-				for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
-					const uint32_t a = __ballot_sync(FULL, ld[u] && (mm[u] <= v[u]));
-					if (src[u] >= 0 && lane == (uint32_t) src[u])
-						am[k] = a;
-				}
-			}
-		}
-	}
-}
-
-// Appends the warp's non-empty masks as alive records of level `lvl` (one atomic
-// per warp) and adds their sizes to the queries' counts (one atomic per run of
-// equal query ids).
-template <int K>
-__device__ __forceinline__ void append_records(const WorkDev &w, uint32_t lvl, uint64_t region_base,
-                                               const uint32_t (&p)[K], const uint32_t (&am)[K], uint32_t q,
-                                               bool valid)
-{
-	const uint32_t lane = lane_id();
-	uint32_t nrec = 0, pts = 0;
-#pragma unroll
-	for (int k = 0; k < K; k++) {
-		nrec += am[k] ? 1u : 0u;
-		pts += __popc(am[k]);
-	}
-	bool last;
-	const uint64_t run = warp_run_sum(valid ? q : 0xFFFFFFFFu, pts, &last);
-	if (valid && last && run)
-		atomicAdd((unsigned long long *) &w.counts[q], (unsigned long long) run);
+		nrec += (r[k].z | r[k].w) ? 1u : 0u;
 	const uint32_t inc = warp_incl_scan(nrec);
 	const uint32_t tot = __shfl_sync(FULL, inc, 31);
 	if (!tot)
@@ -365,13 +211,109 @@ __device__ __forceinline__ void append_records(const WorkDev &w, uint32_t lvl, u
 		return;
 	uint64_t s = slot0 + inc - nrec;
 #pragma unroll
-	for (int k = 0; k < K; k++) {
-		if (am[k]) {
-			w.rec_pq[s] = make_uint2(p[k], q);
-			w.rec_am[s] = am[k];
-			s++;
+	for (int k = 0; k < K; k++)
+		if (r[k].z | r[k].w)
+			w.rec[s++] = r[k];
+}
+
+// Adds the lanes' point counts to their queries' counts (one atomic per run of
+// equal query ids).
+__device__ __forceinline__ void add_counts(const WorkDev &w, uint32_t q, uint32_t pts, bool valid)
+{
+	bool last;
+	const uint64_t run = warp_run_sum(valid ? q : 0xFFFFFFFFu, pts, &last);
+	if (valid && last && run)
+		atomicAdd((unsigned long long *) &w.counts[q], (unsigned long long) run);
+}
+
+// Per-warp shared staging of the 32 records a warp holds: the records, the
+// candidate masks of their four child rows (parents' bits spread to their children,
+// ANDed with the occupancy), their queries' min2, the child rows found, and the
+// list of records that have any candidate at all.
+template <typename T>
+struct WarpStage {
+	uint4 rec[32];
+	uint4 cand[32];
+	uint4 rows[32];
+	T m2[32];
+	uint32_t live[32];
+};
+
+// Expands the records held by the warp (lane k owns record `mine`; the valid lanes
+// are a prefix) into their child records.  Each lane first stages its record's
+// candidate child slots; records without any (all children absent, e.g. above a
+// sparse last level) cost nothing more.  Then the whole warp takes the live records
+// U at a time: lane l tests the child slots [2b + 4l, 2b + 4l + 4) with one 16-byte
+// load (two for doubles), issued only where it has candidates; each 8-lane group
+// ORs its nibbles into one 32-slot child row, and the owner reads the four rows as
+// its two child records (blocks 2b and 2b + 64).
+template <typename T>
+__device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__restrict__ min2s, const uint4 &mine,
+                                               bool valid, WarpStage<T> &st, uint4 (&child)[2], uint32_t &pts)
+{
+	constexpr int U = sizeof(T) == 4 ? 4 : 2;  // records in flight
+	const uint32_t lane = lane_id();
+	const uint32_t r = lane >> 3, qd = lane & 7;
+	uint4 cand = make_uint4(0, 0, 0, 0);
+	if (valid) {
+		const uint4 occ = *reinterpret_cast<const uint4 *>(t.occ + ((2 * mine.x) >> 5));
+		cand = make_uint4(spread16(mine.z) & occ.x, spread16(mine.z >> 16) & occ.y, spread16(mine.w) & occ.z,
+		                  spread16(mine.w >> 16) & occ.w);
+	}
+	const bool live = (cand.x | cand.y | cand.z | cand.w) != 0;
+	const uint32_t lm = __ballot_sync(FULL, live);
+	const int nlive = __popc(lm);
+	if (live) {
+		st.rec[lane] = mine;
+		st.cand[lane] = cand;
+		st.m2[lane] = min2s[mine.y];
+		st.live[__popc(lm & lanemask_lt())] = lane;
+	}
+	__syncwarp();
+	const uint32_t *candw = reinterpret_cast<const uint32_t *>(st.cand);
+	for (int k0 = 0; k0 < nlive; k0 += U) {
+		uint32_t cn[U], kk[U];
+		T v[U][4];
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			const bool on = k0 + u < nlive;
+			const uint32_t k = st.live[on ? k0 + u : 0];
+			kk[u] = k;
+			const uint32_t c4 = on ? (candw[4 * k + r] >> (4 * qd)) & 0xFu : 0u;
+			cn[u] = c4;
+			if (c4) {
+				load_quad(t.dim2 + 2 * st.rec[k].x + 4 * lane, v[u]);
+			} else {
+#pragma unroll
+				for (int j = 0; j < 4; j++)
+					v[u][j] = T(0);
+			}
+		}
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			const T m2 = st.m2[kk[u]];
+			uint32_t bits = 0;
+#pragma unroll
+			for (int j = 0; j < 4; j++)
+				bits |= (((cn[u] >> j) & 1u) && m2 <= v[u][j]) ? 1u << j : 0u;
+			uint32_t row = bits << (4 * qd);
+			row |= __shfl_xor_sync(FULL, row, 1);
+			row |= __shfl_xor_sync(FULL, row, 2);
+			row |= __shfl_xor_sync(FULL, row, 4);
+			if (qd == 0 && k0 + u < nlive)
+				reinterpret_cast<uint32_t *>(st.rows)[4 * kk[u] + r] = row;
 		}
 	}
+	__syncwarp();
+	child[0] = child[1] = make_uint4(0, 0, 0, 0);
+	pts = 0;
+	if (live) {
+		const uint4 rw = st.rows[lane];
+		child[0] = make_uint4(2 * mine.x, mine.y, rw.x, rw.y);
+		child[1] = make_uint4(2 * mine.x + 64, mine.y, rw.z, rw.w);
+		pts = __popc(rw.x) + __popc(rw.y) + __popc(rw.z) + __popc(rw.w);
+	}
+	__syncwarp();  // the stage is reused by the warp's next batch
 }
 
 template <typename T>
@@ -383,6 +325,7 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs_level(TreeDev<T> t, QDev<T>
 	if (w.ctl->flags & BATCH_FLAG_TASK_OVERFLOW)
 		return;
 	__shared__ uint64_t s_base[2];
+	__shared__ WarpStage<T> s_stage[BFS_THREADS / 32];
 	if (threadIdx.x == 0) {
 		uint64_t b = 0;  // start of the previous level's records
 		for (uint32_t e = 0; e + 1 < d; e++)
@@ -399,7 +342,6 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs_level(TreeDev<T> t, QDev<T>
 	const uint64_t gtid = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	const uint64_t gwarps = gthreads / 32, gwarp = gtid / 32;
 	const uint32_t lane = lane_id();
-	const T *__restrict__ dim2 = t.dim2;
 
 	// boundary paths
 	const uint32_t np = min(w.ctl->path_cnt[d], w.path_cap);
@@ -408,33 +350,35 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs_level(TreeDev<T> t, QDev<T>
 		path_step<T>(t, qd, w, d, pin[i]);
 	__syncwarp();
 
-	// report-above seeds of this level (one chunk task each)
+	// report-above seeds of this level: one or two candidate slots each, tested by
+	// their own lane
 	const uint32_t ns = min(w.ctl->seed_cnt[d], w.path_cap);
 	const uint4 *sin = (d & 1) ? w.seed1 : w.seed0;
 	for (uint64_t wb = gwarp * 32; wb < ns; wb += gwarps * 32) {
 		const bool valid = wb + lane < ns;
 		const uint4 sd = valid ? sin[wb + lane] : make_uint4(0, 0, 0, 0);
-		const uint32_t p[1] = {sd.x};
-		const uint32_t cand[1] = {valid ? (sd.z & t.occ[sd.x >> 5]) : 0u};
-		const T m2 = cand[0] ? qd.min2[sd.y] : T(0);
-		uint32_t am[1];
-		test_chunks<T, 1>(dim2, p, cand, m2, am);
-		append_records<1>(w, d, base_cur, p, am, sd.y, valid);
+		uint32_t cand = valid ? (sd.z & t.occ[sd.x >> 5]) : 0u;
+		uint32_t am = 0;
+		const T m2 = cand ? qd.min2[sd.y] : T(0);
+		while (cand) {
+			const uint32_t bt = __ffs(cand) - 1;
+			cand &= cand - 1;
+			am |= m2 <= t.dim2[sd.x + bt] ? 1u << bt : 0u;
+		}
+		add_counts(w, sd.y, __popc(am), valid);
+		const uint4 one[1] = {am ? block_record(sd.x, sd.y, am) : make_uint4(0, 0, 0, 0)};
+		append_blocks<1>(w, d, base_cur, one);
 	}
 
-	// expansion of the previous level's alive records into their two child chunks
+	// expansion of the previous level's alive records into their child blocks
 	for (uint64_t wb = gwarp * 32; wb < n_prev; wb += gwarps * 32) {
 		const bool valid = wb + lane < n_prev;
-		const uint64_t idx = base_prev + wb + lane;
-		const uint2 pq = valid ? w.rec_pq[idx] : make_uint2(0, 0);
-		const uint32_t pam = valid ? w.rec_am[idx] : 0u;
-		const uint32_t lo = spread16(pam), hi = spread16(pam >> 16);
-		const uint32_t p[2] = {2 * pq.x, 2 * pq.x + 32};
-		const uint32_t cand[2] = {lo ? (lo & t.occ[p[0] >> 5]) : 0u, hi ? (hi & t.occ[p[1] >> 5]) : 0u};
-		const T m2 = (cand[0] | cand[1]) ? qd.min2[pq.y] : T(0);
-		uint32_t am[2];
-		test_chunks<T, 2>(dim2, p, cand, m2, am);
-		append_records<2>(w, d, base_cur, p, am, pq.y, valid);
+		const uint4 mine = valid ? w.rec[base_prev + wb + lane] : make_uint4(0, 0, 0, 0);
+		uint4 child[2];
+		uint32_t pts;
+		expand_records<T>(t, qd.min2, mine, valid, s_stage[threadIdx.x >> 5], child, pts);
+		add_counts(w, mine.y, pts, valid);
+		append_blocks<2>(w, d, base_cur, child);
 	}
 }
 
@@ -475,163 +419,10 @@ __global__ void k_check_kinds(const pst_query *raw, BatchCtl *ctl)
 	}
 }
 
-// Writes the results of up to 32 records (lane r owns record (p, am) whose results
-// start at out_base).  A record of at most SPARSE_BITS points is written by its own
-// lane; the others by the whole warp, one row each, LOADS_IN_FLIGHT rows loaded
-// before they are stored.
-template <typename T, bool HAS_ID, bool POINTS>
-__device__ __forceinline__ void emit_one(const TreeDev<T> &t, uint32_t h, uint64_t o, void *__restrict__ out)
-{
-	using Pt = Point<T, HAS_ID>;
-	if constexpr (POINTS) {
-		Pt rec;
-		rec.dim1 = t.dim1[h];
-		rec.dim2 = t.dim2[h];
-		if constexpr (HAS_ID)
-			rec.id = t.id[h];
-		static_cast<Pt *>(out)[o] = rec;
-	} else {
-		static_cast<uint32_t *>(out)[o] = t.id[h];
-	}
-}
-
-// Dense id records, 16 bytes per lane: 8 lanes read a record's row of 32 ids with
-// one vector load each and store the reported ones at their compacted offsets.
-__device__ __forceinline__ void emit_id_quads(const uint32_t *__restrict__ ids, uint32_t p, uint32_t am,
-                                              uint64_t out_base, uint32_t dm, uint32_t *__restrict__ out,
-                                              uint64_t capacity)
-{
-	constexpr int TPG = 4;
-	const uint32_t lane = lane_id();
-	const uint32_t g = lane / 8, qd = lane % 8;
-	const uint32_t below = (1u << (4 * qd)) - 1u;
-	while (dm) {
-		int s[QUAD_GROUPS * TPG];
-		next_owners(dm, s);
-		uint4 v[QUAD_GROUPS];
-		uint32_t nib[QUAD_GROUPS];
-		uint64_t o[QUAD_GROUPS];
-#pragma unroll
-		for (int u = 0; u < QUAD_GROUPS; u++) {
-			const int src = group_src<TPG>(s, u, g);
-			const int sl = src < 0 ? 0 : src;
-			const uint32_t a = __shfl_sync(FULL, am, sl);
-			const uint32_t pp = __shfl_sync(FULL, p, sl);
-			const uint64_t ob = __shfl_sync(FULL, out_base, sl);
-			nib[u] = src >= 0 ? (a >> (4 * qd)) & 0xFu : 0u;
-			o[u] = ob + __popc(a & below);
-			v[u] = nib[u] ? *reinterpret_cast<const uint4 *>(ids + pp + 4 * qd) : make_uint4(0, 0, 0, 0);
-		}
-#pragma unroll
-		for (int u = 0; u < QUAD_GROUPS; u++) {
-			uint64_t oo = o[u];
-			const uint32_t b = nib[u];
-			const uint32_t vals[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
-#pragma unroll
-			for (int j = 0; j < 4; j++) {
-				if ((b >> j) & 1u) {
-					if (oo < capacity)
-						out[oo] = vals[j];
-					oo++;
-				}
-			}
-		}
-	}
-}
-
-template <typename T, bool HAS_ID, bool POINTS>
-__device__ __forceinline__ void emit_rows(const TreeDev<T> &t, uint32_t p, uint32_t am, uint64_t out_base,
-                                          void *__restrict__ out, uint64_t capacity)
-{
-	using Pt = Point<T, HAS_ID>;
-	const uint32_t lane = lane_id();
-	const bool dense = __popc(am) > SPARSE_BITS;
-	if (!dense && am && out_base + __popc(am) <= capacity) {
-		uint32_t bits = am;
-		uint64_t o = out_base;
-		while (bits) {
-			const uint32_t b0 = __ffs(bits) - 1;
-			bits &= bits - 1;
-			if (bits) {
-				const uint32_t b1 = __ffs(bits) - 1;
-				bits &= bits - 1;
-				if constexpr (POINTS) {
-					emit_one<T, HAS_ID, POINTS>(t, p + b0, o, out);
-					emit_one<T, HAS_ID, POINTS>(t, p + b1, o + 1, out);
-				} else {
-					const uint32_t i0 = t.id[p + b0], i1 = t.id[p + b1];
-					static_cast<uint32_t *>(out)[o] = i0;
-					static_cast<uint32_t *>(out)[o + 1] = i1;
-				}
-				o += 2;
-			} else {
-				emit_one<T, HAS_ID, POINTS>(t, p + b0, o, out);
-				o += 1;
-			}
-		}
-	}
-	const uint32_t *__restrict__ ids = t.id;
-	const T *__restrict__ d1 = t.dim1;
-	const T *__restrict__ d2 = t.dim2;
-	uint32_t dm = __ballot_sync(FULL, dense);
-	if constexpr (!POINTS) {
-		if (dm)
-			emit_id_quads(ids, p, am, out_base, dm, static_cast<uint32_t *>(out), capacity);
-	} else {
-		while (dm) {
-			int src[LOADS_IN_FLIGHT];
-#pragma unroll
-			for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
-				src[u] = dm ? __ffs(dm) - 1 : -1;
-				dm &= dm ? dm - 1 : 0u;
-			}
-			uint32_t a[LOADS_IN_FLIGHT];
-			uint64_t ob[LOADS_IN_FLIGHT];
-			uint32_t vid[LOADS_IN_FLIGHT];
-			T v1[LOADS_IN_FLIGHT], v2[LOADS_IN_FLIGHT];
-#pragma unroll
-			for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
-				const int sl = src[u] < 0 ? 0 : src[u];
-				const uint32_t av = __shfl_sync(FULL, am, sl);
-				a[u] = src[u] >= 0 ? av : 0u;
-				const uint32_t pp = __shfl_sync(FULL, p, sl);
-				ob[u] = __shfl_sync(FULL, out_base, sl);
-				const bool on = (a[u] >> lane) & 1u;
-				const uint32_t h = pp + lane;
-				if constexpr (HAS_ID)
-					vid[u] = on ? ids[h] : 0u;
-				if constexpr (POINTS) {
-					v1[u] = on ? d1[h] : T(0);
-					v2[u] = on ? d2[h] : T(0);
-				}
-			}
-#pragma unroll
-			for (int u = 0; u < LOADS_IN_FLIGHT; u++) {
-				if (!((a[u] >> lane) & 1u))
-					continue;
-				const uint64_t o = ob[u] + __popc(a[u] & lanemask_lt());
-				if (o >= capacity)
-					continue;
-				if constexpr (POINTS) {
-					Pt rec;
-					rec.dim1 = v1[u];
-					rec.dim2 = v2[u];
-					if constexpr (HAS_ID)
-						rec.id = vid[u];
-					static_cast<Pt *>(out)[o] = rec;
-				} else {
-					static_cast<uint32_t *>(out)[o] = vid[u];
-				}
-			}
-		}
-	}
-}
-
 // Output slot of this lane's record inside its query's result: one atomic per run
 // of equal query ids on the query's cursor.
-__device__ __forceinline__ uint64_t claim_output(const WorkDev &w, uint32_t q, uint32_t am, bool valid)
+__device__ __forceinline__ uint64_t claim_output(const WorkDev &w, uint32_t q, uint32_t pc, bool valid)
 {
-	const uint32_t pc = __popc(am);
 	bool last;
 	const uint64_t run = warp_run_sum(valid ? q : 0xFFFFFFFFu, pc, &last);
 	const uint32_t lastmask = __ballot_sync(FULL, last);
@@ -640,13 +431,79 @@ __device__ __forceinline__ uint64_t claim_output(const WorkDev &w, uint32_t q, u
 	if (valid && last && run)
 		rb = atomicAdd((unsigned long long *) &w.cursor[q], (unsigned long long) run);
 	rb = __shfl_sync(FULL, rb, run_last);
-	return (valid && am) ? w.offsets[q] + rb + run - pc : 0;
+	return (valid && pc) ? w.offsets[q] + rb + run - pc : 0;
+}
+
+// Writes the results of the warp's records (lane k owns record `mine`, whose results
+// start at out_base; the valid lanes are a prefix): the lanes stage their records
+// and offsets, then the warp writes U records at a time, each by the whole warp,
+// lane l taking slots 2l and 2l + 1 of the 64-slot block.
+struct EmitStage {
+	uint4 rec[32];
+	unsigned long long ob[32];
+};
+
+template <typename T, bool HAS_ID, bool POINTS>
+__device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mine, uint64_t out_base, bool valid,
+                                            EmitStage &st, void *__restrict__ out, uint64_t capacity)
+{
+	using Pt = Point<T, HAS_ID>;
+	constexpr int U = POINTS ? 4 : 8;  // records in flight
+	const uint32_t lane = lane_id();
+	const uint32_t psh = (2 * lane) & 31;
+	st.rec[lane] = mine;
+	st.ob[lane] = out_base;
+	__syncwarp();
+	const int nrec = __popc(__ballot_sync(FULL, valid));
+	for (int k0 = 0; k0 < nrec; k0 += U) {
+		uint32_t b2[U], hb[U];
+		uint64_t o[U];
+		uint2 idv[U];
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			const int k = k0 + u;
+			const int src = k < nrec ? k : 0;
+			const uint4 rc = st.rec[src];
+			b2[u] = k < nrec ? ((lane < 16 ? rc.z : rc.w) >> psh) & 3u : 0u;
+			const uint32_t before = lane < 16 ? __popc(rc.z & ((1u << psh) - 1u))
+			                                  : __popc(rc.z) + __popc(rc.w & ((1u << psh) - 1u));
+			o[u] = st.ob[src] + before;
+			hb[u] = rc.x + 2 * lane;
+			if constexpr (!POINTS)
+				idv[u] = b2[u] ? *reinterpret_cast<const uint2 *>(t.id + hb[u]) : make_uint2(0, 0);
+		}
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			uint64_t oo = o[u];
+#pragma unroll
+			for (int j = 0; j < 2; j++) {
+				if ((b2[u] >> j) & 1u) {
+					if (oo < capacity) {
+						if constexpr (POINTS) {
+							const uint32_t h = hb[u] + j;
+							Pt rec;
+							rec.dim1 = t.dim1[h];
+							rec.dim2 = t.dim2[h];
+							if constexpr (HAS_ID)
+								rec.id = t.id[h];
+							static_cast<Pt *>(out)[oo] = rec;
+						} else {
+							static_cast<uint32_t *>(out)[oo] = j ? idv[u].y : idv[u].x;
+						}
+					}
+					oo++;
+				}
+			}
+		}
+	}
+	__syncwarp();  // the stage is reused by the warp's next batch
 }
 
 template <typename T, bool HAS_ID, bool POINTS>
 __global__ void __launch_bounds__(BFS_THREADS) k_emit(TreeDev<T> t, WorkDev w, void *out, uint64_t capacity)
 {
 	__shared__ uint64_t s_total;
+	__shared__ EmitStage s_stage[BFS_THREADS / 32];
 	if (threadIdx.x == 0) {
 		uint64_t b = 0;
 		for (uint32_t e = 0; e < t.levels; e++)
@@ -665,21 +522,34 @@ __global__ void __launch_bounds__(BFS_THREADS) k_emit(TreeDev<T> t, WorkDev w, v
 	const uint64_t gtid = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	const uint64_t gwarps = (uint64_t) gridDim.x * blockDim.x / 32, gwarp = gtid / 32;
 	for (uint64_t wb = gwarp * 32; wb < total; wb += gwarps * 32) {
-		const uint64_t idx = wb + lane;
-		const bool valid = idx < total;
-		const uint2 pq = valid ? w.rec_pq[idx] : make_uint2(0, 0);
-		const uint32_t am = valid ? w.rec_am[idx] : 0u;
-		const uint64_t ob = claim_output(w, pq.y, am, valid);
-		emit_rows<T, HAS_ID, POINTS>(t, pq.x, am, ob, out, capacity);
+		const bool valid = wb + lane < total;
+		const uint4 mine = valid ? w.rec[wb + lane] : make_uint4(0, 0, 0, 0);
+		const uint64_t ob = claim_output(w, mine.y, __popc(mine.z) + __popc(mine.w), valid);
+		emit_blocks<T, HAS_ID, POINTS>(t, mine, ob, valid, s_stage[threadIdx.x >> 5], out, capacity);
 	}
 	for (uint64_t wb = gwarp * 32; wb < nro; wb += gwarps * 32) {
-		const uint64_t idx = wb + lane;
-		const bool valid = idx < nro;
-		const uint2 pq = valid ? w.ro_pq[idx] : make_uint2(0, 0);
-		const uint32_t am = valid ? w.ro_bit[idx] : 0u;
-		const uint64_t ob = claim_output(w, pq.y, am, valid);
-		emit_rows<T, HAS_ID, POINTS>(t, pq.x, am, ob, out, capacity);
+		const bool valid = wb + lane < nro;
+		const uint4 mine = valid ? w.ro[wb + lane] : make_uint4(0, 0, 0, 0);
+		const uint64_t ob = claim_output(w, mine.y, __popc(mine.z) + __popc(mine.w), valid);
+		emit_blocks<T, HAS_ID, POINTS>(t, mine, ob, valid, s_stage[threadIdx.x >> 5], out, capacity);
 	}
+}
+
+// Grid of k_emit: as many CTAs as fit on the device at once (its own occupancy,
+// which can differ from the level kernel's), so the grid-stride loop has no tail wave.
+template <typename T, bool HAS_ID, bool POINTS>
+unsigned emit_grid()
+{
+	static const int occ = [] {
+		int o = 0;
+		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_emit<T, HAS_ID, POINTS>, BFS_THREADS, 0) !=
+		    cudaSuccess) {
+			cudaGetLastError();
+			o = 1;
+		}
+		return o > 0 ? o : 1;
+	}();
+	return (unsigned) (device_info().sms * occ);
 }
 
 template <typename T>
@@ -701,8 +571,8 @@ void Batch::release()
 		cudaGraphExecDestroy(graph_exec);
 	graph_exec = nullptr;
 	for (void *p : {(void *) q_raw, (void *) kind, min1, max1, min2, (void *) path0, (void *) path1, (void *) seed0,
-	                (void *) seed1, (void *) ro_pq, (void *) ro_bit, (void *) counts, (void *) cursor, (void *) offsets,
-	                (void *) scan_tmp, (void *) ctl, (void *) rec_pq, (void *) rec_am})
+	                (void *) seed1, (void *) ro, (void *) counts, (void *) cursor, (void *) offsets, (void *) scan_tmp,
+	                (void *) ctl, (void *) rec})
 		if (p)
 			cudaFree(p);
 	if (ctl_host)
@@ -712,8 +582,7 @@ void Batch::release()
 	q_raw = nullptr;
 	ctl_host = nullptr;
 	q_stage = nullptr;
-	rec_pq = nullptr;
-	rec_am = nullptr;
+	rec = nullptr;
 }
 
 static void dmalloc(void **p, size_t bytes)
@@ -757,8 +626,7 @@ void Batch::init(TreeStorage *t, const pst_batch_opts &o)
 	dmalloc((void **) &path1, (size_t) path_cap * sizeof(uint4));
 	dmalloc((void **) &seed0, (size_t) path_cap * sizeof(uint4));
 	dmalloc((void **) &seed1, (size_t) path_cap * sizeof(uint4));
-	dmalloc((void **) &ro_pq, (size_t) ro_cap * sizeof(uint2));
-	dmalloc((void **) &ro_bit, (size_t) ro_cap * 4);
+	dmalloc((void **) &ro, (size_t) ro_cap * sizeof(uint4));
 	dmalloc((void **) &counts, (size_t) max_q * 8);
 	dmalloc((void **) &cursor, (size_t) max_q * 8);
 	dmalloc((void **) &offsets, ((size_t) max_q + 1) * 8);
@@ -776,21 +644,17 @@ void Batch::grow_tasks(uint64_t cap, cudaStream_t s)
 {
 	// Stream-ordered on `s` (the stream of every pass that used the old frontier), so
 	// a growth does not wait for work on the device's other streams.
-	if (rec_pq)
-		PST_CUDA(cudaFreeAsync(rec_pq, s));
-	if (rec_am)
-		PST_CUDA(cudaFreeAsync(rec_am, s));
-	rec_pq = nullptr;
-	rec_am = nullptr;
-	for (auto pb : {std::make_pair((void **) &rec_pq, cap * sizeof(uint2)), std::make_pair((void **) &rec_am, cap * 4)}) {
-		cudaError_t e = cudaMallocAsync(pb.first, std::max<size_t>(pb.second, 16), s);
-		if (e == cudaErrorMemoryAllocation) {
-			cudaGetLastError();
-			task_cap = 0;
-			fail(PST_ERR_NOMEM, "frontier allocation of " + std::to_string(pb.second) + " B failed");
-		}
-		check_cuda(e, "cudaMallocAsync(frontier)");
+	if (rec)
+		PST_CUDA(cudaFreeAsync(rec, s));
+	rec = nullptr;
+	const size_t bytes = std::max<size_t>(cap * sizeof(uint4), 16);
+	cudaError_t e = cudaMallocAsync((void **) &rec, bytes, s);
+	if (e == cudaErrorMemoryAllocation) {
+		cudaGetLastError();
+		task_cap = 0;
+		fail(PST_ERR_NOMEM, "frontier allocation of " + std::to_string(bytes) + " B failed");
 	}
+	check_cuda(e, "cudaMallocAsync(frontier)");
 	task_cap = cap;
 	if (graph_exec) {
 		cudaGraphExecDestroy(graph_exec);
@@ -799,8 +663,7 @@ void Batch::grow_tasks(uint64_t cap, cudaStream_t s)
 }
 
 #define PST_WORKDEV                                                                                                   \
-	WorkDev w{rec_pq, rec_am, task_cap, path0, path1, seed0, seed1, path_cap, ro_pq, ro_bit, ro_cap, counts, cursor, \
-	          offsets, ctl}
+	WorkDev w{rec, task_cap, path0, path1, seed0, seed1, path_cap, ro, ro_cap, counts, cursor, offsets, ctl}
 
 template <typename T>
 void Batch::enqueue_count(cudaStream_t s)
@@ -827,7 +690,7 @@ void Batch::enqueue_emit_t(void *out, uint64_t capacity, cudaStream_t s)
 {
 	TreeDev<T> tv = tree->view<T>();
 	PST_WORKDEV;
-	k_emit<T, HAS_ID, POINTS><<<grid, threads, 0, s>>>(tv, w, out, capacity);
+	k_emit<T, HAS_ID, POINTS><<<emit_grid<T, HAS_ID, POINTS>(), threads, 0, s>>>(tv, w, out, capacity);
 	PST_CUDA(cudaGetLastError());
 }
 
@@ -989,25 +852,22 @@ constexpr size_t NA_PATH1 = NA_PATH0 + 256;
 constexpr size_t NA_SEED0 = NA_PATH1 + 256;
 constexpr size_t NA_SEED1 = NA_SEED0 + 256;
 constexpr uint32_t NA_RO_CAP = 2 * 32;  // two boundary results per level
-constexpr size_t NA_RO_PQ = NA_SEED1 + 256;
-constexpr size_t NA_RO_BIT = NA_RO_PQ + NA_RO_CAP * sizeof(uint2);
-constexpr size_t NA_COUNTS = NA_RO_BIT + 256;
+constexpr size_t NA_RO = NA_SEED1 + 256;
+constexpr size_t NA_COUNTS = NA_RO + NA_RO_CAP * sizeof(uint4);
 constexpr size_t NA_CURSOR = NA_COUNTS + 256;
 constexpr size_t NA_OFFSETS = NA_CURSOR + 256;
 constexpr size_t NA_SCAN = NA_OFFSETS + 256;
 constexpr size_t NA_RECS = NA_SCAN + 256;
-// alive records (8 B position/query + 4 B mask) share the rest
-constexpr uint64_t NA_REC_CAP = (NOALLOC_SCRATCH_BYTES - NA_RECS) / (sizeof(uint2) + 4) / 64 * 64;
-constexpr size_t NA_REC_AM = NA_RECS + NA_REC_CAP * sizeof(uint2);
+// alive records (16 B each) take the rest
+constexpr uint64_t NA_REC_CAP = (NOALLOC_SCRATCH_BYTES - NA_RECS) / sizeof(uint4) / 64 * 64;
 static_assert(sizeof(BatchCtl) <= NA_QRAW, "control block");
-static_assert(NA_RO_CAP * 4 <= 256, "boundary-result bits");
-static_assert(NA_REC_AM + NA_REC_CAP * 4 <= NOALLOC_SCRATCH_BYTES, "scratch layout");
-// One query has at most one alive record per 32-slot chunk of every level, plus the
-// records of report-above subtrees that still share a chunk with another subtree:
-// a seed's subtree shares chunks for its first five levels and a query leaves at
-// most two seeds per level, so at most 10 more per level: 2^L/16 + 12L + 32 records
-// for a tree of L levels.
-static_assert((1ull << NOALLOC_MAX_LEVELS) / 16 + 12 * NOALLOC_MAX_LEVELS + 32 <= NA_REC_CAP, "frontier bound");
+static_assert(NA_RECS + NA_REC_CAP * sizeof(uint4) <= NOALLOC_SCRATCH_BYTES, "scratch layout");
+// One query has at most one alive record per 64-slot block of every level, plus the
+// records of report-above subtrees that still share a block with another subtree:
+// a seed's subtree shares blocks for its first six levels and a query leaves at
+// most two seeds per level, so at most 12 more per level: fewer than
+// 2^L/32 + 14L + 64 records for a tree of L levels.
+static_assert((1ull << NOALLOC_MAX_LEVELS) / 32 + 14 * NOALLOC_MAX_LEVELS + 64 <= NA_REC_CAP, "frontier bound");
 
 std::mutex g_noalloc_mu;
 unsigned char *g_noalloc_ptr[64] = {};
@@ -1041,14 +901,12 @@ uint64_t noalloc_run(TreeStorage &t, const pst_query &q, pst_ret ret, void *out,
 	uint4 *path1 = reinterpret_cast<uint4 *>(base + NA_PATH1);
 	uint4 *seed0 = reinterpret_cast<uint4 *>(base + NA_SEED0);
 	uint4 *seed1 = reinterpret_cast<uint4 *>(base + NA_SEED1);
-	uint2 *ro_pq = reinterpret_cast<uint2 *>(base + NA_RO_PQ);
-	uint32_t *ro_bit = reinterpret_cast<uint32_t *>(base + NA_RO_BIT);
+	uint4 *ro = reinterpret_cast<uint4 *>(base + NA_RO);
 	uint64_t *counts = reinterpret_cast<uint64_t *>(base + NA_COUNTS);
 	uint64_t *cursor = reinterpret_cast<uint64_t *>(base + NA_CURSOR);
 	uint64_t *offsets = reinterpret_cast<uint64_t *>(base + NA_OFFSETS);
 	uint64_t *scan = reinterpret_cast<uint64_t *>(base + NA_SCAN);
-	uint2 *rec_pq = reinterpret_cast<uint2 *>(base + NA_RECS);
-	uint32_t *rec_am = reinterpret_cast<uint32_t *>(base + NA_REC_AM);
+	uint4 *rec = reinterpret_cast<uint4 *>(base + NA_RECS);
 
 	// The array keeps the previous call's contents: reset everything that must
 	// start at zero (control block with nq = 1, count, output cursor).
@@ -1064,8 +922,7 @@ uint64_t noalloc_run(TreeStorage &t, const pst_query &q, pst_ret ret, void *out,
 	const unsigned grid = (unsigned) device_info().sms * (unsigned) std::max(occ, 1);
 	TreeDev<T> tv = t.view<T>();
 	QDev<T> qd{kind, min1, max1, min2};
-	WorkDev w{rec_pq, rec_am, NA_REC_CAP, path0, path1, seed0, seed1, 2u, ro_pq, ro_bit, NA_RO_CAP,
-	          counts, cursor, offsets, ctl};
+	WorkDev w{rec, NA_REC_CAP, path0, path1, seed0, seed1, 2u, ro, NA_RO_CAP, counts, cursor, offsets, ctl};
 	k_check_kinds<<<1, 32, 0, s>>>(qraw, ctl);
 	k_unpack_queries<T><<<1, 32, 0, s>>>(qraw, ctl, kind, min1, max1, min2, path0);
 	for (uint32_t d = 0; d < tv.levels; d++)
@@ -1081,11 +938,11 @@ uint64_t noalloc_run(TreeStorage &t, const pst_query &q, pst_ret ret, void *out,
 		return h.total;
 	const bool has_id = t.idtype == PST_ID_U32;
 	if (ret == PST_RET_IDS)
-		k_emit<T, true, false><<<grid, BFS_THREADS, 0, s>>>(tv, w, out, capacity);
+		k_emit<T, true, false><<<emit_grid<T, true, false>(), BFS_THREADS, 0, s>>>(tv, w, out, capacity);
 	else if (has_id)
-		k_emit<T, true, true><<<grid, BFS_THREADS, 0, s>>>(tv, w, out, capacity);
+		k_emit<T, true, true><<<emit_grid<T, true, true>(), BFS_THREADS, 0, s>>>(tv, w, out, capacity);
 	else
-		k_emit<T, false, true><<<grid, BFS_THREADS, 0, s>>>(tv, w, out, capacity);
+		k_emit<T, false, true><<<emit_grid<T, false, true>(), BFS_THREADS, 0, s>>>(tv, w, out, capacity);
 	PST_CUDA(cudaGetLastError());
 	PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
 	PST_CUDA(cudaStreamSynchronize(s));

@@ -41,14 +41,12 @@ struct Batch {
 	uint32_t *kind = nullptr;
 	void *min1 = nullptr, *max1 = nullptr, *min2 = nullptr;
 	// frontier and results
-	uint2 *rec_pq = nullptr;   // alive records: (chunk base position, query)
-	uint32_t *rec_am = nullptr; // ... and their masks of reported slots
+	uint4 *rec = nullptr;       // alive records: (64-slot block base, query, reported-slot mask lo, hi)
 	uint64_t task_cap = 0;      // alive-record capacity
 	uint4 *path0 = nullptr, *path1 = nullptr;
 	uint4 *seed0 = nullptr, *seed1 = nullptr;
 	uint32_t path_cap = 0;
-	uint2 *ro_pq = nullptr;     // reported boundary nodes
-	uint32_t *ro_bit = nullptr;
+	uint4 *ro = nullptr;        // reported boundary nodes, as one-bit records
 	uint32_t ro_cap = 0;
 	uint64_t *counts = nullptr, *cursor = nullptr, *offsets = nullptr, *scan_tmp = nullptr;
 	BatchCtl *ctl = nullptr;

@@ -429,9 +429,9 @@ uint32_t server_add_tree(Server *s, TreeStorage *t)
 		pst_batch_opts bo{};
 		bo.max_queries = s->opts.max_batch;
 		bo.use_graph = s->opts.use_graph;
-		// frontier sized from the tree (a quarter record per point) so that batches
+		// frontier sized from the tree (one 64-slot record per 8 points) so that batches
 		// rarely grow it while requests wait
-		bo.task_capacity = std::max<uint64_t>(1ull << 16, t->n / 4);
+		bo.task_capacity = std::max<uint64_t>(1ull << 16, t->n / 8);
 		sl->eng.init(t, bo);
 		check_cuda(cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking), "cudaStreamCreate");
 		// warm-up pass: captures the slot's graph now rather than under the first request
