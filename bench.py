@@ -611,10 +611,12 @@ def main():
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None, "kernel": "batched search pass (k_bfs_level x levels + scan + k_emit)",
             "bytes_per_unit": BYTES_PER_PT, "units_per_launch": total, "peak_source": f"{peak_kind} hbm_gbs"}
-    prof = ROOT / "profiles" / "traffic.json"
-    if prof.exists():
+    prof = ROOT / "profiles" / "search_traffic.json"
+    if prof.exists() and n == N_POINTS:
         try:
-            roof["traffic"] = json.loads(prof.read_text()).get("search_bytes_per_step")
+            tr = json.loads(prof.read_text())
+            roof["traffic"] = tr["search_bytes_per_step"]
+            roof["traffic_source"] = f"ncu dram bytes on {tr['measured_on']}, scaled to {tr['scaled_to']}"
         except Exception:
             pass
 
