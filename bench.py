@@ -249,10 +249,11 @@ def sweep(pst, torch, n, seed=1):
                 # one plain drop-in query (callee-allocated result), wall clock
                 name = {0: "three", 1: "left", 2: "right"}[kind]
                 args = (float(a[0]), float(b[0]), float(c[0])) if dt != "i32" else (int(a[0]), int(b[0]), int(c[0]))
-                tree.search(name, *args, ret=ret)
+                pst.free_device(tree.search_device(name, *args, ret=ret)[0])
                 torch.cuda.synchronize()
                 t1 = time.perf_counter()
-                k1 = len(tree.search(name, *args, ret=ret))
+                ptr, k1 = tree.search_device(name, *args, ret=ret)
+                pst.free_device(ptr)
                 plain_s = time.perf_counter() - t1
                 row = {"dtype": dt, "ids": has_id, "kind": name, "sel": s, "queries": SWEEP_BATCH,
                        "mean_points": total / SWEEP_BATCH, "batch_ms": ms, "pts_per_s": total / (ms / 1000),
@@ -592,15 +593,20 @@ def main():
     e2e_val = total / (statistics.mean(e2e_ms) / 1000.0) * world
     log(f"e2e {statistics.mean(e2e_ms):.3f} ms/step")
 
-    # ---- plain per-query drop-in path on a sample of the same queries
+    # ---- plain per-query drop-in path on a sample of the same queries: the blocking
+    # call that hands back a device array of exactly `count` ids (as the reference's
+    # searches do), released after each call
     plain_n = min(args.plain_queries, NQ)
     names = {0: "three", 1: "left", 2: "right"}
+    ptr, _ = tree.search_device(names[int(kinds[0])], float(min1[0]), float(max1[0]), float(min2[0]))
+    pst.free_device(ptr)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     plain_pts = 0
     for i in range(plain_n):
-        r = tree.search(names[int(kinds[i])], float(min1[i]), float(max1[i]), float(min2[i]))
-        plain_pts += len(r)
+        ptr, cnt = tree.search_device(names[int(kinds[i])], float(min1[i]), float(max1[i]), float(min2[i]))
+        pst.free_device(ptr)
+        plain_pts += cnt
     plain_s = time.perf_counter() - t0
     plain_qps = plain_n / plain_s
     log(f"plain per-query path: {plain_qps:.1f} queries/s")

@@ -19,6 +19,7 @@ from .pst import (  # noqa: F401
     StaticPSTGPUArr,
     calcNumMetacells,
     formMetacellTags,
+    free_device,
     intervalParallelSearch,
     lib,
     library_path,

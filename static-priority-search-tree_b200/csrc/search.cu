@@ -459,6 +459,7 @@ __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mi
 		uint32_t b2[U], hb[U];
 		uint64_t o[U];
 		uint2 idv[U];
+		T d1[POINTS ? U : 1][2], d2[POINTS ? U : 1][2];
 #pragma unroll
 		for (int u = 0; u < U; u++) {
 			const int k = k0 + u;
@@ -469,8 +470,29 @@ __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mi
 			                                  : __popc(rc.z) + __popc(rc.w & ((1u << psh) - 1u));
 			o[u] = st.ob[src] + before;
 			hb[u] = rc.x + 2 * lane;
-			if constexpr (!POINTS)
+			if constexpr (!POINTS || HAS_ID)
 				idv[u] = b2[u] ? *reinterpret_cast<const uint2 *>(t.id + hb[u]) : make_uint2(0, 0);
+			if constexpr (POINTS) {
+				// the slot pair's dim1 and dim2 with one 8-byte (16 for doubles) load each
+				d1[u][0] = d1[u][1] = d2[u][0] = d2[u][1] = T(0);
+				if (b2[u]) {
+					if constexpr (sizeof(T) == 4) {
+						const uint2 a = *reinterpret_cast<const uint2 *>(t.dim1 + hb[u]);
+						const uint2 c = *reinterpret_cast<const uint2 *>(t.dim2 + hb[u]);
+						memcpy(&d1[u][0], &a.x, 4);
+						memcpy(&d1[u][1], &a.y, 4);
+						memcpy(&d2[u][0], &c.x, 4);
+						memcpy(&d2[u][1], &c.y, 4);
+					} else {
+						const double2 a = *reinterpret_cast<const double2 *>(t.dim1 + hb[u]);
+						const double2 c = *reinterpret_cast<const double2 *>(t.dim2 + hb[u]);
+						d1[u][0] = a.x;
+						d1[u][1] = a.y;
+						d2[u][0] = c.x;
+						d2[u][1] = c.y;
+					}
+				}
+			}
 		}
 #pragma unroll
 		for (int u = 0; u < U; u++) {
@@ -480,12 +502,11 @@ __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mi
 				if ((b2[u] >> j) & 1u) {
 					if (oo < capacity) {
 						if constexpr (POINTS) {
-							const uint32_t h = hb[u] + j;
 							Pt rec;
-							rec.dim1 = t.dim1[h];
-							rec.dim2 = t.dim2[h];
+							rec.dim1 = d1[u][j];
+							rec.dim2 = d2[u][j];
 							if constexpr (HAS_ID)
-								rec.id = t.id[h];
+								rec.id = j ? idv[u].y : idv[u].x;
 							static_cast<Pt *>(out)[oo] = rec;
 						} else {
 							static_cast<uint32_t *>(out)[oo] = j ? idv[u].y : idv[u].x;
@@ -521,11 +542,24 @@ __global__ void __launch_bounds__(BFS_THREADS) k_emit(TreeDev<T> t, WorkDev w, v
 	const uint32_t lane = lane_id();
 	const uint64_t gtid = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	const uint64_t gwarps = (uint64_t) gridDim.x * blockDim.x / 32, gwarp = gtid / 32;
-	for (uint64_t wb = gwarp * 32; wb < total; wb += gwarps * 32) {
-		const bool valid = wb + lane < total;
-		const uint4 mine = valid ? w.rec[wb + lane] : make_uint4(0, 0, 0, 0);
-		const uint64_t ob = claim_output(w, mine.y, __popc(mine.z) + __popc(mine.w), valid);
-		emit_blocks<T, HAS_ID, POINTS>(t, mine, ob, valid, s_stage[threadIdx.x >> 5], out, capacity);
+	// Two batches in flight: the next batch's records are read and its output claimed
+	// (an atomic whose result is needed only one batch later) before this batch's
+	// results are written.
+	const uint64_t stride = gwarps * 32;
+	uint64_t wb = gwarp * 32;
+	bool v0 = wb + lane < total;
+	uint4 m0 = v0 ? w.rec[wb + lane] : make_uint4(0, 0, 0, 0);
+	uint64_t ob0 = wb < total ? claim_output(w, m0.y, __popc(m0.z) + __popc(m0.w), v0) : 0;
+	while (wb < total) {
+		const uint64_t nb = wb + stride;
+		const bool v1 = nb + lane < total;
+		const uint4 m1 = v1 ? w.rec[nb + lane] : make_uint4(0, 0, 0, 0);
+		const uint64_t ob1 = nb < total ? claim_output(w, m1.y, __popc(m1.z) + __popc(m1.w), v1) : 0;
+		emit_blocks<T, HAS_ID, POINTS>(t, m0, ob0, v0, s_stage[threadIdx.x >> 5], out, capacity);
+		wb = nb;
+		v0 = v1;
+		m0 = m1;
+		ob0 = ob1;
 	}
 	for (uint64_t wb = gwarp * 32; wb < nro; wb += gwarps * 32) {
 		const bool valid = wb + lane < nro;

@@ -183,6 +183,12 @@ def _take_device_result(ptr: int, count: int, rec: np.dtype | type) -> np.ndarra
             _check(lib().pst_free(C.c_void_p(ptr)))
 
 
+def free_device(ptr: int):
+    """Releases a result returned by a drop-in search (pst_free)."""
+    if ptr:
+        _check(lib().pst_free(C.c_void_p(ptr)))
+
+
 def make_queries(kinds, min1, max1, min2, dt: str) -> np.ndarray:
     """pst_query records (kind, bounds in the tree's value type)."""
     n = len(kinds)
@@ -248,6 +254,16 @@ class StaticPSTGPU:
     def _ret(self, ret):
         r = ret if isinstance(ret, str) else ("ids" if ret is np.uint32 else "points")
         return r, (np.uint32 if r == "ids" else self.rec_point)
+
+    def search_device(self, kind: str, min1=0, max1=0, min2=0, ret="ids", stream=None):
+        """The drop-in call itself: returns (device pointer, count) of the
+        library-allocated result, which the caller releases with free_device (the
+        reference's searches hand back a cudaMalloc'd array the same way)."""
+        r, _ = self._ret(ret)
+        q = Query(KIND[kind], 0, value(self.dt, min1), value(self.dt, max1), value(self.dt, min2))
+        out, cnt = C.c_void_p(), C.c_uint64()
+        _check(lib().pst_search(self._h, C.byref(q), RET[r], C.byref(out), C.byref(cnt), _stream(stream)))
+        return out.value or 0, cnt.value
 
     def search(self, kind: str, min1=0, max1=0, min2=0, ret="ids", stream=None) -> np.ndarray:
         """One query through the drop-in call (callee-allocated result)."""
