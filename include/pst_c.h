@@ -101,6 +101,22 @@ pst_status pst_create(pst_tree **out, pst_dtype dtype, pst_idtype idtype, const 
 /* Frees the tree.  Replaces ~StaticPSTGPU (pst/static-pst-gpu.h:80-88). */
 pst_status pst_destroy(pst_tree *tree);
 
+/* Tree images (no reference counterpart: the reference rebuilds every tree from
+ * its points).  An image is a 64-byte header followed by the tree's device
+ * arrays; loading one recreates the tree on the current device without a build.
+ * pst_image_size gives the bytes pst_save writes; pst_save copies the image to
+ * host memory of `capacity` bytes (PST_ERR_CAPACITY if too small; *written = the
+ * image size either way); pst_load creates a tree from an image in host memory
+ * (PST_ERR_INVALID for a bad or truncated image, PST_ERR_UNSUPPORTED for another
+ * image version).  The _file forms stream the image through pinned staging
+ * buffers, the disk transfer overlapping the host-device copy. */
+pst_status pst_image_size(const pst_tree *tree, uint64_t *bytes);
+pst_status pst_save(const pst_tree *tree, void *host, uint64_t capacity, uint64_t *written,
+                    pst_stream_t stream);
+pst_status pst_load(pst_tree **out, const void *host, uint64_t size, pst_stream_t stream);
+pst_status pst_save_file(const pst_tree *tree, const char *path);
+pst_status pst_load_file(pst_tree **out, const char *path, pst_stream_t stream);
+
 /* Tree facts: number of points, levels, slots of the reference's layout
  * (2^levels - 1), device bytes held.  Any output pointer may be NULL.
  * Replaces the getters of pst/static-pst-gpu.h:96-98 and the slot count of
@@ -287,6 +303,24 @@ pst_status pst_num_metacells(const uint32_t pt_dims[3], const uint32_t mc_dims[3
 pst_status pst_form_metacells(pst_dtype dtype, pst_idtype idtype, const void *vert_d,
                               const uint32_t pt_dims[3], const uint32_t mc_dims[3], void *out_d,
                               pst_stream_t stream);
+
+/* Reads a raw volume file (num_vertices values of dtype, x fastest, no header)
+ * into device memory vert_d.  Replaces readInVertices
+ * (helpers/isosurface-data-processing.h:205-229), which reads into host memory and
+ * exits on a missing or short file; here those are PST_ERR_INVALID.  The file
+ * streams through pinned double buffers: the disk read of one chunk overlaps the
+ * host-to-device copy of the previous one. */
+pst_status pst_read_volume(const char *path, pst_dtype dtype, uint64_t num_vertices, void *vert_d,
+                           pst_stream_t stream);
+
+/* readInVertices followed by formMetacellTags without holding the volume on the
+ * device: the volume streams in z-slabs of metacell layers (about slab_bytes each;
+ * 0 = 64 MiB), each slab reduced to its metacells while the next is read.  Output as
+ * pst_form_metacells; the records are bit-identical to pst_form_metacells over the
+ * whole volume. */
+pst_status pst_form_metacells_from_file(const char *path, pst_dtype dtype, pst_idtype idtype,
+                                        const uint32_t pt_dims[3], const uint32_t mc_dims[3], void *out_d,
+                                        uint64_t slab_bytes, pst_stream_t stream);
 
 #ifdef __cplusplus
 }

@@ -19,6 +19,7 @@ from .pst import (  # noqa: F401
     StaticPSTGPUArr,
     calcNumMetacells,
     formMetacellTags,
+    formMetacellTagsFromFile,
     free_device,
     intervalParallelSearch,
     lib,
@@ -26,4 +27,5 @@ from .pst import (  # noqa: F401
     make_queries,
     point_dtype,
     points_to_device,
+    readInVertices,
 )

@@ -959,6 +959,19 @@ void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 
 uint64_t tree_bytes(pst_dtype dt, pst_idtype it, uint64_t n) { return tree_layout(dt, it, n).total; }
 
+void attach_tree_memory(TreeStorage &t, void *mem)
+{
+	const TreeLayout L = tree_layout(t.dtype, t.idtype, t.n);
+	t.mem = mem;
+	t.bytes = L.total;
+	char *b = static_cast<char *>(mem);
+	t.dim1 = b + L.off_dim1;
+	t.dim2 = b + L.off_dim2;
+	t.med = b + L.off_med;
+	t.id = t.idtype == PST_ID_U32 ? reinterpret_cast<uint32_t *>(b + L.off_id) : nullptr;
+	t.occ = reinterpret_cast<uint32_t *>(b + L.off_occ);
+}
+
 uint64_t build_bytes_needed(pst_dtype dt, pst_idtype it, uint64_t n)
 {
 	return tree_bytes(dt, it, n) + build_scratch_bytes(dt, it, n);
@@ -981,13 +994,7 @@ void build_tree(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 		fail(PST_ERR_NOMEM, "tree allocation of " + std::to_string(L.total) + " B failed");
 	}
 	check_cuda(e, "cudaMalloc(tree)");
-	t.bytes = L.total;
-	char *b = static_cast<char *>(t.mem);
-	t.dim1 = b + L.off_dim1;
-	t.dim2 = b + L.off_dim2;
-	t.med = b + L.off_med;
-	t.id = t.idtype == PST_ID_U32 ? reinterpret_cast<uint32_t *>(b + L.off_id) : nullptr;
-	t.occ = reinterpret_cast<uint32_t *>(b + L.off_occ);
+	attach_tree_memory(t, t.mem);
 	PST_CUDA(cudaMemsetAsync(t.occ, 0, L.total - L.off_occ, s));
 	try {
 		switch (t.dtype) {

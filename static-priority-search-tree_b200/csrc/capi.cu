@@ -218,6 +218,63 @@ pst_status pst_create(pst_tree **out, pst_dtype dtype, pst_idtype idtype, const 
 	});
 }
 
+pst_status pst_image_size(const pst_tree *tree, uint64_t *bytes)
+{
+	return guarded([&] {
+		if (!tree || !bytes)
+			fail(PST_ERR_INVALID, "null argument");
+		*bytes = serialized_size(tree->t);
+	});
+}
+
+pst_status pst_save(const pst_tree *tree, void *host, uint64_t capacity, uint64_t *written, pst_stream_t stream)
+{
+	return guarded([&] {
+		if (!tree)
+			fail(PST_ERR_INVALID, "null tree");
+		if (written)
+			*written = serialized_size(tree->t);
+		save_tree(tree->t, host, capacity, reinterpret_cast<cudaStream_t>(stream));
+	});
+}
+
+pst_status pst_load(pst_tree **out, const void *host, uint64_t size, pst_stream_t stream)
+{
+	return guarded([&] {
+		if (!out)
+			fail(PST_ERR_INVALID, "null output handle");
+		*out = nullptr;
+		require_device();
+		auto tr = std::make_unique<pst_tree>();
+		check_cuda(cudaGetDevice(&tr->t.device), "cudaGetDevice");
+		load_tree(tr->t, host, size, reinterpret_cast<cudaStream_t>(stream));
+		*out = tr.release();
+	});
+}
+
+pst_status pst_save_file(const pst_tree *tree, const char *path)
+{
+	return guarded([&] {
+		if (!tree)
+			fail(PST_ERR_INVALID, "null tree");
+		save_tree_file(tree->t, path);
+	});
+}
+
+pst_status pst_load_file(pst_tree **out, const char *path, pst_stream_t stream)
+{
+	return guarded([&] {
+		if (!out)
+			fail(PST_ERR_INVALID, "null output handle");
+		*out = nullptr;
+		require_device();
+		auto tr = std::make_unique<pst_tree>();
+		check_cuda(cudaGetDevice(&tr->t.device), "cudaGetDevice");
+		load_tree_file(tr->t, path, reinterpret_cast<cudaStream_t>(stream));
+		*out = tr.release();
+	});
+}
+
 pst_status pst_destroy(pst_tree *tree)
 {
 	return guarded([&] {
@@ -578,6 +635,34 @@ pst_status pst_form_metacells(pst_dtype dtype, pst_idtype idtype, const void *ve
 			fail(PST_ERR_INVALID, "null buffer");
 		require_device();
 		metacells_run(dtype, idtype, vert_d, pt_dims, mc_dims, M, out_d, reinterpret_cast<cudaStream_t>(stream));
+	});
+}
+
+pst_status pst_read_volume(const char *path, pst_dtype dtype, uint64_t num_vertices, void *vert_d,
+                           pst_stream_t stream)
+{
+	return guarded([&] {
+		check_types(dtype, PST_ID_NONE);
+		require_device();
+		read_volume(path, dtype, num_vertices, vert_d, reinterpret_cast<cudaStream_t>(stream));
+	});
+}
+
+pst_status pst_form_metacells_from_file(const char *path, pst_dtype dtype, pst_idtype idtype,
+                                        const uint32_t pt_dims[3], const uint32_t mc_dims[3], void *out_d,
+                                        uint64_t slab_bytes, pst_stream_t stream)
+{
+	return guarded([&] {
+		check_types(dtype, idtype);
+		uint32_t M[3];
+		uint64_t nm = 0;
+		if (pst_num_metacells(pt_dims, mc_dims, M, &nm) != PST_OK)
+			fail(PST_ERR_INVALID, g_last_error);
+		if (nm >= (1ull << 32) && idtype == PST_ID_U32)
+			fail(PST_ERR_INVALID, "metacell ids must fit in 32 bits");
+		require_device();
+		metacells_from_file(path, dtype, idtype, pt_dims, mc_dims, M, out_d, slab_bytes,
+		                    reinterpret_cast<cudaStream_t>(stream));
 	});
 }
 

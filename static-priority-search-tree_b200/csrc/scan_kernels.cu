@@ -100,15 +100,17 @@ __device__ __forceinline__ void plane_minmax(const T *__restrict__ vol, uint64_t
 	}
 }
 
+// Metacell layers [mz_begin, mz_end); `vol` holds the vertex planes from z_base on
+// (the whole volume: z_base = 0; one z-slab of it: its first plane).
 template <typename T, bool HAS_ID>
 __global__ void k_metacells(const T *__restrict__ vol, uint32_t px, uint32_t py, uint32_t pz, uint32_t mcx,
-                            uint32_t mcy, uint32_t mcz, uint32_t Mx, uint32_t My, uint32_t Mz, uint32_t mz_per_cta,
-                            Point<T, HAS_ID> *__restrict__ out)
+                            uint32_t mcy, uint32_t mcz, uint32_t Mx, uint32_t My, uint32_t mz_begin, uint32_t mz_end,
+                            uint32_t z_base, uint32_t mz_per_cta, Point<T, HAS_ID> *__restrict__ out)
 {
 	const uint32_t mx = blockIdx.x * blockDim.x + threadIdx.x;
 	const uint32_t my = blockIdx.y;
-	const uint32_t mz0 = blockIdx.z * mz_per_cta;
-	const uint32_t mz1 = min(mz0 + mz_per_cta, Mz);
+	const uint32_t mz0 = mz_begin + blockIdx.z * mz_per_cta;
+	const uint32_t mz1 = min(mz0 + mz_per_cta, mz_end);
 	if (mx >= Mx)
 		return;
 	const uint32_t x0 = mx * mcx, x1 = min(x0 + mcx, px - 1);
@@ -122,10 +124,10 @@ __global__ void k_metacells(const T *__restrict__ vol, uint32_t px, uint32_t py,
 			lo = plo;
 			hi = phi;
 		} else {
-			plane_minmax(vol, px, py, z0, x0, x1, y0, y1, lo, hi);
+			plane_minmax(vol, px, py, z0 - z_base, x0, x1, y0, y1, lo, hi);
 		}
 		for (uint32_t z = z0 + 1; z <= z1; z++) {
-			plane_minmax(vol, px, py, z, x0, x1, y0, y1, plo, phi);
+			plane_minmax(vol, px, py, z - z_base, x0, x1, y0, y1, plo, phi);
 			lo = plo < lo ? plo : lo;
 			hi = phi > hi ? phi : hi;
 			pz_done = z;
@@ -168,16 +170,19 @@ void ips_dispatch(pst_idtype it, pst_ret ret, const void *pts, uint64_t n, T v, 
 }
 
 template <typename T, bool HAS_ID>
-void metacell_launch(const void *vol, const uint32_t P[3], const uint32_t mc[3], const uint32_t M[3], void *out,
-                     cudaStream_t s)
+void metacell_launch(const void *vol, const uint32_t P[3], const uint32_t mc[3], const uint32_t M[3],
+                     uint32_t mz_begin, uint32_t mz_end, void *out, cudaStream_t s)
 {
+	if (mz_end <= mz_begin)
+		return;
 	const uint32_t threads = M[0] >= 256 ? 256 : ((M[0] + 31) / 32) * 32;
 	const uint32_t mzp = 8;
-	dim3 grid((M[0] + threads - 1) / threads, M[1], (M[2] + mzp - 1) / mzp);
+	dim3 grid((M[0] + threads - 1) / threads, M[1], (mz_end - mz_begin + mzp - 1) / mzp);
 	if (grid.y > 65535 || grid.z > 65535)
 		fail(PST_ERR_INVALID, "metacell grid too large");
 	k_metacells<T, HAS_ID><<<grid, threads, 0, s>>>(static_cast<const T *>(vol), P[0], P[1], P[2], mc[0], mc[1], mc[2],
-	                                                M[0], M[1], M[2], mzp, static_cast<Point<T, HAS_ID> *>(out));
+	                                                M[0], M[1], mz_begin, mz_end, mz_begin * mc[2], mzp,
+	                                                static_cast<Point<T, HAS_ID> *>(out));
 	PST_CUDA(cudaGetLastError());
 }
 
@@ -194,16 +199,23 @@ void ips_run(pst_dtype dt, pst_idtype it, pst_ret ret, const void *pts, uint64_t
 	}
 }
 
+void metacells_run_layers(pst_dtype dt, pst_idtype it, const void *vol, const uint32_t P[3], const uint32_t mc[3],
+                          const uint32_t M[3], uint32_t mz_begin, uint32_t mz_end, void *out, cudaStream_t s)
+{
+	const bool id = it == PST_ID_U32;
+	const uint32_t b = mz_begin, e = mz_end;
+	switch (dt) {
+	case PST_F32: id ? metacell_launch<float, true>(vol, P, mc, M, b, e, out, s) : metacell_launch<float, false>(vol, P, mc, M, b, e, out, s); break;
+	case PST_F64: id ? metacell_launch<double, true>(vol, P, mc, M, b, e, out, s) : metacell_launch<double, false>(vol, P, mc, M, b, e, out, s); break;
+	case PST_I32: id ? metacell_launch<int32_t, true>(vol, P, mc, M, b, e, out, s) : metacell_launch<int32_t, false>(vol, P, mc, M, b, e, out, s); break;
+	default: fail(PST_ERR_INVALID, "bad dtype");
+	}
+}
+
 void metacells_run(pst_dtype dt, pst_idtype it, const void *vol, const uint32_t P[3], const uint32_t mc[3],
                    const uint32_t M[3], void *out, cudaStream_t s)
 {
-	const bool id = it == PST_ID_U32;
-	switch (dt) {
-	case PST_F32: id ? metacell_launch<float, true>(vol, P, mc, M, out, s) : metacell_launch<float, false>(vol, P, mc, M, out, s); break;
-	case PST_F64: id ? metacell_launch<double, true>(vol, P, mc, M, out, s) : metacell_launch<double, false>(vol, P, mc, M, out, s); break;
-	case PST_I32: id ? metacell_launch<int32_t, true>(vol, P, mc, M, out, s) : metacell_launch<int32_t, false>(vol, P, mc, M, out, s); break;
-	default: fail(PST_ERR_INVALID, "bad dtype");
-	}
+	metacells_run_layers(dt, it, vol, P, mc, M, 0, M[2], out, s);
 }
 
 }  // namespace pst

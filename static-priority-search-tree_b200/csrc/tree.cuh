@@ -40,6 +40,15 @@ size_t point_size(pst_dtype dt, pst_idtype it);
 uint64_t tree_bytes(pst_dtype dt, pst_idtype it, uint64_t n);
 // Tree arrays plus the peak construction working set.
 uint64_t build_bytes_needed(pst_dtype dt, pst_idtype it, uint64_t n);
+// Points the field pointers of t (dtype, idtype, n set) into one allocation of
+// tree_bytes(...) bytes laid out as the builder lays it out.
+void attach_tree_memory(TreeStorage &t, void *mem);
+// Tree image: a 64-byte header followed by the device allocation byte for byte.
+uint64_t serialized_size(const TreeStorage &t);
+void save_tree(const TreeStorage &t, void *host, uint64_t capacity, cudaStream_t s);
+void load_tree(TreeStorage &t, const void *host, uint64_t size, cudaStream_t s);
+void save_tree_file(const TreeStorage &t, const char *path);
+void load_tree_file(TreeStorage &t, const char *path, cudaStream_t s);
 
 void build_tree(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s);
 void free_tree(TreeStorage &t);

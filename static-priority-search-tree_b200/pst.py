@@ -78,6 +78,11 @@ def lib():
         "pst_mem_needed": (i32, [i32, i32, u64, P(u64)]),
         "pst_create": (i32, [P(vp), i32, i32, vp, u64, vp]),
         "pst_destroy": (i32, [vp]),
+        "pst_image_size": (i32, [vp, P(u64)]),
+        "pst_save": (i32, [vp, vp, u64, P(u64), vp]),
+        "pst_load": (i32, [P(vp), vp, u64, vp]),
+        "pst_save_file": (i32, [vp, C.c_char_p]),
+        "pst_load_file": (i32, [P(vp), C.c_char_p, vp]),
         "pst_info": (i32, [vp, P(u64), P(u32), P(u64), P(u64), P(i32), P(i32)]),
         "pst_export": (i32, [vp, vp, vp, vp, vp, vp]),
         "pst_search": (i32, [vp, P(Query), i32, P(vp), P(u64), vp]),
@@ -105,6 +110,8 @@ def lib():
         "pst_server_reset_stats": (i32, [vp]),
         "pst_server_destroy": (i32, [vp]),
         "pst_form_metacells": (i32, [i32, i32, vp, P(u32), P(u32), vp, vp]),
+        "pst_read_volume": (i32, [C.c_char_p, i32, u64, vp, vp]),
+        "pst_form_metacells_from_file": (i32, [C.c_char_p, i32, i32, P(u32), P(u32), vp, u64, vp]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(L, name)
@@ -212,6 +219,45 @@ class StaticPSTGPU:
         ptr = C.c_void_p(pts_d.data_ptr() if hasattr(pts_d, "data_ptr") else (pts_d or 0))
         _check(lib().pst_create(C.byref(self._h), DTYPE[dt], IDTYPE[has_id], ptr, self.n, _stream(stream)))
         self.rec_point = point_dtype(dt, has_id)
+
+    @classmethod
+    def _adopt(cls, handle: C.c_void_p):
+        """Wraps a tree handle created by the library (a loaded image)."""
+        self = cls.__new__(cls)
+        self._h = handle
+        n, lv, sl, by = C.c_uint64(), C.c_uint32(), C.c_uint64(), C.c_uint64()
+        d, i = C.c_int32(), C.c_int32()
+        _check(lib().pst_info(handle, C.byref(n), C.byref(lv), C.byref(sl), C.byref(by), C.byref(d), C.byref(i)))
+        self.dt = {v: k for k, v in DTYPE.items()}[d.value]
+        self.has_id = i.value == IDTYPE[True]
+        self.n = n.value
+        self.rec_point = point_dtype(self.dt, self.has_id)
+        return self
+
+    def to_bytes(self) -> bytes:
+        """The tree's image (pst_save): a 64-byte header and the device arrays."""
+        size = C.c_uint64()
+        _check(lib().pst_image_size(self._h, C.byref(size)))
+        buf = np.empty(size.value, np.uint8)
+        _check(lib().pst_save(self._h, buf.ctypes.data_as(C.c_void_p), size.value, C.byref(size), _stream()))
+        return buf.tobytes()
+
+    @classmethod
+    def from_bytes(cls, image: bytes):
+        """Recreates a tree from its image without rebuilding it (pst_load)."""
+        h = C.c_void_p()
+        buf = np.frombuffer(image, np.uint8)
+        _check(lib().pst_load(C.byref(h), buf.ctypes.data_as(C.c_void_p), len(buf), _stream()))
+        return cls._adopt(h)
+
+    def save(self, path):
+        _check(lib().pst_save_file(self._h, str(path).encode()))
+
+    @classmethod
+    def load(cls, path):
+        h = C.c_void_p()
+        _check(lib().pst_load_file(C.byref(h), str(path).encode(), _stream()))
+        return cls._adopt(h)
 
     @classmethod
     def from_numpy(cls, pts: np.ndarray, dt: str):
@@ -501,6 +547,33 @@ def formMetacellTags(vert_d, pt_grid_dims, metacell_dims, dt: str = "f32", has_i
     M = (C.c_uint32 * 3)(*metacell_dims)
     _check(lib().pst_form_metacells(DTYPE[dt], IDTYPE[has_id], C.c_void_p(vert_d.data_ptr()), P, M,
                                     C.c_void_p(out.data_ptr()), _stream(stream)))
+    return out[: n * rec.itemsize], n
+
+
+def readInVertices(path, num_vertices: int, dt: str = "f32", stream=None):
+    """Mirror of readInVertices (helpers/isosurface-data-processing.h:205-229), reading
+    the raw volume straight into a device tensor (pst_read_volume)."""
+    torch = _torch()
+    tt = {"f32": torch.float32, "f64": torch.float64, "i32": torch.int32}[dt]
+    out = torch.empty(max(int(num_vertices), 1), dtype=tt, device="cuda")
+    _check(lib().pst_read_volume(str(path).encode(), DTYPE[dt], int(num_vertices), C.c_void_p(out.data_ptr()),
+                                 _stream(stream)))
+    return out[: int(num_vertices)]
+
+
+def formMetacellTagsFromFile(path, pt_grid_dims, metacell_dims, dt: str = "f32", has_id: bool = True,
+                             slab_bytes: int = 0, stream=None):
+    """readInVertices + formMetacellTags in one stream (pst_form_metacells_from_file):
+    the volume never sits on the device whole; returns (records, n) like
+    formMetacellTags."""
+    torch = _torch()
+    _, n = calcNumMetacells(pt_grid_dims, metacell_dims)
+    rec = point_dtype(dt, has_id)
+    out = torch.empty(max(n * rec.itemsize, 16), dtype=torch.uint8, device="cuda")
+    P = (C.c_uint32 * 3)(*pt_grid_dims)
+    M = (C.c_uint32 * 3)(*metacell_dims)
+    _check(lib().pst_form_metacells_from_file(str(path).encode(), DTYPE[dt], IDTYPE[has_id], P, M,
+                                              C.c_void_p(out.data_ptr()), int(slab_bytes), _stream(stream)))
     return out[: n * rec.itemsize], n
 
 
