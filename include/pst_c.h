@@ -304,6 +304,29 @@ pst_status pst_form_metacells(pst_dtype dtype, pst_idtype idtype, const void *ve
                               const uint32_t pt_dims[3], const uint32_t mc_dims[3], void *out_d,
                               pst_stream_t stream);
 
+/* ------------------------------------------------------------------------- */
+/* Marching cubes over active metacells (float32 volumes), headless.            */
+
+/* Triangles of the cells (voxel cubes) of the metacells ids_d[0..n_ids) (ids as
+ * pst_form_metacells numbers them, e.g. the result of pst_two_sided_left(iso, iso)
+ * on the metacell tree): a corner is inside when its value is >= iso; each
+ * triangle is 9 floats (three vertices x, y, z in vertex-index units), wound so
+ * that its normal points from inside to outside; output ordered by the given ids,
+ * then cell (x fastest), then table order.  The triangle table is this library's
+ * own (pst_mc_tables returns it: ntri[256], edges[256][15] with edge 4a + u + 2v
+ * along axis a), giving a closed, consistently oriented surface.  No reference
+ * counterpart runs headless: the reference's isosurface sample
+ * (.marching-cubes/marchingCubes_kernel.cu:155-413) renders through OpenGL.
+ * pst_mc_count returns the number of triangles; pst_mc_triangles writes them
+ * into tri_d (capacity triangles; PST_ERR_CAPACITY with the full count otherwise). */
+pst_status pst_mc_tables(uint8_t ntri[256], uint8_t edges[256 * 15]);
+pst_status pst_mc_count(const float *vol_d, const uint32_t pt_dims[3], const uint32_t mc_dims[3],
+                        const uint32_t *ids_d, uint64_t n_ids, float iso, uint64_t *n_triangles,
+                        pst_stream_t stream);
+pst_status pst_mc_triangles(const float *vol_d, const uint32_t pt_dims[3], const uint32_t mc_dims[3],
+                            const uint32_t *ids_d, uint64_t n_ids, float iso, float *tri_d,
+                            uint64_t capacity, uint64_t *n_triangles, pst_stream_t stream);
+
 /* Reads a raw volume file (num_vertices values of dtype, x fastest, no header)
  * into device memory vert_d.  Replaces readInVertices
  * (helpers/isosurface-data-processing.h:205-229), which reads into host memory and

@@ -25,6 +25,8 @@ from .pst import (  # noqa: F401
     lib,
     library_path,
     make_queries,
+    marchingCubes,
+    marchingCubesTables,
     point_dtype,
     points_to_device,
     readInVertices,

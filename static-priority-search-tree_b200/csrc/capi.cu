@@ -666,4 +666,60 @@ pst_status pst_form_metacells_from_file(const char *path, pst_dtype dtype, pst_i
 	});
 }
 
+pst_status pst_mc_tables(uint8_t ntri[256], uint8_t edges[256 * 15])
+{
+	return guarded([&] {
+		if (!ntri || !edges)
+			fail(PST_ERR_INVALID, "null table buffer");
+		mc_tables(ntri, edges);
+	});
+}
+
+static void mc_check(const float *vol_d, const uint32_t pt_dims[3], const uint32_t mc_dims[3], const uint32_t *ids_d,
+                     uint64_t n_ids)
+{
+	if (!pt_dims || !mc_dims)
+		fail(PST_ERR_INVALID, "null dims");
+	for (int i = 0; i < 3; i++) {
+		if (pt_dims[i] < 2)
+			fail(PST_ERR_INVALID, "a volume needs at least 2 vertices per axis");
+		if (mc_dims[i] == 0)
+			fail(PST_ERR_INVALID, "metacell dims must be positive");
+	}
+	if (n_ids && (!vol_d || !ids_d))
+		fail(PST_ERR_INVALID, "null buffer");
+	require_device();
+}
+
+pst_status pst_mc_count(const float *vol_d, const uint32_t pt_dims[3], const uint32_t mc_dims[3], const uint32_t *ids_d,
+                        uint64_t n_ids, float iso, uint64_t *n_triangles, pst_stream_t stream)
+{
+	return guarded([&] {
+		if (!n_triangles)
+			fail(PST_ERR_INVALID, "null output");
+		*n_triangles = 0;
+		mc_check(vol_d, pt_dims, mc_dims, ids_d, n_ids);
+		*n_triangles = mc_run(vol_d, pt_dims, mc_dims, ids_d, n_ids, iso, nullptr, 0, false,
+		                      reinterpret_cast<cudaStream_t>(stream));
+	});
+}
+
+pst_status pst_mc_triangles(const float *vol_d, const uint32_t pt_dims[3], const uint32_t mc_dims[3],
+                            const uint32_t *ids_d, uint64_t n_ids, float iso, float *tri_d, uint64_t capacity,
+                            uint64_t *n_triangles, pst_stream_t stream)
+{
+	return guarded([&] {
+		if (!n_triangles)
+			fail(PST_ERR_INVALID, "null output");
+		*n_triangles = 0;
+		mc_check(vol_d, pt_dims, mc_dims, ids_d, n_ids);
+		const uint64_t total = mc_run(vol_d, pt_dims, mc_dims, ids_d, n_ids, iso, tri_d, capacity, true,
+		                              reinterpret_cast<cudaStream_t>(stream));
+		*n_triangles = total;
+		if (total > capacity)
+			fail(PST_ERR_CAPACITY, "triangle buffer holds " + std::to_string(capacity) + " of " +
+			                           std::to_string(total) + " triangles");
+	});
+}
+
 }  // extern "C"

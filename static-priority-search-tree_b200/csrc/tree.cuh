@@ -49,6 +49,11 @@ void save_tree(const TreeStorage &t, void *host, uint64_t capacity, cudaStream_t
 void load_tree(TreeStorage &t, const void *host, uint64_t size, cudaStream_t s);
 void save_tree_file(const TreeStorage &t, const char *path);
 void load_tree_file(TreeStorage &t, const char *path, cudaStream_t s);
+// Marching cubes over the cells of the given metacells (mc.cu).  Returns the
+// triangle count; writes the triangles only when emit and they fit `capacity`.
+void mc_tables(uint8_t *ntri, uint8_t *edges);
+uint64_t mc_run(const float *vol, const uint32_t P[3], const uint32_t mc[3], const uint32_t *ids, uint64_t n, float iso,
+                float *tri, uint64_t capacity, bool emit, cudaStream_t s);
 
 void build_tree(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s);
 void free_tree(TreeStorage &t);

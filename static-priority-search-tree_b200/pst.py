@@ -111,6 +111,9 @@ def lib():
         "pst_server_destroy": (i32, [vp]),
         "pst_form_metacells": (i32, [i32, i32, vp, P(u32), P(u32), vp, vp]),
         "pst_read_volume": (i32, [C.c_char_p, i32, u64, vp, vp]),
+        "pst_mc_tables": (i32, [vp, vp]),
+        "pst_mc_count": (i32, [vp, P(u32), P(u32), vp, u64, C.c_float, P(u64), vp]),
+        "pst_mc_triangles": (i32, [vp, P(u32), P(u32), vp, u64, C.c_float, vp, u64, P(u64), vp]),
         "pst_form_metacells_from_file": (i32, [C.c_char_p, i32, i32, P(u32), P(u32), vp, u64, vp]),
     }
     for name, (res, args) in sigs.items():
@@ -575,6 +578,32 @@ def formMetacellTagsFromFile(path, pt_grid_dims, metacell_dims, dt: str = "f32",
     _check(lib().pst_form_metacells_from_file(str(path).encode(), DTYPE[dt], IDTYPE[has_id], P, M,
                                               C.c_void_p(out.data_ptr()), int(slab_bytes), _stream(stream)))
     return out[: n * rec.itemsize], n
+
+
+def marchingCubesTables():
+    """The library's triangle table: (ntri[256], edges[256, 15]) uint8."""
+    ntri = np.zeros(256, np.uint8)
+    edges = np.zeros((256, 15), np.uint8)
+    _check(lib().pst_mc_tables(ntri.ctypes.data_as(C.c_void_p), edges.ctypes.data_as(C.c_void_p)))
+    return ntri, edges
+
+
+def marchingCubes(vol_d, pt_grid_dims, metacell_dims, ids_d, iso: float, stream=None):
+    """Triangles (n, 9) float32 on the device of the cells of the metacells ids_d
+    (a device uint32 tensor, e.g. a twoSidedLeftSearch(iso, iso) result)."""
+    torch = _torch()
+    P = (C.c_uint32 * 3)(*pt_grid_dims)
+    M = (C.c_uint32 * 3)(*metacell_dims)
+    n_ids = int(ids_d.numel()) if ids_d is not None else 0
+    vp = C.c_void_p(vol_d.data_ptr())
+    ip = C.c_void_p(ids_d.data_ptr() if n_ids else 0)
+    cnt = C.c_uint64()
+    _check(lib().pst_mc_count(vp, P, M, ip, n_ids, float(iso), C.byref(cnt), _stream(stream)))
+    out = torch.empty((max(cnt.value, 1), 9), dtype=torch.float32, device="cuda")
+    got = C.c_uint64()
+    _check(lib().pst_mc_triangles(vp, P, M, ip, n_ids, float(iso), C.c_void_p(out.data_ptr()), cnt.value,
+                                  C.byref(got), _stream(stream)))
+    return out[: got.value]
 
 
 def _env_flag(name: str) -> bool:
