@@ -26,6 +26,8 @@ import threading
 import time
 from pathlib import Path
 
+import ctypes as C
+
 import numpy as np
 
 ROOT = Path(__file__).resolve().parent
@@ -270,6 +272,74 @@ def sweep(pst, torch, n, seed=1):
     return out
 
 
+# ---------------------------------------------------------------------------
+# isosurface pipeline (run with --isosurface)
+
+def isosurface_bench(pst, torch, dims=(512, 512, 512), seed=1):
+    """512^3 float32 blob volume -> 4^3 metacells (128^3 points) -> tree; at 16
+    isovalues 0.05 + 0.06 i: the active metacells by twoSidedLeftSearch(iso, iso)
+    (batched and plain) and by the interval parallel search, then marching cubes
+    over the active metacells.  Device times by CUDA events."""
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        ev[0].record()
+        for _ in range(reps):
+            r = fn()
+        ev[1].record()
+        ev[1].synchronize()
+        return r, ev[0].elapsed_time(ev[1]) / reps
+
+    vol = blob_volume_device(*dims, seed, torch).reshape(-1).contiguous()
+    recs, n = timed(lambda: pst.formMetacellTags(vol, dims, (4, 4, 4), "f32", True))[0], None
+    (recs, n), mc_ms = timed(lambda: pst.formMetacellTags(vol, dims, (4, 4, 4), "f32", True))
+    tree, build_ms = timed(lambda: pst.StaticPSTGPU(recs, n, "f32", True), reps=1)
+    isos = [0.05 + 0.06 * i for i in range(16)]
+    eng = pst.BatchEngine(tree, max_queries=16)
+    q = pst.make_queries(np.full(16, 1, np.int32), np.zeros(16), np.array(isos), np.array(isos), "f32")
+    offs, res = eng.search(q)
+    qd = torch.from_numpy(q.view(np.uint8).copy()).to("cuda")
+    out_d = torch.empty(max(len(res) * 4, 16), dtype=torch.uint8, device="cuda")
+    offs_d = torch.empty(17, dtype=torch.int64, device="cuda")
+    _, batch_ms = timed(lambda: eng.run(qd, out_d, offs_d, queries_on_device=True, sync=False))
+    ips_buf = torch.empty(n * 4, dtype=torch.uint8, device="cuda")
+    lib = pst.lib()
+
+    def ips(iso32):
+        cnt = C.c_uint64()
+        pst.pst._check(lib.pst_ips_search_into(0, 1, C.c_void_p(recs.data_ptr()), n, pst.pst.value_arg("f32", iso32),
+                                               0, C.c_void_p(ips_buf.data_ptr()), n, C.byref(cnt), None))
+        return cnt.value
+    rows = []
+    tri_total, mc_total_ms = 0, 0.0
+    for i, iso in enumerate(isos):
+        iso32 = float(np.float32(iso))
+        t0 = time.perf_counter()
+        ptr, k = tree.search_device("left", 0.0, iso32, iso32)
+        torch.cuda.synchronize()
+        plain_ms = 1000 * (time.perf_counter() - t0)
+        pst.free_device(ptr)
+        ids = torch.from_numpy(np.ascontiguousarray(res[int(offs[i]):int(offs[i + 1])]).view(np.int32)).to("cuda")
+        k_ips, ips_ms = timed(lambda: ips(iso32))
+        assert k_ips == k
+        tri, mc_ms_i = timed(lambda: pst.marchingCubes(vol, dims, (4, 4, 4), ids, iso32))
+        tri_total += len(tri)
+        mc_total_ms += mc_ms_i
+        rows.append({"iso": iso32, "active_metacells": int(k), "plain_query_ms": plain_ms, "ips_ms": ips_ms,
+                     "triangles": int(len(tri)), "marching_cubes_ms": mc_ms_i})
+        del tri, ids
+    out = {"volume": list(dims), "metacells": n, "form_metacells_ms": mc_ms, "build_ms": build_ms,
+           "batched_16_isovalues_ms": batch_ms, "marching_cubes_triangles_per_s": tri_total / (mc_total_ms / 1000),
+           "per_isovalue": rows}
+    eng.close()
+    tree.close()
+    del vol, recs
+    torch.cuda.empty_cache()
+    return out
+
+
 SERVING_VOLUMES = [(64, 64, 64), (128, 128, 128), (192, 192, 192), (256, 256, 256), (384, 384, 384),
                    (512, 512, 512), (768, 768, 512), (1024, 1024, 512)]
 
@@ -482,6 +552,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--plain-queries", type=int, default=256)
     ap.add_argument("--sweep", action="store_true", help="also run every value type x kind x selectivity")
+    ap.add_argument("--isosurface", action="store_true", help="also run the 512^3 isosurface pipeline")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -635,6 +706,14 @@ def main():
         tree = pst.StaticPSTGPU(gen_points_device(n, seed=1 + rank, torch=torch), n, "f32", True)
         eng = pst.BatchEngine(tree, max_queries=NQ)
 
+    iso_res = None
+    if rank == 0 and args.isosurface:
+        iso_res = isosurface_bench(pst, torch)
+        log("isosurface: metacells {:.2f} ms, build {:.2f} ms, 16 isovalues batched {:.3f} ms, "
+            "marching cubes {:.3g} triangles/s".format(iso_res["form_metacells_ms"], iso_res["build_ms"],
+                                                     iso_res["batched_16_isovalues_ms"],
+                                                     iso_res["marching_cubes_triangles_per_s"]))
+
     serving = None
     if rank == 0 and not args.no_serving:
         try:
@@ -674,6 +753,8 @@ def main():
                 "serving": serving}
         if sweep_rows is not None:
             line["sweep"] = sweep_rows
+        if iso_res is not None:
+            line["isosurface"] = iso_res
         levels = tree.info()["levels"]
         line["gpu_launches"] = (levels + 6) * args.steps  # unpack+check + levels + 3 scan + emit per step
         print(json.dumps(line))
