@@ -187,7 +187,8 @@ class Orc:
 
 
 class Ref:
-    """The reference's StaticPSTCPUIter compiled from its own sources."""
+    """The reference's StaticPSTCPUIter (or, with recursive=True, its
+    StaticPSTCPURecur: searches only) compiled from its own sources."""
 
     _lib = None
 
@@ -201,6 +202,8 @@ class Ref:
             lib = C.CDLL(str(REF_SO))
             lib.ref_build.restype = C.c_void_p
             lib.ref_build.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_uint64]
+            lib.ref_build_recur.restype = C.c_void_p
+            lib.ref_build_recur.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_uint64]
             lib.ref_destroy.argtypes = [C.c_void_p]
             lib.ref_num_slots.restype = C.c_uint64
             lib.ref_num_slots.argtypes = [C.c_void_p]
@@ -211,12 +214,14 @@ class Ref:
             cls._lib = lib
         return cls._lib
 
-    def __init__(self, pts: np.ndarray, dt: str):
+    def __init__(self, pts: np.ndarray, dt: str, recursive: bool = False):
         self.pts = np.ascontiguousarray(pts)
         self.dt = dt
         self.has_id = "id" in pts.dtype.names
         self.n = len(pts)
-        self.h = self.lib().ref_build(DTYPE_CODE[dt], int(self.has_id), _ptr(self.pts), self.n)
+        self.recursive = recursive
+        build = self.lib().ref_build_recur if recursive else self.lib().ref_build
+        self.h = build(DTYPE_CODE[dt], int(self.has_id), _ptr(self.pts), self.n)
         if not self.h:
             raise RuntimeError("reference build failed")
 

@@ -1,6 +1,8 @@
-// Host-only harness that compiles the reference's own StaticPSTCPUIter, unmodified,
-// from its sources (pst/static-pst-cpu-iter.h and the headers it includes) into
-// oracle/_ref/libpstref.so.  TEST INFRASTRUCTURE ONLY: it pins the oracle, makes
+// Host-only harness that compiles the reference's own StaticPSTCPUIter and
+// StaticPSTCPURecur, unmodified, from their sources (pst/static-pst-cpu-iter.h,
+// pst/static-pst-cpu-recur.h and the headers they include) into
+// oracle/_ref/libpstref.so.  The recursive tree is a second, independent CPU
+// implementation of the same searches in the reference; it cross-checks the first.  TEST INFRASTRUCTURE ONLY: it pins the oracle, makes
 // the golden fixtures, and is the timed CPU baseline ("reference" kind) of the
 // benchmark.  Nothing in the product links it.
 //
@@ -23,6 +25,7 @@
 #define private public
 #include "point-struct.h"
 #include "static-pst-cpu-iter.h"
+#include "static-pst-cpu-recur.h"
 #undef private
 
 namespace {
@@ -34,6 +37,7 @@ struct Handle {
 	int dtype;
 	int has_id;
 	void *tree;
+	int recur;  // StaticPSTCPURecur instead of StaticPSTCPUIter
 };
 
 template <typename T, int HAS_ID>
@@ -42,26 +46,29 @@ template <typename T>
 struct Types<T, 1> {
 	using Pt = PointStruct<T, uint32_t, 1>;
 	using Tree = StaticPSTCPUIter<T, PointStruct, uint32_t, 1>;
+	using Recur = StaticPSTCPURecur<T, PointStruct, uint32_t, 1>;
 };
 template <typename T>
 struct Types<T, 0> {
 	using Pt = PointStruct<T, void, 0>;
 	using Tree = StaticPSTCPUIter<T, PointStruct, void, 0>;
+	using Recur = StaticPSTCPURecur<T, PointStruct, void, 0>;
 };
 
-template <typename T, int HAS_ID>
+template <typename T, int HAS_ID, bool RECUR = false>
 void *build(const void *pts, uint64_t n)
 {
-	using Tr = typename Types<T, HAS_ID>::Tree;
+	using Tr = std::conditional_t<RECUR, typename Types<T, HAS_ID>::Recur, typename Types<T, HAS_ID>::Tree>;
 	using Pt = typename Types<T, HAS_ID>::Pt;
 	// The constructor only reads the array, but its signature takes a non-const pointer
 	return new Tr(const_cast<Pt *>(static_cast<const Pt *>(pts)), n);
 }
 
-template <typename T, int HAS_ID>
+template <typename T, int HAS_ID, bool RECUR = false>
 void destroy(void *t)
 {
-	delete static_cast<typename Types<T, HAS_ID>::Tree *>(t);
+	using Tr = std::conditional_t<RECUR, typename Types<T, HAS_ID>::Recur, typename Types<T, HAS_ID>::Tree>;
+	delete static_cast<Tr *>(t);
 }
 
 template <typename T, int HAS_ID>
@@ -91,10 +98,10 @@ void export_tree(void *tp, T *dim1, T *dim2, T *med, uint32_t *ids, uint8_t *bit
 // Runs one reference search.  ret_points = 0 returns ids (id trees only), 1 returns
 // PointStruct records.  The result array is allocated by the reference (new[]),
 // copied out (up to cap records) and freed here.  Returns the count, or -1.
-template <typename T, int HAS_ID>
+template <typename T, int HAS_ID, bool RECUR = false>
 int64_t search(void *tp, int kind, T min1, T max1, T min2, int ret_points, void *out, uint64_t cap)
 {
-	using Tr = typename Types<T, HAS_ID>::Tree;
+	using Tr = std::conditional_t<RECUR, typename Types<T, HAS_ID>::Recur, typename Types<T, HAS_ID>::Tree>;
 	using Pt = typename Types<T, HAS_ID>::Pt;
 	Tr *t = static_cast<Tr *>(tp);
 	size_t cnt = 0;
@@ -145,8 +152,20 @@ extern "C" {
 void *ref_build(int dtype, int has_id, const void *pts, uint64_t n)
 {
 	try {
-		Handle *h = new Handle{dtype, has_id, nullptr};
+		Handle *h = new Handle{dtype, has_id, nullptr, 0};
 		h->tree = dispatch(dtype, has_id, [&]<typename T, int I>() { return build<T, I>(pts, n); });
+		return h;
+	} catch (...) {
+		return nullptr;
+	}
+}
+
+// Builds a StaticPSTCPURecur (searches only: ref_search; no export).
+void *ref_build_recur(int dtype, int has_id, const void *pts, uint64_t n)
+{
+	try {
+		Handle *h = new Handle{dtype, has_id, nullptr, 1};
+		h->tree = dispatch(dtype, has_id, [&]<typename T, int I>() { return build<T, I, true>(pts, n); });
 		return h;
 	} catch (...) {
 		return nullptr;
@@ -158,7 +177,13 @@ void ref_destroy(void *hp)
 	if (!hp)
 		return;
 	Handle *h = static_cast<Handle *>(hp);
-	dispatch(h->dtype, h->has_id, [&]<typename T, int I>() { destroy<T, I>(h->tree); return 0; });
+	dispatch(h->dtype, h->has_id, [&]<typename T, int I>() {
+		if (h->recur)
+			destroy<T, I, true>(h->tree);
+		else
+			destroy<T, I>(h->tree);
+		return 0;
+	});
 	delete h;
 }
 
@@ -185,6 +210,8 @@ int64_t ref_search(void *hp, int kind, const void *min1, const void *max1, const
 	Handle *h = static_cast<Handle *>(hp);
 	try {
 		return dispatch(h->dtype, h->has_id, [&]<typename T, int I>() {
+			if (h->recur)
+				return search<T, I, true>(h->tree, kind, as<T>(min1), as<T>(max1), as<T>(min2), ret_points, out, cap);
 			return search<T, I>(h->tree, kind, as<T>(min1), as<T>(max1), as<T>(min2), ret_points, out, cap);
 		});
 	} catch (...) {
