@@ -141,6 +141,11 @@ pst_status pst_export(const pst_tree *tree, void *dim1, void *dim2, void *med, u
 pst_status pst_search(pst_tree *tree, const pst_query *query, pst_ret ret, void **out_d,
                       uint64_t *count, pst_stream_t stream);
 
+/* Size prepass: the number of records the query would return (what the
+ * reference's searches leave in num_res_elems, pst/static-pst-gpu.tu:533-538),
+ * without producing them.  Blocks. */
+pst_status pst_count(pst_tree *tree, const pst_query *query, uint64_t *count, pst_stream_t stream);
+
 /* The three reference search calls with the reference's bound order. */
 pst_status pst_three_sided(pst_tree *tree, pst_value min1, pst_value max1, pst_value min2,
                            pst_ret ret, void **out_d, uint64_t *count, pst_stream_t stream);

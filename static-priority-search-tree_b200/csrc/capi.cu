@@ -319,6 +319,17 @@ pst_status pst_export(const pst_tree *tree, void *dim1, void *dim2, void *med, u
 	});
 }
 
+pst_status pst_count(pst_tree *tree, const pst_query *query, uint64_t *count, pst_stream_t stream)
+{
+	return guarded([&] {
+		if (!count)
+			fail(PST_ERR_INVALID, "null output");
+		*count = 0;
+		void *none = nullptr;
+		*count = run_single(tree, query, PST_RET_POINTS, &none, 0, false, reinterpret_cast<cudaStream_t>(stream));
+	});
+}
+
 pst_status pst_search(pst_tree *tree, const pst_query *query, pst_ret ret, void **out_d, uint64_t *count,
                       pst_stream_t stream)
 {

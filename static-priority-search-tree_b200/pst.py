@@ -86,6 +86,7 @@ def lib():
         "pst_info": (i32, [vp, P(u64), P(u32), P(u64), P(u64), P(i32), P(i32)]),
         "pst_export": (i32, [vp, vp, vp, vp, vp, vp]),
         "pst_search": (i32, [vp, P(Query), i32, P(vp), P(u64), vp]),
+        "pst_count": (i32, [vp, P(Query), P(u64), vp]),
         "pst_three_sided": (i32, [vp, u64, u64, u64, i32, P(vp), P(u64), vp]),
         "pst_two_sided_left": (i32, [vp, u64, u64, i32, P(vp), P(u64), vp]),
         "pst_two_sided_right": (i32, [vp, u64, u64, i32, P(vp), P(u64), vp]),
@@ -303,6 +304,13 @@ class StaticPSTGPU:
     def _ret(self, ret):
         r = ret if isinstance(ret, str) else ("ids" if ret is np.uint32 else "points")
         return r, (np.uint32 if r == "ids" else self.rec_point)
+
+    def count(self, kind: str, min1=0, max1=0, min2=0, stream=None) -> int:
+        """Number of points the query reports (pst_count), without producing them."""
+        q = Query(KIND[kind], 0, value(self.dt, min1), value(self.dt, max1), value(self.dt, min2))
+        cnt = C.c_uint64()
+        _check(lib().pst_count(self._h, C.byref(q), C.byref(cnt), _stream(stream)))
+        return cnt.value
 
     def search_device(self, kind: str, min1=0, max1=0, min2=0, ret="ids", stream=None):
         """The drop-in call itself: returns (device pointer, count) of the

@@ -26,6 +26,7 @@ def test_plain_search(pst, oracle, dt, n, ids, dup):
         points = (i % 2 == 1) or ids == "none"
         got = tr.search(kind, a, b, m2, ret="points" if points else "ids")
         assert np.array_equal(oracle.canon(got), _oracle_set(oracle, ref, kind, a, b, m2, points)), (kind, a, b, m2)
+        assert tr.count(kind, a, b, m2) == len(got)  # the size prepass
     tr.close()
 
 
