@@ -343,42 +343,51 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs_level(TreeDev<T> t, QDev<T>
 	const uint64_t gwarps = gthreads / 32, gwarp = gtid / 32;
 	const uint32_t lane = lane_id();
 
-	// boundary paths
+	// The level's three kinds of work go to disjoint sets of warps so that their
+	// dependent-load chains overlap instead of adding up: a few warps take the
+	// boundary paths, a few the seeds, the rest the records.
 	const uint32_t np = min(w.ctl->path_cnt[d], w.path_cap);
-	const uint4 *pin = (d & 1) ? w.path1 : w.path0;
-	for (uint64_t i = gtid; i < np; i += gthreads)
-		path_step<T>(t, qd, w, d, pin[i]);
-	__syncwarp();
-
-	// report-above seeds of this level: one or two candidate slots each, tested by
-	// their own lane
 	const uint32_t ns = min(w.ctl->seed_cnt[d], w.path_cap);
-	const uint4 *sin = (d & 1) ? w.seed1 : w.seed0;
-	for (uint64_t wb = gwarp * 32; wb < ns; wb += gwarps * 32) {
-		const bool valid = wb + lane < ns;
-		const uint4 sd = valid ? sin[wb + lane] : make_uint4(0, 0, 0, 0);
-		uint32_t cand = valid ? (sd.z & t.occ[sd.x >> 5]) : 0u;
-		uint32_t am = 0;
-		const T m2 = cand ? qd.min2[sd.y] : T(0);
-		while (cand) {
-			const uint32_t bt = __ffs(cand) - 1;
-			cand &= cand - 1;
-			am |= m2 <= t.dim2[sd.x + bt] ? 1u << bt : 0u;
-		}
-		add_counts(w, sd.y, __popc(am), valid);
-		const uint4 one[1] = {am ? block_record(sd.x, sd.y, am) : make_uint4(0, 0, 0, 0)};
-		append_blocks<1>(w, d, base_cur, one);
-	}
+	const uint64_t cap = gwarps / 8 + 1;
+	const uint64_t wp = min((uint64_t) (np + 31) / 32, cap);
+	const uint64_t ws = min((uint64_t) (ns + 31) / 32, cap);
+	const uint64_t wr = gwarps - wp - ws;  // >= 1: the grid has at least 4 warps
 
-	// expansion of the previous level's alive records into their child blocks
-	for (uint64_t wb = gwarp * 32; wb < n_prev; wb += gwarps * 32) {
-		const bool valid = wb + lane < n_prev;
-		const uint4 mine = valid ? w.rec[base_prev + wb + lane] : make_uint4(0, 0, 0, 0);
-		uint4 child[2];
-		uint32_t pts;
-		expand_records<T>(t, qd.min2, mine, valid, s_stage[threadIdx.x >> 5], child, pts);
-		add_counts(w, mine.y, pts, valid);
-		append_blocks<2>(w, d, base_cur, child);
+	if (gwarp < wp) {
+		// boundary paths, one task per lane
+		const uint4 *pin = (d & 1) ? w.path1 : w.path0;
+		for (uint64_t i = gwarp * 32 + lane; i < np; i += wp * 32)
+			path_step<T>(t, qd, w, d, pin[i]);
+	} else if (gwarp < wp + ws) {
+		// report-above seeds of this level: one or two candidate slots each, tested
+		// by their own lane
+		const uint4 *sin = (d & 1) ? w.seed1 : w.seed0;
+		for (uint64_t wb = (gwarp - wp) * 32; wb < ns; wb += ws * 32) {
+			const bool valid = wb + lane < ns;
+			const uint4 sd = valid ? sin[wb + lane] : make_uint4(0, 0, 0, 0);
+			uint32_t cand = valid ? (sd.z & t.occ[sd.x >> 5]) : 0u;
+			uint32_t am = 0;
+			const T m2 = cand ? qd.min2[sd.y] : T(0);
+			while (cand) {
+				const uint32_t bt = __ffs(cand) - 1;
+				cand &= cand - 1;
+				am |= m2 <= t.dim2[sd.x + bt] ? 1u << bt : 0u;
+			}
+			add_counts(w, sd.y, __popc(am), valid);
+			const uint4 one[1] = {am ? block_record(sd.x, sd.y, am) : make_uint4(0, 0, 0, 0)};
+			append_blocks<1>(w, d, base_cur, one);
+		}
+	} else {
+		// expansion of the previous level's alive records into their child blocks
+		for (uint64_t wb = (gwarp - wp - ws) * 32; wb < n_prev; wb += wr * 32) {
+			const bool valid = wb + lane < n_prev;
+			const uint4 mine = valid ? w.rec[base_prev + wb + lane] : make_uint4(0, 0, 0, 0);
+			uint4 child[2];
+			uint32_t pts;
+			expand_records<T>(t, qd.min2, mine, valid, s_stage[threadIdx.x >> 5], child, pts);
+			add_counts(w, mine.y, pts, valid);
+			append_blocks<2>(w, d, base_cur, child);
+		}
 	}
 }
 
