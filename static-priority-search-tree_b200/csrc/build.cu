@@ -1008,13 +1008,54 @@ void build_tree(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 			t.idtype == PST_ID_U32 ? build_impl<int32_t, true>(t, pts_d, n, s) : build_impl<int32_t, false>(t, pts_d, n, s);
 			break;
 		}
+		finish_tree_aux(t, s);
 		PST_CUDA(cudaStreamSynchronize(s));
 	} catch (...) {
 		cudaStreamSynchronize(s);
-		cudaFree(t.mem);
-		t.mem = nullptr;
+		free_tree(t);
 		throw;
 	}
+}
+
+namespace {
+
+// Block j of level L: positions [2^L + 64 j, 2^L + 64 j + 64); its children are the
+// 128 positions from 2^(L+1) + 128 j, i.e. occupancy words 2^(L+1)/32 + 4 j .. + 3.
+__global__ void k_last_par(const uint32_t *__restrict__ occ, uint32_t L, uint32_t *out)
+{
+	const uint64_t nb = (1ull << L) / 64;
+	const uint64_t w0 = (1ull << (L + 1)) / 32;
+	for (uint64_t j = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; j < ((nb + 31) & ~31ull);
+	     j += (uint64_t) gridDim.x * blockDim.x) {
+		bool any = false;
+		if (j < nb) {
+			const uint4 o = *reinterpret_cast<const uint4 *>(occ + w0 + 4 * j);
+			any = (o.x | o.y | o.z | o.w) != 0;
+		}
+		const uint32_t bits = __ballot_sync(0xFFFFFFFFu, any);
+		if ((threadIdx.x & 31) == 0)
+			out[j >> 5] = bits;
+	}
+}
+
+}  // namespace
+
+void finish_tree_aux(TreeStorage &t, cudaStream_t s)
+{
+	if (t.levels < 8)  // level D-2 spans less than one 64-slot block
+		return;
+	const uint32_t L = t.levels - 2;
+	const uint64_t nb = (1ull << L) / 64;
+	const uint64_t words = (nb + 31) / 32;
+	cudaError_t e = cudaMalloc(&t.last_par, words * 4);
+	if (e == cudaErrorMemoryAllocation) {
+		cudaGetLastError();
+		fail(PST_ERR_NOMEM, "search index allocation failed");
+	}
+	check_cuda(e, "cudaMalloc(search index)");
+	const unsigned g = (unsigned) std::max<uint64_t>(1, std::min<uint64_t>((nb + 255) / 256, 65535));
+	k_last_par<<<g, 256, 0, s>>>(t.occ, L, t.last_par);
+	PST_CUDA(cudaGetLastError());
 }
 
 void free_tree(TreeStorage &t)
@@ -1022,6 +1063,9 @@ void free_tree(TreeStorage &t)
 	if (t.mem)
 		cudaFree(t.mem);
 	t.mem = nullptr;
+	if (t.last_par)
+		cudaFree(t.last_par);
+	t.last_par = nullptr;
 }
 
 void export_tree(const TreeStorage &t, void *dim1, void *dim2, void *med, uint32_t *ids, uint8_t *bitcodes)

@@ -101,6 +101,10 @@ struct TreeDev {
 	const uint32_t *occ;  // occupancy bitmap, 2^levels bits
 	uint64_t n;
 	uint32_t levels;      // D = floor(log2 n) + 1
+	// One bit per 64-slot block of level D-2: does any of its children exist?
+	// (null when D-2 < 6).  A sparse last level lets the last expansion skip the
+	// records whose blocks have no children before reading their occupancy.
+	const uint32_t *last_par;
 };
 
 // Number of levels of a tree of n points: floor(log2 n) + 1 (0 for n == 0).

@@ -249,13 +249,21 @@ struct WarpStage {
 // its two child records (blocks 2b and 2b + 64).
 template <typename T>
 __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__restrict__ min2s, const uint4 &mine,
-                                               bool valid, WarpStage<T> &st, uint4 (&child)[2], uint32_t &pts)
+                                               bool valid, bool last_level, WarpStage<T> &st, uint4 (&child)[2],
+                                               uint32_t &pts)
 {
 	constexpr int U = sizeof(T) == 4 ? 4 : 2;  // records in flight
 	const uint32_t lane = lane_id();
 	const uint32_t r = lane >> 3, qd = lane & 7;
 	uint4 cand = make_uint4(0, 0, 0, 0);
-	if (valid) {
+	bool has_children = valid;
+	if (valid && last_level && t.last_par) {
+		// expanding into the last level: most blocks of a sparse last level have no
+		// children, which one bit per parent block tells before any occupancy read
+		const uint32_t j = (mine.x - (1u << (t.levels - 2))) >> 6;
+		has_children = (t.last_par[j >> 5] >> (j & 31)) & 1u;
+	}
+	if (has_children) {
 		const uint4 occ = *reinterpret_cast<const uint4 *>(t.occ + ((2 * mine.x) >> 5));
 		cand = make_uint4(spread16(mine.z) & occ.x, spread16(mine.z >> 16) & occ.y, spread16(mine.w) & occ.z,
 		                  spread16(mine.w >> 16) & occ.w);
@@ -384,7 +392,7 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs_level(TreeDev<T> t, QDev<T>
 			const uint4 mine = valid ? w.rec[base_prev + wb + lane] : make_uint4(0, 0, 0, 0);
 			uint4 child[2];
 			uint32_t pts;
-			expand_records<T>(t, qd.min2, mine, valid, s_stage[threadIdx.x >> 5], child, pts);
+			expand_records<T>(t, qd.min2, mine, valid, d + 1 == t.levels, s_stage[threadIdx.x >> 5], child, pts);
 			add_counts(w, mine.y, pts, valid);
 			append_blocks<2>(w, d, base_cur, child);
 		}

@@ -149,10 +149,11 @@ void load_tree(TreeStorage &t, const void *host, uint64_t size, cudaStream_t s)
 		try {
 			PST_CUDA(cudaMemcpyAsync(t.mem, static_cast<const unsigned char *>(host) + HEADER_BYTES, bytes,
 			                         cudaMemcpyHostToDevice, s));
+			finish_tree_aux(t, s);
 			PST_CUDA(cudaStreamSynchronize(s));
 		} catch (...) {
-			cudaFree(t.mem);
-			t.mem = nullptr;
+			cudaStreamSynchronize(s);
+			free_tree(t);
 			throw;
 		}
 	}
@@ -220,11 +221,11 @@ void load_tree_file(TreeStorage &t, const char *path, cudaStream_t s)
 			                         cudaMemcpyHostToDevice, s));
 			PST_CUDA(cudaEventRecord(pp.done[i & 1], s));
 		}
+		finish_tree_aux(t, s);
 		PST_CUDA(cudaStreamSynchronize(s));
 	} catch (...) {
 		cudaStreamSynchronize(s);
-		cudaFree(t.mem);
-		t.mem = nullptr;
+		free_tree(t);
 		throw;
 	}
 }
