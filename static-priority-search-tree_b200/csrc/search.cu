@@ -247,17 +247,16 @@ struct WarpStage {
 // load (two for doubles), issued only where it has candidates; each 8-lane group
 // ORs its nibbles into one 32-slot child row, and the owner reads the four rows as
 // its two child records (blocks 2b and 2b + 64).
-template <typename T>
+template <typename T, bool LAST>
 __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__restrict__ min2s, const uint4 &mine,
-                                               bool valid, bool last_level, WarpStage<T> &st, uint4 (&child)[2],
-                                               uint32_t &pts)
+                                               bool valid, WarpStage<T> &st, uint4 (&child)[2], uint32_t &pts)
 {
 	constexpr int U = sizeof(T) == 4 ? 4 : 2;  // records in flight
 	const uint32_t lane = lane_id();
 	const uint32_t r = lane >> 3, qd = lane & 7;
 	uint4 cand = make_uint4(0, 0, 0, 0);
 	bool has_children = valid;
-	if (valid && last_level && t.last_par) {
+	if (LAST && valid) {
 		// expanding into the last level: most blocks of a sparse last level have no
 		// children, which one bit per parent block tells before any occupancy read
 		const uint32_t j = (mine.x - (1u << (t.levels - 2))) >> 6;
@@ -324,7 +323,9 @@ __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__r
 	__syncwarp();  // the stage is reused by the warp's next batch
 }
 
-template <typename T>
+// LAST: the expansion into the last level of a tree with TreeDev::last_par (its own
+// instantiation, so the other levels keep their register budget).
+template <typename T, bool LAST>
 __global__ void __launch_bounds__(BFS_THREADS) k_bfs_level(TreeDev<T> t, QDev<T> qd, WorkDev w, uint32_t d)
 {
 	// Once the frontier has overflowed, the reservation that crossed the capacity
@@ -392,7 +393,7 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs_level(TreeDev<T> t, QDev<T>
 			const uint4 mine = valid ? w.rec[base_prev + wb + lane] : make_uint4(0, 0, 0, 0);
 			uint4 child[2];
 			uint32_t pts;
-			expand_records<T>(t, qd.min2, mine, valid, d + 1 == t.levels, s_stage[threadIdx.x >> 5], child, pts);
+			expand_records<T, LAST>(t, qd.min2, mine, valid, s_stage[threadIdx.x >> 5], child, pts);
 			add_counts(w, mine.y, pts, valid);
 			append_blocks<2>(w, d, base_cur, child);
 		}
@@ -604,9 +605,19 @@ unsigned emit_grid()
 }
 
 template <typename T>
+void launch_level(const TreeDev<T> &tv, const QDev<T> &qd, const WorkDev &w, uint32_t d, unsigned grid,
+                  unsigned threads, cudaStream_t s)
+{
+	if (d + 1 == tv.levels && tv.last_par)
+		k_bfs_level<T, true><<<grid, threads, 0, s>>>(tv, qd, w, d);
+	else
+		k_bfs_level<T, false><<<grid, threads, 0, s>>>(tv, qd, w, d);
+}
+
+template <typename T>
 const void *bfs_kernel_ptr()
 {
-	return reinterpret_cast<const void *>(&k_bfs_level<T>);
+	return reinterpret_cast<const void *>(&k_bfs_level<T, false>);
 }
 
 }  // namespace
@@ -730,7 +741,7 @@ void Batch::enqueue_count(cudaStream_t s)
 	k_unpack_queries<T><<<ug, 256, 0, s>>>(q_raw, ctl, kind, static_cast<T *>(min1), static_cast<T *>(max1),
 	                                       static_cast<T *>(min2), path0);
 	for (uint32_t d = 0; d < tv.levels; d++)
-		k_bfs_level<T><<<grid, threads, 0, s>>>(tv, qd, w, d);
+		launch_level<T>(tv, qd, w, d, grid, threads, s);
 	exclusive_scan<uint64_t>(counts, offsets, max_q, scan_tmp, &ctl->total, s);
 	PST_CUDA(cudaMemcpyAsync(offsets + max_q, &ctl->total, 8, cudaMemcpyDeviceToDevice, s));
 	PST_CUDA(cudaGetLastError());
@@ -977,7 +988,7 @@ uint64_t noalloc_run(TreeStorage &t, const pst_query &q, pst_ret ret, void *out,
 	k_check_kinds<<<1, 32, 0, s>>>(qraw, ctl);
 	k_unpack_queries<T><<<1, 32, 0, s>>>(qraw, ctl, kind, min1, max1, min2, path0);
 	for (uint32_t d = 0; d < tv.levels; d++)
-		k_bfs_level<T><<<grid, BFS_THREADS, 0, s>>>(tv, qd, w, d);
+		launch_level<T>(tv, qd, w, d, grid, BFS_THREADS, s);
 	exclusive_scan<uint64_t>(counts, offsets, 1, scan, &ctl->total, s);
 	PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
 	PST_CUDA(cudaStreamSynchronize(s));
