@@ -14,7 +14,10 @@
 //     chunk: 32 consecutive slots of one level, tested by one warp with one coalesced
 //     load.  The frontier is kept as "alive records" only — (chunk, query, mask of
 //     reported slots) — and the next level expands each record into its two child
-//     chunks (spread16), masked by occupancy before anything is loaded.
+//     chunks (spread16), masked by occupancy before anything is loaded.  Every
+//     level but the last is full (a level-d node holds at least
+//     floor((n + 1) / 2^d) - 1 >= 1 points for d <= D - 2), so occupancy is read
+//     only for children on the last level.
 // A count of every query falls out of the pass; an exclusive scan gives each
 // query's exact output offset, and a flat emit kernel writes ids (or points) from
 // the alive records.
@@ -34,7 +37,6 @@ namespace {
 constexpr uint32_t MODE_THREE = 3, MODE_LEFT = 1, MODE_RIGHT = 2;
 constexpr uint32_t FULL = 0xFFFFFFFFu;
 
-__device__ __forceinline__ bool occ_bit(const uint32_t *occ, uint32_t h) { return (occ[h >> 5] >> (h & 31)) & 1u; }
 
 template <typename T>
 struct QDev {
@@ -69,80 +71,107 @@ __device__ __forceinline__ uint4 block_record(uint32_t pos32, uint32_t q, uint32
 }
 
 template <typename T>
-__device__ void path_step(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev &w, uint32_t d, uint4 task)
+__device__ __forceinline__ void path_step(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev &w, uint32_t d,
+                                          uint4 task, bool valid)
 {
+	const uint32_t lane = lane_id();
 	const uint32_t h = task.x, q = task.y, mode = task.z;
-	const T min2 = qd.min2[q];
-	const T v2 = t.dim2[h];
-	if (!(min2 <= v2))
-		return;
-	const uint32_t kind = qd.kind[q];
-	const T min1 = qd.min1[q], max1 = qd.max1[q];
-	const T v1 = t.dim1[h];
-	const bool rep = kind == PST_Q_THREE ? (min1 <= v1 && v1 <= max1) : kind == PST_Q_LEFT ? (v1 <= max1) : (v1 >= min1);
+	const uint32_t l = 2 * h, r = 2 * h + 1;
+	const bool inner = d + 1 < t.levels;  // the node has a median and may have children
+	bool rep = false;
+	uint32_t pl = 0, pr = 0;      // continue as a path task with this mode (0 = no)
+	bool rl = false, rr = false;  // report-above subtree
+	if (valid) {
+		// every value the step may use is loaded at once: one round trip, not a chain.
+		// Every level but the last is full, so only children on the last level need
+		// their occupancy read.
+		const T min2 = qd.min2[q];
+		const T v2 = t.dim2[h];
+		const uint32_t kind = qd.kind[q];
+		const T min1 = qd.min1[q], max1 = qd.max1[q];
+		const T v1 = t.dim1[h];
+		const uint32_t ow = !inner ? 0u : d + 2 < t.levels ? FULL : t.occ[l >> 5];
+		const T m = inner ? t.med[h] : T(0);
+		if (min2 <= v2) {
+			rep = kind == PST_Q_THREE ? (min1 <= v1 && v1 <= max1) : kind == PST_Q_LEFT ? (v1 <= max1) : (v1 >= min1);
+			const bool hl = (ow >> (l & 31)) & 1u, hr = (ow >> (r & 31)) & 1u;
+			if (mode == MODE_THREE) {
+				if (min1 <= m && m <= max1) {
+					pl = hl ? MODE_RIGHT : 0;
+					pr = hr ? MODE_LEFT : 0;
+				} else if (max1 < m && hl) {
+					pl = MODE_THREE;
+				} else if (m < min1 && hr) {
+					pr = MODE_THREE;
+				}
+			} else if (mode == MODE_LEFT) {
+				if (m <= max1) {
+					rl = hl;
+					pr = hr ? MODE_LEFT : 0;
+				} else if (hl) {
+					pl = MODE_LEFT;
+				}
+			} else {
+				if (m >= min1) {
+					pl = hl ? MODE_RIGHT : 0;
+					rr = hr;
+				} else if (hr) {
+					pr = MODE_RIGHT;
+				}
+			}
+		}
+	}
+	// The warp's reported nodes, next-level paths and seeds each take one reservation,
+	// and lane 0 issues the three together.  At most two boundary paths per query and
+	// level, each leaving at most one seed, so path_cap = 2 * max_q holds every list.
+	const bool seed = rl || rr;
+	const uint32_t repm = __ballot_sync(FULL, rep);
+	const uint32_t seedm = __ballot_sync(FULL, seed);
+	const uint32_t npl = (pl ? 1u : 0u) + (pr ? 1u : 0u);
+	const uint32_t inc = warp_incl_scan(npl);
+	const uint32_t tot = __shfl_sync(FULL, inc, 31);
+	uint32_t b_rep = 0, b_path = 0, b_seed = 0;
+	if (lane == 0) {
+		if (repm)
+			b_rep = atomicAdd(&w.ctl->rec_cnt, (uint32_t) __popc(repm));
+		if (tot)
+			b_path = atomicAdd(&w.ctl->path_cnt[d + 1], tot);
+		if (seedm)
+			b_seed = atomicAdd(&w.ctl->seed_cnt[d + 1], (uint32_t) __popc(seedm));
+	}
+	b_rep = __shfl_sync(FULL, b_rep, 0);
+	b_path = __shfl_sync(FULL, b_path, 0);
+	b_seed = __shfl_sync(FULL, b_seed, 0);
 	if (rep) {
-		const uint32_t i = atomicAdd(&w.ctl->rec_cnt, 1u);
+		const uint32_t i = b_rep + __popc(repm & lanemask_lt());
 		if (i < w.ro_cap)
 			w.ro[i] = block_record(h & ~31u, q, 1u << (h & 31));
 		else
 			atomicOr(&w.ctl->flags, BATCH_FLAG_INTERNAL);
 		atomicAdd((unsigned long long *) &w.counts[q], 1ull);
 	}
-	if (d + 1 >= t.levels)
-		return;
-	const uint32_t l = 2 * h, r = 2 * h + 1;
-	const bool hl = occ_bit(t.occ, l), hr = occ_bit(t.occ, r);
-	if (!hl && !hr)
-		return;
-	const T m = t.med[h];
-	uint32_t pl = 0, pr = 0;      // continue as a path task with this mode (0 = no)
-	bool rl = false, rr = false;  // report-above subtree
-	if (mode == MODE_THREE) {
-		if (min1 <= m && m <= max1) {
-			pl = hl ? MODE_RIGHT : 0;
-			pr = hr ? MODE_LEFT : 0;
-		} else if (max1 < m && hl) {
-			pl = MODE_THREE;
-		} else if (m < min1 && hr) {
-			pr = MODE_THREE;
+	if (npl) {
+		uint32_t i = b_path + inc - npl;
+		uint4 *pout = ((d + 1) & 1) ? w.path1 : w.path0;
+		if (pl) {
+			if (i < w.path_cap)
+				pout[i] = make_uint4(l, q, pl, 0);
+			else
+				atomicOr(&w.ctl->flags, BATCH_FLAG_INTERNAL);
+			i++;
 		}
-	} else if (mode == MODE_LEFT) {
-		if (m <= max1) {
-			rl = hl;
-			pr = hr ? MODE_LEFT : 0;
-		} else if (hl) {
-			pl = MODE_LEFT;
-		}
-	} else {
-		if (m >= min1) {
-			pl = hl ? MODE_RIGHT : 0;
-			rr = hr;
-		} else if (hr) {
-			pr = MODE_RIGHT;
+		if (pr) {
+			if (i < w.path_cap)
+				pout[i] = make_uint4(r, q, pr, 0);
+			else
+				atomicOr(&w.ctl->flags, BATCH_FLAG_INTERNAL);
 		}
 	}
-	// at most two boundary paths per query and level, each leaving at most one seed,
-	// so path_cap = 2 * max_q holds every list
-	uint4 *pout = ((d + 1) & 1) ? w.path1 : w.path0;
-	if (pl) {
-		const uint32_t i = atomicAdd(&w.ctl->path_cnt[d + 1], 1u);
-		if (i < w.path_cap)
-			pout[i] = make_uint4(l, q, pl, 0);
-		else
-			atomicOr(&w.ctl->flags, BATCH_FLAG_INTERNAL);
-	}
-	if (pr) {
-		const uint32_t i = atomicAdd(&w.ctl->path_cnt[d + 1], 1u);
-		if (i < w.path_cap)
-			pout[i] = make_uint4(r, q, pr, 0);
-		else
-			atomicOr(&w.ctl->flags, BATCH_FLAG_INTERNAL);
-	}
-	if (rl || rr) {
+	if (seed) {
 		// l and r share a chunk
 		const uint32_t bits = (rl ? 1u << (l & 31) : 0u) | (rr ? 1u << (r & 31) : 0u);
 		uint4 *sout = ((d + 1) & 1) ? w.seed1 : w.seed0;
-		const uint32_t i = atomicAdd(&w.ctl->seed_cnt[d + 1], 1u);
+		const uint32_t i = b_seed + __popc(seedm & lanemask_lt());
 		if (i < w.path_cap)
 			sout[i] = make_uint4(l & ~31u, q, bits, 0u);
 		else
@@ -241,15 +270,17 @@ struct WarpStage {
 
 // Expands the records held by the warp (lane k owns record `mine`; the valid lanes
 // are a prefix) into their child records.  Each lane first stages its record's
-// candidate child slots; records without any (all children absent, e.g. above a
-// sparse last level) cost nothing more.  Then the whole warp takes the live records
+// candidate child slots (`full`: the children's level is full, so the candidates
+// are the spread parent bits with no occupancy read); records without any (all
+// children absent, e.g. above a sparse last level) cost nothing more.  Then the whole warp takes the live records
 // U at a time: lane l tests the child slots [2b + 4l, 2b + 4l + 4) with one 16-byte
 // load (two for doubles), issued only where it has candidates; each 8-lane group
 // ORs its nibbles into one 32-slot child row, and the owner reads the four rows as
 // its two child records (blocks 2b and 2b + 64).
 template <typename T, bool LAST>
 __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__restrict__ min2s, const uint4 &mine,
-                                               bool valid, WarpStage<T> &st, uint4 (&child)[2], uint32_t &pts)
+                                               bool valid, bool full, WarpStage<T> &st, uint4 (&child)[2],
+                                               uint32_t &pts)
 {
 	constexpr int U = sizeof(T) == 4 ? 4 : 2;  // records in flight
 	const uint32_t lane = lane_id();
@@ -263,7 +294,9 @@ __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__r
 		has_children = (t.last_par[j >> 5] >> (j & 31)) & 1u;
 	}
 	if (has_children) {
-		const uint4 occ = *reinterpret_cast<const uint4 *>(t.occ + ((2 * mine.x) >> 5));
+		// children on a full level (every level but the last) need no occupancy read
+		const uint4 occ = full ? make_uint4(FULL, FULL, FULL, FULL)
+		                       : *reinterpret_cast<const uint4 *>(t.occ + ((2 * mine.x) >> 5));
 		cand = make_uint4(spread16(mine.z) & occ.x, spread16(mine.z >> 16) & occ.y, spread16(mine.w) & occ.z,
 		                  spread16(mine.w >> 16) & occ.w);
 	}
@@ -326,7 +359,7 @@ __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__r
 // LAST: the expansion into the last level of a tree with TreeDev::last_par (its own
 // instantiation, so the other levels keep their register budget).
 template <typename T, bool LAST>
-__global__ void __launch_bounds__(BFS_THREADS) k_bfs_level(TreeDev<T> t, QDev<T> qd, WorkDev w, uint32_t d)
+__global__ void __launch_bounds__(BFS_THREADS, 4) k_bfs_level(TreeDev<T> t, QDev<T> qd, WorkDev w, uint32_t d)
 {
 	// Once the frontier has overflowed, the reservation that crossed the capacity
 	// left some slots below it unwritten, so nothing of the previous level may be
@@ -365,8 +398,10 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs_level(TreeDev<T> t, QDev<T>
 	if (gwarp < wp) {
 		// boundary paths, one task per lane
 		const uint4 *pin = (d & 1) ? w.path1 : w.path0;
-		for (uint64_t i = gwarp * 32 + lane; i < np; i += wp * 32)
-			path_step<T>(t, qd, w, d, pin[i]);
+		for (uint64_t wb = gwarp * 32; wb < np; wb += wp * 32) {
+			const bool valid = wb + lane < np;
+			path_step<T>(t, qd, w, d, valid ? pin[wb + lane] : make_uint4(0, 0, 0, 0), valid);
+		}
 	} else if (gwarp < wp + ws) {
 		// report-above seeds of this level: one or two candidate slots each, tested
 		// by their own lane
@@ -374,26 +409,43 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs_level(TreeDev<T> t, QDev<T>
 		for (uint64_t wb = (gwarp - wp) * 32; wb < ns; wb += ws * 32) {
 			const bool valid = wb + lane < ns;
 			const uint4 sd = valid ? sin[wb + lane] : make_uint4(0, 0, 0, 0);
-			uint32_t cand = valid ? (sd.z & t.occ[sd.x >> 5]) : 0u;
 			uint32_t am = 0;
-			const T m2 = cand ? qd.min2[sd.y] : T(0);
-			while (cand) {
-				const uint32_t bt = __ffs(cand) - 1;
-				cand &= cand - 1;
-				am |= m2 <= t.dim2[sd.x + bt] ? 1u << bt : 0u;
+			if (sd.z) {
+				// a seed's candidates are the two children of one node, an aligned pair of
+				// slots: their dim2, the occupancy (read on the last level only, all
+				// others being full) and min2 come in one round trip
+				const uint32_t p = (__ffs(sd.z) - 1) & ~1u;
+				const uint32_t cand = sd.z & (d + 1 < t.levels ? FULL : t.occ[sd.x >> 5]);
+				const T m2 = qd.min2[sd.y];
+				T v[2];
+				if constexpr (sizeof(T) == 4) {
+					const uint2 x = *reinterpret_cast<const uint2 *>(t.dim2 + sd.x + p);
+					memcpy(&v[0], &x.x, 4);
+					memcpy(&v[1], &x.y, 4);
+				} else {
+					const double2 x = *reinterpret_cast<const double2 *>(t.dim2 + sd.x + p);
+					v[0] = x.x;
+					v[1] = x.y;
+				}
+#pragma unroll
+				for (int j = 0; j < 2; j++)
+					am |= (((cand >> (p + j)) & 1u) && m2 <= v[j]) ? 1u << (p + j) : 0u;
 			}
 			add_counts(w, sd.y, __popc(am), valid);
 			const uint4 one[1] = {am ? block_record(sd.x, sd.y, am) : make_uint4(0, 0, 0, 0)};
 			append_blocks<1>(w, d, base_cur, one);
 		}
 	} else {
-		// expansion of the previous level's alive records into their child blocks
+		// expansion of the previous level's alive records into their child blocks, 32
+		// consecutive records per warp (their children stay together in the next
+		// level's region, which keeps that level's chunks local)
 		for (uint64_t wb = (gwarp - wp - ws) * 32; wb < n_prev; wb += wr * 32) {
 			const bool valid = wb + lane < n_prev;
 			const uint4 mine = valid ? w.rec[base_prev + wb + lane] : make_uint4(0, 0, 0, 0);
 			uint4 child[2];
 			uint32_t pts;
-			expand_records<T, LAST>(t, qd.min2, mine, valid, s_stage[threadIdx.x >> 5], child, pts);
+			expand_records<T, LAST>(t, qd.min2, mine, valid, !LAST && d + 1 < t.levels, s_stage[threadIdx.x >> 5],
+			                        child, pts);
 			add_counts(w, mine.y, pts, valid);
 			append_blocks<2>(w, d, base_cur, child);
 		}
