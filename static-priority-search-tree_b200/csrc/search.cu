@@ -579,7 +579,9 @@ __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mi
 								rec.id = j ? idv[u].y : idv[u].x;
 							static_cast<Pt *>(out)[oo] = rec;
 						} else {
-							static_cast<uint32_t *>(out)[oo] = j ? idv[u].y : idv[u].x;
+							// evict-first: the output streams through L2 once and should not push
+							// out tree rows that other queries' records read again
+							__stcs(static_cast<uint32_t *>(out) + oo, j ? idv[u].y : idv[u].x);
 						}
 					}
 					oo++;
