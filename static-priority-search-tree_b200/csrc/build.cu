@@ -506,6 +506,10 @@ struct SubtreeSmem {
 	static_assert(KEYA % 8 == 0 && BYTES <= 227 * 1024, "subtree builder shared memory");
 };
 
+// Chunks of ST_THREADS positions the key gather reads: a node's range holds its
+// cN <= ST_CAP free points and at most one point taken by each ancestor (< 32).
+constexpr int ST_GATHER = ST_CAP / ST_THREADS + 1;
+
 // Count and start of every sub-node of the current sub-level (in that sub-level's
 // compacted key order) are kept in shared memory and derived level to level
 // without a scan: going down one level removes each node's point (every node
@@ -529,6 +533,9 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 	uint16_t *scnt = reinterpret_cast<uint16_t *>(st_smem + SM::CNT);     // [ST_CAP]
 	uint16_t *sstart = reinterpret_cast<uint16_t *>(st_smem + SM::START); // [ST_CAP]
 	uint32_t *ws = reinterpret_cast<uint32_t *>(st_smem + SM::WS);        // [33]
+	__shared__ uint32_t s_pre[ST_GATHER][ST_THREADS / 32];
+	__shared__ uint64_t s_pk[ST_THREADS / 32];
+	__shared__ uint32_t s_pi[ST_THREADS / 32];
 	__shared__ uint32_t s_n;
 
 	const uint32_t j = blockIdx.x;
@@ -537,7 +544,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 		return;
 	const uint32_t lo = L0 ? B[j] : 0u;
 	const uint32_t hi = L0 ? B[j + 1] : (uint32_t) c.n;
-	if (lo >= hi || hi > c.n || cN64 > ST_CAP) {
+	if (lo >= hi || hi > c.n || cN64 > ST_CAP || hi - lo > (uint32_t) (ST_GATHER * ST_THREADS)) {
 		if (threadIdx.x == 0)
 			atomicOr(c.err, 16u);
 		return;
@@ -545,26 +552,57 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 	const uint32_t cN = (uint32_t) cN64;
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = ST_THREADS / 32;
 
-	// Gather the keys of the points still free in [lo, hi), in dim1 order.
-	if (threadIdx.x == 0)
-		s_n = 0;
-	__syncthreads();
-	for (uint32_t b = lo; b < hi; b += ST_THREADS) {
-		const uint32_t i = b + threadIdx.x;
-		const bool keep = i < hi && !c.is_taken(i);
-		const uint64_t v = keep ? c.c2s[i] : 0;
-		uint32_t tot;
-		const uint32_t off = block_excl_scan<uint32_t>(keep ? 1u : 0u, &tot, ws);
-		const uint32_t base = s_n;
-		if (keep && base + off < ST_CAP) {
-			kc[base + off] = v;
-			sc[base + off] = (uint16_t) (base + off);
+	// Gather the keys of the points still free in [lo, hi), in dim1 order: every
+	// read in flight at once, then one prefix over (chunk, warp).
+	{
+		uint64_t v[ST_GATHER];
+		uint32_t m[ST_GATHER];
+#pragma unroll
+		for (int u = 0; u < ST_GATHER; u++) {
+			const uint32_t i = lo + (uint32_t) u * ST_THREADS + threadIdx.x;
+			const bool keep = i < hi && !c.is_taken(i);
+			v[u] = keep ? c.c2s[i] : 0;
+			m[u] = __ballot_sync(0xFFFFFFFFu, keep);
+			if (lane == 0)
+				s_pre[u][warp] = __popc(m[u]);
 		}
 		__syncthreads();
-		if (threadIdx.x == 0)
-			s_n = base + tot;
+		if (warp == 0) {
+			// (chunk, warp) pairs in order; lane l sums pairs [l * PER, l * PER + PER)
+			constexpr int PAIRS = ST_GATHER * (ST_THREADS / 32), PER = (PAIRS + 31) / 32;
+			uint32_t *flat = &s_pre[0][0];
+			uint32_t loc[PER], sum = 0;
+#pragma unroll
+			for (int k = 0; k < PER; k++) {
+				const int q = lane * PER + k;
+				loc[k] = q < PAIRS ? flat[q] : 0u;
+				sum += loc[k];
+			}
+			const uint32_t inc = warp_incl_scan(sum);
+			uint32_t run = inc - sum;
+#pragma unroll
+			for (int k = 0; k < PER; k++) {
+				const int q = lane * PER + k;
+				if (q < PAIRS)
+					flat[q] = run;
+				run += loc[k];
+			}
+			if (lane == 31)
+				s_n = inc;
+		}
 		__syncthreads();
+#pragma unroll
+		for (int u = 0; u < ST_GATHER; u++) {
+			if ((m[u] >> lane) & 1u) {
+				const uint32_t pos = s_pre[u][warp] + __popc(m[u] & lanemask_lt());
+				if (pos < ST_CAP) {
+					kc[pos] = v[u];
+					sc[pos] = (uint16_t) pos;
+				}
+			}
+		}
 	}
+	__syncthreads();
 	if (s_n != cN) {
 		if (threadIdx.x == 0)
 			atomicOr(c.err, 2u);
@@ -601,7 +639,44 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 		const uint32_t nsub = 1u << s;
 		const bool wide = present / nsub >= 64;
 		// arg-max of every sub-node (keys are distinct)
-		if (wide) {
+		if (wide && nsub < (uint32_t) nwarps) {
+			// fewer sub-nodes than warps: each sub-node's keys are split over
+			// nwarps / nsub warps, whose maxima meet in shared memory
+			const uint32_t W = (uint32_t) nwarps / nsub, t = warp / W, p = warp % W;
+			const uint32_t ct = scnt[t], st = sstart[t];
+			const uint32_t a = st + (uint32_t) ((uint64_t) ct * p / W), e = st + (uint32_t) ((uint64_t) ct * (p + 1) / W);
+			uint64_t bk = 0;
+			uint32_t bi = 0;
+			for (uint32_t i = a + lane; i < e; i += 32)
+				if (kc[i] > bk) {
+					bk = kc[i];
+					bi = i;
+				}
+#pragma unroll
+			for (int o = 16; o > 0; o >>= 1) {
+				const uint64_t ok = __shfl_xor_sync(0xFFFFFFFFu, bk, o);
+				const uint32_t oi = __shfl_xor_sync(0xFFFFFFFFu, bi, o);
+				if (ok > bk) {
+					bk = ok;
+					bi = oi;
+				}
+			}
+			if (lane == 0) {
+				s_pk[warp] = bk;
+				s_pi[warp] = bi;
+			}
+			__syncthreads();
+			if (threadIdx.x < nsub) {
+				uint64_t mk = 0;
+				uint32_t mi = 0;
+				for (uint32_t q = threadIdx.x * W; q < threadIdx.x * W + W; q++)
+					if (s_pk[q] > mk) {
+						mk = s_pk[q];
+						mi = s_pi[q];
+					}
+				topi[threadIdx.x] = (uint16_t) mi;
+			}
+		} else if (wide) {
 			for (uint32_t t = warp; t < nsub; t += nwarps) {
 				const uint32_t ct = scnt[t], st = sstart[t];
 				uint64_t bk = 0;
@@ -675,17 +750,28 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 		}
 		if (s == last_s)
 			break;
-		// drop each sub-node's point; every sub-node above the last level holds one
-		if (wide) {
-			for (uint32_t t = warp; t < nsub; t += nwarps) {
-				const uint32_t ct = scnt[t], st = sstart[t];
-				const uint32_t ti = topi[t];
-				for (uint32_t i = st + lane; i < st + ct; i += 32)
-					if (i != ti) {
-						const uint32_t ni = i - t - (i > ti ? 1u : 0u);
-						kn[ni] = kc[i];
-						sn[ni] = sc[i];
-					}
+		// drop each sub-node's point; every sub-node above the last level holds one.
+		// Up to 64 sub-nodes the keys move independently (each finds its sub-node by
+		// a binary search of the starts); below that each thread moves a sub-node's
+		// few keys.
+		if (nsub <= 64) {
+			for (uint32_t i = threadIdx.x; i < present; i += ST_THREADS) {
+				// the sub-node holding i: the last one starting at or before i (an empty
+				// sub-node starts where the next one does, so this one is not empty)
+				uint32_t tl = 0, th = nsub;
+				while (th - tl > 1) {
+					const uint32_t mid = (tl + th) / 2;
+					if (sstart[mid] <= i)
+						tl = mid;
+					else
+						th = mid;
+				}
+				const uint32_t ti = topi[tl];
+				if (i != ti) {
+					const uint32_t ni = i - tl - (i > ti ? 1u : 0u);
+					kn[ni] = kc[i];
+					sn[ni] = sc[i];
+				}
 			}
 		} else {
 			for (uint32_t t = threadIdx.x; t < nsub; t += ST_THREADS) {
