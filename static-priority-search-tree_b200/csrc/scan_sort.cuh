@@ -210,8 +210,27 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_global_hist(const K *__restri
 	}
 }
 
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+	             "l"(src)
+	             : "memory");
+}
+
+__device__ __forceinline__ void cp_async4(void *dst, const void *src)
+{
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+	             "l"(src)
+	             : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // One pass.  vals_in == nullptr means the identity payload (the key's input index;
-// 32-bit payloads only).
+// 32-bit payloads only).  The tile's payloads are copied into shared memory
+// asynchronously as soon as the tile is known, so their reads overlap the ranking
+// and the look-back; each sorted key carries its input slot to find its payload.
 template <typename K, typename V>
 __global__ void __launch_bounds__(RS_THREADS, 3) k_rs_onesweep(const K *keys_in, const V *vals_in, K *keys_out,
                                                             V *vals_out, uint64_t n, int shift,
@@ -219,9 +238,10 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_rs_onesweep(const K *keys_in,
                                                             uint32_t *tile_counter, uint32_t epoch, uint32_t *err)
 {
 	extern __shared__ __align__(16) unsigned char rs_smem[];
-	V *sv = reinterpret_cast<V *>(rs_smem);
-	K *sk = reinterpret_cast<K *>(sv + RS_TILE);
-	uint32_t *whist = reinterpret_cast<uint32_t *>(sk + RS_TILE);  // [RS_WARPS][256]
+	V *sv = reinterpret_cast<V *>(rs_smem);                         // payloads, input order
+	K *sk = reinterpret_cast<K *>(sv + RS_TILE);                    // keys, sorted within the tile
+	uint16_t *si = reinterpret_cast<uint16_t *>(sk + RS_TILE);      // input slot of each sorted key
+	uint32_t *whist = reinterpret_cast<uint32_t *>(si + RS_TILE);   // [RS_WARPS][256]
 	uint32_t *dstart = whist + RS_WARPS * 256;                      // [256] tile-local digit start
 	uint32_t *gbase = dstart + 256;                                 // [256] global start of the digit for this tile
 	uint32_t *wsum = gbase + 256;                                   // [33]
@@ -237,6 +257,19 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_rs_onesweep(const K *keys_in,
 	__syncthreads();
 	const uint32_t tile = s_tile;
 	const uint64_t t0 = (uint64_t) tile * RS_TILE;
+	const uint64_t rem_n = n - t0;
+	const uint32_t tile_n = rem_n < (uint64_t) RS_TILE ? (uint32_t) rem_n : (uint32_t) RS_TILE;
+	if (vals_in) {
+		// 16-byte copies, then the (4-byte multiple) tail of a partial last tile
+		const unsigned char *src = reinterpret_cast<const unsigned char *>(vals_in + t0);
+		unsigned char *dst = reinterpret_cast<unsigned char *>(sv);
+		const uint32_t bytes = tile_n * (uint32_t) sizeof(V), body = bytes & ~15u;
+		for (uint32_t o = threadIdx.x * 16u; o < body; o += RS_THREADS * 16u)
+			cp_async16(dst + o, src + o);
+		for (uint32_t o = body + threadIdx.x * 4u; o < bytes; o += RS_THREADS * 4u)
+			cp_async4(dst + o, src + o);
+		cp_async_commit();
+	}
 	K k[RS_ITEMS];
 	uint32_t loc[RS_ITEMS];
 #pragma unroll
@@ -305,29 +338,29 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_rs_onesweep(const K *keys_in,
 		gbase[d] = hb + (uint32_t) excl;
 	}
 	__syncthreads();
-	if (s_fail)
+	if (s_fail) {
+		cp_async_wait_all();  // no copy may still target this CTA's shared memory
 		return;
-	// payloads are read only now, so they hold no registers through the ranking
+	}
 #pragma unroll
 	for (int i = 0; i < RS_ITEMS; i++) {
-		const uint64_t idx = t0 + (uint64_t) warp * (RS_ITEMS * 32) + i * 32 + lane;
-		if (idx < n) {
+		const uint32_t local = (uint32_t) warp * (RS_ITEMS * 32) + i * 32 + lane;
+		if (t0 + local < n) {
 			const uint32_t d = rs_digit(k[i], shift);
 			const uint32_t lp = dstart[d] + whist[warp * 256 + d] + loc[i];
 			sk[lp] = k[i];
-			sv[lp] = vals_in ? vals_in[idx] : (V) idx;
+			si[lp] = (uint16_t) local;
 		}
 	}
+	cp_async_wait_all();
 	__syncthreads();
-	const uint64_t rem_n = n - t0;
-	const uint32_t tile_n = rem_n < (uint64_t) RS_TILE ? (uint32_t) rem_n : (uint32_t) RS_TILE;
 	for (uint32_t j = threadIdx.x; j < tile_n; j += RS_THREADS) {
 		const K key = sk[j];
 		const uint32_t d = rs_digit(key, shift);
 		const uint64_t g = (uint64_t) gbase[d] + (j - dstart[d]);
 		if (g < n) {
 			keys_out[g] = key;
-			vals_out[g] = sv[j];
+			vals_out[g] = vals_in ? sv[si[j]] : (V) (t0 + si[j]);
 		}
 	}
 }
@@ -335,7 +368,7 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_rs_onesweep(const K *keys_in,
 template <typename K, typename V>
 constexpr size_t rs_onesweep_smem()
 {
-	return RS_TILE * (sizeof(K) + sizeof(V)) + (RS_WARPS * 256 + 256 + 256 + 33) * 4;
+	return RS_TILE * (sizeof(K) + sizeof(V) + 2) + (RS_WARPS * 256 + 256 + 256 + 33) * 4;
 }
 
 inline uint64_t rs_num_tiles(uint64_t n) { return (n + RS_TILE - 1) / RS_TILE; }
