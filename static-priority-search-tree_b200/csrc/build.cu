@@ -82,13 +82,13 @@ TreeLayout tree_layout(pst_dtype dt, pst_idtype it, uint64_t n)
 // Subtree builder capacity: nodes of at most ST_CAP points are finished by one CTA
 // (a power of two; PST_SUBTREE_CAP overrides it at build time).
 #ifndef PST_SUBTREE_CAP
-#define PST_SUBTREE_CAP 2048
+#define PST_SUBTREE_CAP 512
 #endif
 constexpr uint32_t ST_CAP = PST_SUBTREE_CAP;
 constexpr int ST_THREADS = 256;
 // Arg-max tiles: every segment of a level before the subtree level spans at least
 // ST_CAP >= TM_TILE positions, so a tile is cut by at most one segment boundary.
-constexpr uint32_t TM_TILE = 512;
+constexpr uint32_t TM_TILE = ST_CAP < 512 ? ST_CAP : 512;
 constexpr int AM_THREADS = 256;
 static_assert(ST_CAP >= TM_TILE, "tile/segment invariant");
 static_assert(TM_TILE % 32 == 0, "tiles are whole bitmap words");
@@ -508,7 +508,7 @@ struct SubtreeSmem {
 
 // Chunks of ST_THREADS positions the key gather reads: a node's range holds its
 // cN <= ST_CAP free points and at most one point taken by each ancestor (< 32).
-constexpr int ST_GATHER = ST_CAP / ST_THREADS + 1;
+constexpr int ST_GATHER = (ST_CAP + ST_THREADS - 1) / ST_THREADS + 1;
 
 // Count and start of every sub-node of the current sub-level (in that sub-level's
 // compacted key order) are kept in shared memory and derived level to level
@@ -610,7 +610,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 	}
 	// ... and their points, every read of the CTA in flight at once
 	{
-		constexpr int PER = ST_CAP / ST_THREADS;
+		constexpr int PER = (ST_CAP + ST_THREADS - 1) / ST_THREADS;
 		Pt tmp[PER];
 #pragma unroll
 		for (int u = 0; u < PER; u++) {
@@ -786,7 +786,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 			}
 		}
 		// spans of the next sub-level, in place: parents to registers, then children
-		constexpr int PMAX = ST_CAP / 2 / ST_THREADS;
+		constexpr int PMAX = (ST_CAP / 2 + ST_THREADS - 1) / ST_THREADS;
 		uint32_t pc[PMAX], ps[PMAX];
 #pragma unroll
 		for (int u = 0; u < PMAX; u++) {
