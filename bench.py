@@ -199,10 +199,46 @@ def gen_points_typed(n, seed, dt, has_id, torch):
     return rec
 
 
+def ips_scan(pst, torch, pts, n, dt, has_id, reps=5):
+    """Interval parallel search (the full-scan comparator) over n device points for a
+    stabbing value in the middle of the dim1 domain: ms per call (device time between
+    CUDA events, each call returning its count), hits, and GB/s of points read plus
+    records written."""
+    import ctypes as C
+    lib = pst.lib()
+    vs = 8 if dt == "f64" else 4
+    v = (1 << 23) if dt == "i32" else float(1 << 23)
+    ret = 0 if has_id else 1
+    rec_bytes = 4 if has_id else 2 * vs
+    cap = max(n // 16, 1)
+    buf = torch.empty(cap * rec_bytes, dtype=torch.uint8, device="cuda")
+    cnt = C.c_uint64()
+
+    def call():
+        pst.pst._check(lib.pst_ips_search_into(pst.pst.DTYPE[dt], 1 if has_id else 0, C.c_void_p(pts.data_ptr()), n,
+                                               pst.pst.value_arg(dt, v), ret, C.c_void_p(buf.data_ptr()), cap,
+                                               C.byref(cnt), None))
+        return cnt.value
+    for _ in range(2):
+        call()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    ev[0].record()
+    for _ in range(reps):
+        k = call()
+    ev[1].record()
+    ev[1].synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / reps
+    pt_bytes = pts.element_size() * pts.numel() // n
+    return {"dtype": dt, "ids": has_id, "n": n, "v": v, "hits": k, "ms": ms,
+            "gbs": (n * pt_bytes + k * rec_bytes) / (ms / 1000) / 1e9, "bytes_per_point": pt_bytes}
+
+
 def sweep(pst, torch, n, seed=1):
     """Per value type: build, then for each kind and selectivity a batch of 32 queries
-    calibrated to s * n points each: batched pass time and one plain query."""
-    out = []
+    calibrated to s * n points each: batched pass time and one plain query; and one
+    interval parallel search over the same points (returned as the "ips" rows)."""
+    out, ips_rows = [], []
     rng = np.random.default_rng(seed)
     for dt, has_id in SWEEP_TYPES:
         vs = 8 if dt == "f64" else 4
@@ -212,6 +248,9 @@ def sweep(pst, torch, n, seed=1):
         tree = pst.StaticPSTGPU(pts, n, dt, has_id)
         torch.cuda.synchronize()
         build_ms = 1000 * (time.perf_counter() - t0)
+        r = ips_scan(pst, torch, pts, n, dt, has_id)
+        ips_rows.append(r)
+        log(f"ips {dt}{'' if has_id else '-noid'}: {r['hits']} hits, {r['ms']:.3f} ms = {r['gbs']:.0f} GB/s")
         del pts
         torch.cuda.empty_cache()
         ret = "ids" if has_id else "points"
@@ -269,7 +308,7 @@ def sweep(pst, torch, n, seed=1):
         eng.close()
         tree.close()
         torch.cuda.empty_cache()
-    return out
+    return out, ips_rows
 
 
 # ---------------------------------------------------------------------------
@@ -702,7 +741,7 @@ def main():
         eng.close()
         tree.close()
         torch.cuda.empty_cache()
-        sweep_rows = sweep(pst, torch, n)
+        sweep_rows, ips_rows = sweep(pst, torch, n)
         tree = pst.StaticPSTGPU(gen_points_device(n, seed=1 + rank, torch=torch), n, "f32", True)
         eng = pst.BatchEngine(tree, max_queries=NQ)
 
@@ -753,6 +792,7 @@ def main():
                 "serving": serving}
         if sweep_rows is not None:
             line["sweep"] = sweep_rows
+            line["ips"] = ips_rows
         if iso_res is not None:
             line["isosurface"] = iso_res
         levels = tree.info()["levels"]

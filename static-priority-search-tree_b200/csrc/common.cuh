@@ -181,6 +181,31 @@ __device__ __forceinline__ uint64_t warp_run_sum(uint32_t key, uint64_t v, bool 
 	return v;
 }
 
+// Asynchronous global -> shared copies (cp.async): 16 or 4 bytes per thread, in
+// commit groups; wait_group<N> waits until at most N of this thread's groups are
+// still in flight.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+	             "l"(src)
+	             : "memory");
+}
+
+__device__ __forceinline__ void cp_async4(void *dst, const void *src)
+{
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+	             "l"(src)
+	             : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group()
+{
+	asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Per-stream device facts used for grid sizing.
 struct DeviceInfo {
 	int device;

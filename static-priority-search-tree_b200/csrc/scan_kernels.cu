@@ -20,31 +20,88 @@ constexpr int IPS_PER_LANE = 8;
 constexpr uint64_t IPS_WARP_SPAN = 32 * IPS_PER_LANE;
 constexpr uint64_t IPS_TILE = IPS_WARP_SPAN * (IPS_THREADS / 32);
 
+// Records of 4-byte values (8 or 12 bytes) would take two or three 4-byte loads per
+// lane; a whole, 16-byte aligned warp span is instead copied with 16-byte cp.async
+// into shared memory (two buffers per warp: the next tile's span is in flight while
+// the current one is tested and written) and the lanes pick their records there.
+template <typename Pt>
+constexpr bool ips_staged() { return sizeof(Pt) <= 12 && (IPS_WARP_SPAN * sizeof(Pt)) % (16 * 32) == 0; }
+
+// 16-byte copies per lane of one staged warp span, and the dynamic shared memory of
+// k_ips (two spans per warp).
+template <typename Pt>
+constexpr int ips_vec() { return ips_staged<Pt>() ? (int) (IPS_WARP_SPAN * sizeof(Pt) / 16 / 32) : 0; }
+template <typename Pt>
+constexpr size_t ips_smem() { return (size_t) 2 * (IPS_THREADS / 32) * ips_vec<Pt>() * 32 * 16; }
+
 template <typename T, bool HAS_ID, bool POINTS>
 __global__ void __launch_bounds__(IPS_THREADS) k_ips(const Point<T, HAS_ID> *__restrict__ pts, uint64_t n, T v,
-                                                    void *out, uint64_t capacity, unsigned long long *counter)
+                                                    void *out, uint64_t capacity, unsigned long long *counter,
+                                                    bool aligned16)
 {
 	using Pt = Point<T, HAS_ID>;
+	constexpr bool STAGED = ips_staged<Pt>();
+	constexpr int VEC = ips_vec<Pt>();
+	extern __shared__ __align__(16) uint4 s_span[];  // [2][IPS_THREADS / 32][VEC * 32] when STAGED
 	__shared__ uint32_t s_warp[IPS_THREADS / 32 + 1];
 	__shared__ unsigned long long s_base;
 	const int warp = threadIdx.x >> 5;
 	const uint32_t lane = lane_id();
 	const uint64_t tiles = (n + IPS_TILE - 1) / IPS_TILE;
+	const bool staging = STAGED && aligned16;
+	// a tile's span of this warp can be staged when it is whole
+	auto whole = [&](uint64_t tl) { return tl < tiles && tl * IPS_TILE + (warp + 1) * IPS_WARP_SPAN <= n; };
+	auto issue = [&](uint64_t tl, int b) {
+		const uint4 *src = reinterpret_cast<const uint4 *>(pts + tl * IPS_TILE + warp * IPS_WARP_SPAN);
+		uint4 *dst = s_span + ((size_t) b * (IPS_THREADS / 32) + warp) * (VEC * 32);
+#pragma unroll
+		for (int j = 0; j < VEC; j++)
+			cp_async16(dst + j * 32 + lane, src + j * 32 + lane);
+	};
+	int cur = 0;
+	bool staged_cur = false;
+	if (staging) {
+		staged_cur = whole(blockIdx.x);
+		if (staged_cur)
+			issue(blockIdx.x, 0);
+		cp_async_commit();
+	}
 	for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
 		const uint64_t wbase = tile * IPS_TILE + warp * IPS_WARP_SPAN;
 		uint32_t hit[IPS_PER_LANE];
 		Pt rec[IPS_PER_LANE];
 		uint32_t wcount = 0;
+		bool staged_next = false;
+		if (staging) {
+			staged_next = whole(tile + gridDim.x);
+			if (staged_next)
+				issue(tile + gridDim.x, cur ^ 1);
+			cp_async_commit();
+			cp_async_wait_group<1>();  // this tile's span has landed
+			__syncwarp();
+		}
+		if (staged_cur) {
+			const Pt *sp = reinterpret_cast<const Pt *>(s_span + ((size_t) cur * (IPS_THREADS / 32) + warp) * (VEC * 32));
 #pragma unroll
-		for (int k = 0; k < IPS_PER_LANE; k++) {
-			const uint64_t i = wbase + 32 * k + lane;
-			bool ok = false;
-			if (i < n) {
-				rec[k] = pts[i];
-				ok = rec[k].dim1 <= v && v <= rec[k].dim2;
+			for (int k = 0; k < IPS_PER_LANE; k++) {
+				rec[k] = sp[32 * k + lane];
+				const bool ok = rec[k].dim1 <= v && v <= rec[k].dim2;
+				hit[k] = __ballot_sync(0xFFFFFFFFu, ok);
+				wcount += __popc(hit[k]);
 			}
-			hit[k] = __ballot_sync(0xFFFFFFFFu, ok);
-			wcount += __popc(hit[k]);
+			__syncwarp();  // the buffer is refilled for the tile after next
+		} else {
+#pragma unroll
+			for (int k = 0; k < IPS_PER_LANE; k++) {
+				const uint64_t i = wbase + 32 * k + lane;
+				bool ok = false;
+				if (i < n) {
+					rec[k] = pts[i];
+					ok = rec[k].dim1 <= v && v <= rec[k].dim2;
+				}
+				hit[k] = __ballot_sync(0xFFFFFFFFu, ok);
+				wcount += __popc(hit[k]);
+			}
 		}
 		if (lane == 0)
 			s_warp[warp] = wcount;
@@ -74,7 +131,11 @@ __global__ void __launch_bounds__(IPS_THREADS) k_ips(const Point<T, HAS_ID> *__r
 			o += __popc(hit[k]);
 		}
 		__syncthreads();
+		staged_cur = staged_next;
+		cur ^= 1;
 	}
+	if (staging)
+		cp_async_wait_all();  // nothing may still target this CTA's shared memory
 }
 
 // ---------------------------------------------------------------------------
@@ -149,8 +210,12 @@ void ips_launch(const void *pts, uint64_t n, T v, void *out, uint64_t cap, unsig
 	const uint64_t tiles = (n + IPS_TILE - 1) / IPS_TILE;
 	uint64_t g = blocks ? blocks : std::min<uint64_t>(tiles, (uint64_t) device_info().sms * 8);
 	g = std::max<uint64_t>(g, 1);
-	k_ips<T, HAS_ID, POINTS><<<(unsigned) g, IPS_THREADS, 0, s>>>(static_cast<const Point<T, HAS_ID> *>(pts), n, v,
-	                                                               out, cap, counter);
+	const bool aligned16 = (reinterpret_cast<uintptr_t>(pts) & 15u) == 0;
+	constexpr size_t smem = ips_smem<Point<T, HAS_ID>>();
+	if (smem > 0)  // above the default 48 KB with the static part
+		PST_CUDA(cudaFuncSetAttribute(k_ips<T, HAS_ID, POINTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+	k_ips<T, HAS_ID, POINTS><<<(unsigned) g, IPS_THREADS, smem, s>>>(static_cast<const Point<T, HAS_ID> *>(pts), n, v,
+	                                                                  out, cap, counter, aligned16);
 	PST_CUDA(cudaGetLastError());
 }
 

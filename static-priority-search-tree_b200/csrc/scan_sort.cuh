@@ -210,23 +210,6 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_global_hist(const K *__restri
 	}
 }
 
-__device__ __forceinline__ void cp_async16(void *dst, const void *src)
-{
-	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
-	             "l"(src)
-	             : "memory");
-}
-
-__device__ __forceinline__ void cp_async4(void *dst, const void *src)
-{
-	asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
-	             "l"(src)
-	             : "memory");
-}
-
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
 // One pass.  vals_in == nullptr means the identity payload (the key's input index;
 // 32-bit payloads only).  The tile's payloads are copied into shared memory
 // asynchronously as soon as the tile is known, so their reads overlap the ranking
