@@ -203,6 +203,91 @@ __global__ void k_metacells(const T *__restrict__ vol, uint32_t px, uint32_t py,
 	}
 }
 
+// The common layout: metacells 4 vertices wide over 4-byte values, rows a multiple of
+// 4 vertices long, the volume 16-byte aligned.  A metacell's 4 low vertices of a row
+// are one aligned 16-byte load; its fifth (the next metacell's first) comes from the
+// next lane, or from memory for a warp's last metacell.  Same walk as k_metacells.
+template <typename T>
+struct Quad;
+template <>
+struct Quad<float> {
+	using V = float4;
+};
+template <>
+struct Quad<int32_t> {
+	using V = int4;
+};
+
+template <typename T, bool HAS_ID>
+__global__ void k_metacells4(const T *__restrict__ vol, uint32_t px, uint32_t py, uint32_t pz, uint32_t mcy,
+                             uint32_t mcz, uint32_t Mx, uint32_t My, uint32_t mz_begin, uint32_t mz_end,
+                             uint32_t z_base, uint32_t mz_per_cta, Point<T, HAS_ID> *__restrict__ out)
+{
+	using V = typename Quad<T>::V;
+	const uint32_t mx = blockIdx.x * blockDim.x + threadIdx.x;
+	const uint32_t lane = lane_id();
+	const bool active = mx < Mx;  // inactive lanes still take part in the shuffles
+	const uint32_t my = blockIdx.y;
+	const uint32_t mz0 = mz_begin + blockIdx.z * mz_per_cta;
+	const uint32_t mz1 = min(mz0 + mz_per_cta, mz_end);
+	const uint32_t x0 = 4 * mx;
+	const bool has5 = active && x0 + 4 <= px - 1;         // the metacell has a fifth vertex column
+	const bool from_next = lane < 31 && mx + 1 < Mx;     // ... and the next lane holds it
+	const uint32_t y0 = my * mcy, y1 = min(y0 + mcy, py - 1);
+	auto plane = [&](uint32_t z, T &lo, T &hi) {
+		const T *pl = vol + (uint64_t) (z - z_base) * py * px;
+		for (uint32_t y = y0; y <= y1; y++) {
+			const T *row = pl + (uint64_t) y * px;
+			const V a = active ? *reinterpret_cast<const V *>(row + x0) : V{};
+			const T nx = __shfl_down_sync(0xFFFFFFFFu, a.x, 1);
+			const T e = from_next ? nx : has5 ? row[x0 + 4] : a.x;
+			// folds in row-major order that keep the first of equal values (as
+			// k_metacells does), so -0.0 and +0.0 come out as they do there
+			const T r[5] = {a.x, a.y, a.z, a.w, e};
+			T l = r[0], h = r[0];
+#pragma unroll
+			for (int k = 1; k < 5; k++) {
+				l = r[k] < l ? r[k] : l;
+				h = r[k] > h ? r[k] : h;
+			}
+			if (y == y0) {
+				lo = l;
+				hi = h;
+			} else {
+				lo = l < lo ? l : lo;
+				hi = h > hi ? h : hi;
+			}
+		}
+	};
+	T plo = T(0), phi = T(0);  // the last plane reduced
+	uint32_t pz_done = 0xFFFFFFFFu;
+	for (uint32_t mz = mz0; mz < mz1; mz++) {
+		const uint32_t z0 = mz * mcz, z1 = min(z0 + mcz, pz - 1);
+		T lo, hi;
+		if (pz_done == z0) {
+			lo = plo;
+			hi = phi;
+		} else {
+			plane(z0, lo, hi);
+		}
+		for (uint32_t z = z0 + 1; z <= z1; z++) {
+			plane(z, plo, phi);
+			lo = plo < lo ? plo : lo;
+			hi = phi > hi ? phi : hi;
+			pz_done = z;
+		}
+		if (active) {
+			const uint64_t id = (uint64_t) mx + ((uint64_t) my + (uint64_t) mz * My) * Mx;
+			Point<T, HAS_ID> p;
+			p.dim1 = lo;
+			p.dim2 = hi;
+			if constexpr (HAS_ID)
+				p.id = (uint32_t) id;
+			out[id] = p;
+		}
+	}
+}
+
 template <typename T, bool HAS_ID, bool POINTS>
 void ips_launch(const void *pts, uint64_t n, T v, void *out, uint64_t cap, unsigned long long *counter,
                 uint32_t blocks, cudaStream_t s)
@@ -245,9 +330,19 @@ void metacell_launch(const void *vol, const uint32_t P[3], const uint32_t mc[3],
 	dim3 grid((M[0] + threads - 1) / threads, M[1], (mz_end - mz_begin + mzp - 1) / mzp);
 	if (grid.y > 65535 || grid.z > 65535)
 		fail(PST_ERR_INVALID, "metacell grid too large");
-	k_metacells<T, HAS_ID><<<grid, threads, 0, s>>>(static_cast<const T *>(vol), P[0], P[1], P[2], mc[0], mc[1], mc[2],
-	                                                M[0], M[1], mz_begin, mz_end, mz_begin * mc[2], mzp,
-	                                                static_cast<Point<T, HAS_ID> *>(out));
+	bool quad = false;
+	if constexpr (sizeof(T) == 4)
+		quad = mc[0] == 4 && P[0] % 4 == 0 && (reinterpret_cast<uintptr_t>(vol) & 15u) == 0;
+	if constexpr (sizeof(T) == 4) {
+		if (quad)
+			k_metacells4<T, HAS_ID><<<grid, threads, 0, s>>>(static_cast<const T *>(vol), P[0], P[1], P[2], mc[1], mc[2],
+			                                                 M[0], M[1], mz_begin, mz_end, mz_begin * mc[2], mzp,
+			                                                 static_cast<Point<T, HAS_ID> *>(out));
+	}
+	if (!quad)
+		k_metacells<T, HAS_ID><<<grid, threads, 0, s>>>(static_cast<const T *>(vol), P[0], P[1], P[2], mc[0], mc[1],
+		                                                mc[2], M[0], M[1], mz_begin, mz_end, mz_begin * mc[2], mzp,
+		                                                static_cast<Point<T, HAS_ID> *>(out));
 	PST_CUDA(cudaGetLastError());
 }
 

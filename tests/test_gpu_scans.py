@@ -52,3 +52,32 @@ def test_metacells(pst, oracle, dims, mc, dt):
     out2, _ = pst.formMetacellTags(vd, dims, mc, dt, False)
     rec2 = out2.cpu().numpy().view(pst.point_dtype(dt, False))
     assert rec2["dim1"].tobytes() == lo.tobytes() and rec2["dim2"].tobytes() == hi.tobytes()
+
+
+@pytest.mark.parametrize("dims,mc", [((64, 13, 9), (4, 4, 4)), ((36, 33, 17), (4, 4, 4)), ((4, 4, 4), (4, 4, 4)),
+                                     ((8, 5, 6), (4, 2, 3)), ((1028, 3, 3), (4, 4, 4)), ((16, 9, 2), (4, 4, 1))])
+@pytest.mark.parametrize("dt", ["f32", "i32", "f64"])
+@pytest.mark.parametrize("zeros", [False, True])
+def test_metacells_aligned_rows(pst, oracle, dims, mc, dt, zeros):
+    """Rows a multiple of 4 vertices long under 4-wide metacells (the layout whose rows
+    are read 16 bytes at a time for 4-byte values): ragged last metacells, rows wider
+    than one CTA, and (zeros) volumes of -0.0 / +0.0 / +-1 / 2, whose min and max
+    must keep the same zero as the CPU restatement, bit for bit."""
+    import torch
+    rng = np.random.default_rng(sum(dims) + 3)
+    px, py, pz = dims
+    npdt = {"f32": np.float32, "f64": np.float64, "i32": np.int32}[dt]
+    if zeros and dt != "i32":
+        vol = rng.choice(np.array([-0.0, 0.0, -1.0, 1.0, 2.0], npdt), (pz, py, px))
+    elif dt == "i32":
+        vol = rng.integers(-50, 50, (pz, py, px)).astype(np.int32)
+    else:
+        vol = rng.standard_normal((pz, py, px)).astype(npdt)
+    lo, hi, ids = oracle.Orc.metacells(vol, dt, dims, mc)
+    vd = torch.from_numpy(vol.reshape(-1).copy()).to("cuda")
+    out, n = pst.formMetacellTags(vd, dims, mc, dt, True)
+    rec = out.cpu().numpy().view(pst.point_dtype(dt, True))
+    assert n == len(lo)
+    assert rec["dim1"].tobytes() == lo.tobytes()
+    assert rec["dim2"].tobytes() == hi.tobytes()
+    assert np.array_equal(rec["id"], ids)
