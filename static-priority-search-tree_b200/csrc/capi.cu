@@ -539,22 +539,54 @@ pst_status pst_batch_last_stats(pst_batch *batch, pst_batch_stats *stats, uint32
 	});
 }
 
+// The result counter of an interval search: one device word and one pinned host
+// word per calling thread and device, made on first use and kept (a call waits for
+// its count before it returns, so a thread's calls never overlap).
+namespace {
+struct IpsCounter {
+	unsigned long long *dev = nullptr;
+	unsigned long long *host = nullptr;
+};
+struct IpsCounters {
+	IpsCounter c[64];
+	~IpsCounters()
+	{
+		for (IpsCounter &x : c) {
+			if (x.dev)
+				cudaFree(x.dev);
+			if (x.host)
+				cudaFreeHost(x.host);
+		}
+	}
+};
+thread_local IpsCounters t_ips_counters;
+
+IpsCounter &ips_counter()
+{
+	const int dev = device_info().device;
+	IpsCounter &x = t_ips_counters.c[dev];
+	if (!x.dev) {
+		check_cuda(cudaMalloc((void **) &x.dev, 8), "cudaMalloc(interval search counter)");
+		if (cudaMallocHost((void **) &x.host, 8) != cudaSuccess) {
+			cudaGetLastError();
+			cudaFree(x.dev);
+			x.dev = nullptr;
+			fail(PST_ERR_NOMEM, "pinned interval search counter");
+		}
+	}
+	return x;
+}
+}  // namespace
+
 static uint64_t ips_common(pst_dtype dtype, pst_idtype idtype, const void *pts_d, uint64_t n, pst_value v, pst_ret ret,
                            void *out, uint64_t cap, uint32_t blocks, cudaStream_t s)
 {
-	unsigned long long *ctr = nullptr;
-	check_cuda(cudaMallocAsync((void **) &ctr, 8, s), "cudaMallocAsync");
-	struct F {
-		unsigned long long *p;
-		cudaStream_t s;
-		~F() { cudaFreeAsync(p, s); }
-	} f{ctr, s};
-	check_cuda(cudaMemsetAsync(ctr, 0, 8, s), "memset");
-	ips_run(dtype, idtype, ret, pts_d, n, v, out, cap, ctr, blocks, s);
-	unsigned long long c = 0;
-	check_cuda(cudaMemcpyAsync(&c, ctr, 8, cudaMemcpyDeviceToHost, s), "copy count");
+	IpsCounter &ctr = ips_counter();
+	check_cuda(cudaMemsetAsync(ctr.dev, 0, 8, s), "memset");
+	ips_run(dtype, idtype, ret, pts_d, n, v, out, cap, ctr.dev, blocks, s);
+	check_cuda(cudaMemcpyAsync(ctr.host, ctr.dev, 8, cudaMemcpyDeviceToHost, s), "copy count");
 	check_cuda(cudaStreamSynchronize(s), "sync");
-	return c;
+	return *ctr.host;
 }
 
 pst_status pst_ips_search(pst_dtype dtype, pst_idtype idtype, const void *pts_d, uint64_t n, pst_value v, pst_ret ret,

@@ -1,5 +1,6 @@
 // Streaming kernels: the interval parallel search comparator and metacell formation.
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "scan_kernels.cuh"
@@ -297,8 +298,18 @@ void ips_launch(const void *pts, uint64_t n, T v, void *out, uint64_t cap, unsig
 	g = std::max<uint64_t>(g, 1);
 	const bool aligned16 = (reinterpret_cast<uintptr_t>(pts) & 15u) == 0;
 	constexpr size_t smem = ips_smem<Point<T, HAS_ID>>();
-	if (smem > 0)  // above the default 48 KB with the static part
-		PST_CUDA(cudaFuncSetAttribute(k_ips<T, HAS_ID, POINTS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+	if (smem > 0) {
+		// above the default 48 KB with the static part: opt in once per device
+		static std::mutex mu;
+		static bool done[64] = {};
+		const int dev = device_info().device;
+		std::lock_guard<std::mutex> lk(mu);
+		if (dev >= 0 && dev < 64 && !done[dev]) {
+			PST_CUDA(cudaFuncSetAttribute(k_ips<T, HAS_ID, POINTS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			                              (int) smem));
+			done[dev] = true;
+		}
+	}
 	k_ips<T, HAS_ID, POINTS><<<(unsigned) g, IPS_THREADS, smem, s>>>(static_cast<const Point<T, HAS_ID> *>(pts), n, v,
 	                                                                  out, cap, counter, aligned16);
 	PST_CUDA(cudaGetLastError());
