@@ -24,7 +24,8 @@
 //
 // Kernels (k_mc_cells): one warp per metacell, 32 cells at a time; the count pass
 // sums each metacell's triangles, an exclusive scan gives offsets, the emit pass
-// writes each cell's triangles at its warp-scanned position, so the output is
+// computes each cell's triangles at its warp-scanned position in a per-warp shared
+// stage and writes the 32 cells' triangles out as one contiguous run, so the output is
 // ordered by metacell (as given), then cell (x fastest), then table order.
 #include <algorithm>
 #include <cstring>
@@ -245,13 +246,19 @@ struct McGrid {
 	uint32_t px, py, pz, mcx, mcy, mcz, Mx, My;
 };
 
+constexpr int MC_THREADS = 128;
+// Triangles a warp stages per 32 cells (at most MC_MAX_TRI each), 9 floats each.
+constexpr int MC_STAGE_FLOATS = 32 * MC_MAX_TRI * 9;
+
 template <bool EMIT>
-__global__ void __launch_bounds__(256) k_mc_cells(const float *__restrict__ vol, McGrid g,
+__global__ void __launch_bounds__(MC_THREADS) k_mc_cells(const float *__restrict__ vol, McGrid g,
                                                   const uint32_t *__restrict__ ids, uint64_t n, float iso,
                                                   uint64_t *__restrict__ counts, const uint64_t *__restrict__ offsets,
                                                   float *__restrict__ tri, uint64_t capacity)
 {
 	__shared__ McTables s_t;
+	// the warp's triangles of 32 cells, in output order, written out together
+	__shared__ float s_tri[EMIT ? MC_THREADS / 32 : 1][EMIT ? MC_STAGE_FLOATS : 1];
 	for (int i = threadIdx.x; i < (int) sizeof(McTables) / 4; i += blockDim.x)
 		reinterpret_cast<uint32_t *>(&s_t)[i] = reinterpret_cast<const uint32_t *>(&c_mc)[i];
 	__syncthreads();
@@ -289,12 +296,10 @@ __global__ void __launch_bounds__(256) k_mc_cells(const float *__restrict__ vol,
 				total += nt;
 			} else {
 				const uint32_t inc = warp_incl_scan(nt);
-				const uint64_t o = base + inc - nt;
-				base += __shfl_sync(0xFFFFFFFFu, inc, 31);
+				const uint32_t tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
+				float *stage = s_tri[threadIdx.x >> 5];
 				for (uint32_t k = 0; k < nt; k++) {
-					if (o + k >= capacity)
-						break;
-					float *dst = tri + (o + k) * 9;
+					float *dst = stage + (inc - nt + k) * 9;
 #pragma unroll
 					for (int v = 0; v < 3; v++) {
 						const uint32_t e = s_t.edges[cfg][3 * k + v];
@@ -309,6 +314,16 @@ __global__ void __launch_bounds__(256) k_mc_cells(const float *__restrict__ vol,
 						dst[3 * v + 2] = pos[2];
 					}
 				}
+				__syncwarp();
+				// the 32 cells' triangles are one contiguous range: consecutive lanes
+				// write consecutive floats
+				const uint64_t nf = (uint64_t) tot * 9;
+				const uint64_t room = base < capacity ? (capacity - base) * 9 : 0;
+				float *out = tri + base * 9;
+				for (uint32_t j = lane; j < nf && j < room; j += 32)
+					out[j] = stage[j];
+				__syncwarp();  // the stage is refilled by the next 32 cells
+				base += tot;
 			}
 		}
 		if constexpr (!EMIT) {
@@ -337,8 +352,8 @@ McGrid make_grid(const uint32_t P[3], const uint32_t mc[3])
 
 unsigned mc_grid_blocks(uint64_t n)
 {
-	const uint64_t want = (n + 7) / 8;  // 8 warps per block, one metacell each
-	return (unsigned) std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t) device_info().sms * 8));
+	const uint64_t want = (n + MC_THREADS / 32 - 1) / (MC_THREADS / 32);  // one metacell per warp
+	return (unsigned) std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t) device_info().sms * 16));
 }
 
 }  // namespace
@@ -377,7 +392,7 @@ uint64_t mc_run(const float *vol, const uint32_t P[3], const uint32_t mc[3], con
 	total_d = reinterpret_cast<uint64_t *>(buf + (n + 1) * 8 + tmp);
 	counts = reinterpret_cast<uint64_t *>(buf + (n + 1) * 8 + tmp + 64);
 	const unsigned blocks = mc_grid_blocks(n);
-	k_mc_cells<false><<<blocks, 256, 0, s>>>(vol, g, ids, n, iso, counts, nullptr, nullptr, 0);
+	k_mc_cells<false><<<blocks, MC_THREADS, 0, s>>>(vol, g, ids, n, iso, counts, nullptr, nullptr, 0);
 	PST_CUDA(cudaGetLastError());
 	exclusive_scan<uint64_t>(counts, offsets, n, scan, total_d, s);
 	uint64_t total = 0;
@@ -387,7 +402,7 @@ uint64_t mc_run(const float *vol, const uint32_t P[3], const uint32_t mc[3], con
 		return total;
 	if (!tri)
 		fail(PST_ERR_INVALID, "null triangle buffer");
-	k_mc_cells<true><<<blocks, 256, 0, s>>>(vol, g, ids, n, iso, nullptr, offsets, tri, capacity);
+	k_mc_cells<true><<<blocks, MC_THREADS, 0, s>>>(vol, g, ids, n, iso, nullptr, offsets, tri, capacity);
 	PST_CUDA(cudaGetLastError());
 	PST_CUDA(cudaStreamSynchronize(s));
 	return total;
