@@ -81,3 +81,41 @@ def test_metacells_aligned_rows(pst, oracle, dims, mc, dt, zeros):
     assert rec["dim1"].tobytes() == lo.tobytes()
     assert rec["dim2"].tobytes() == hi.tobytes()
     assert np.array_equal(rec["id"], ids)
+
+
+@pytest.mark.parametrize("dt", ["f32", "i32", "f64"])
+def test_ips_unaligned_points(pst, oracle, dt):
+    """A point array that starts one record into its allocation (not on a 16-byte
+    boundary) is scanned without the 16-byte staging; the results are the same."""
+    pts = rand_points(50001, dt, ids="arange", dup=(dt == "i32"), seed=9)
+    d = pst.points_to_device(pts)
+    sub = pts[1:]
+    dv = d[pts.dtype.itemsize:]
+    for v in [sub["dim1"][3], sub["dim2"][100], sub["dim1"][-1]]:
+        idx = oracle.Orc.ips(sub, dt, v)
+        got = pst.intervalParallelSearch(dv, len(sub), v, dt, True, ret="ids")
+        assert np.array_equal(np.sort(got), np.sort(sub["id"][idx]))
+        gotp = pst.intervalParallelSearch(dv, len(sub), v, dt, True, ret="points")
+        assert np.array_equal(oracle.canon(gotp), oracle.canon(sub[idx]))
+
+
+@pytest.mark.parametrize("dt", ["f32", "i32"])
+def test_metacells_unaligned_volume(pst, oracle, dt):
+    """A volume that starts one value into its allocation (not on a 16-byte
+    boundary) is reduced without the 16-byte row loads; the records are the same."""
+    import torch
+    dims, mc = (64, 9, 7), (4, 4, 4)
+    rng = np.random.default_rng(77)
+    px, py, pz = dims
+    if dt == "i32":
+        vol = rng.integers(-99, 99, (pz, py, px)).astype(np.int32)
+    else:
+        vol = rng.standard_normal((pz, py, px)).astype(np.float32)
+    lo, hi, ids = oracle.Orc.metacells(vol, dt, dims, mc)
+    big = np.concatenate([np.zeros(1, vol.dtype), vol.reshape(-1)])
+    vd = torch.from_numpy(big).to("cuda")[1:]
+    out, n = pst.formMetacellTags(vd, dims, mc, dt, True)
+    rec = out.cpu().numpy().view(pst.point_dtype(dt, True))
+    assert n == len(lo)
+    assert rec["dim1"].tobytes() == lo.tobytes() and rec["dim2"].tobytes() == hi.tobytes()
+    assert np.array_equal(rec["id"], ids)
