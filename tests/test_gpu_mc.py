@@ -25,6 +25,7 @@ def _grid(dims, mcd):
     ((18, 14, 10), (4, 4, 4), 0.3),   # ragged last metacells
     ((9, 10, 12), (2, 3, 5), 0.7),
     ((8, 8, 8), (1, 1, 1), 0.5),      # one cell per metacell
+    ((21, 14, 13), (8, 4, 4), 0.4),   # metacells of more vertices than a warp holds in registers
 ])
 def test_random_volume_equals_cpu(pst, dims, mcd, iso):
     import torch
