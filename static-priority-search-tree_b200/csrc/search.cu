@@ -361,6 +361,10 @@ __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__r
 template <typename T, bool LAST>
 __global__ void __launch_bounds__(BFS_THREADS, 4) k_bfs_level(TreeDev<T> t, QDev<T> qd, WorkDev w, uint32_t d)
 {
+	// Launched as a programmatic dependent of the previous level: its CTAs may be
+	// scheduled while that level drains, and wait here until it has completed and
+	// its writes are visible (a no-op for an ordinary launch).
+	asm volatile("griddepcontrol.wait;" ::: "memory");
 	// Once the frontier has overflowed, the reservation that crossed the capacity
 	// left some slots below it unwritten, so nothing of the previous level may be
 	// read: the pass stops here and the host repeats it with a larger buffer.
@@ -662,10 +666,22 @@ template <typename T>
 void launch_level(const TreeDev<T> &tv, const QDev<T> &qd, const WorkDev &w, uint32_t d, unsigned grid,
                   unsigned threads, cudaStream_t s)
 {
+	// programmatic dependent launch: the level's CTAs start as the previous kernel
+	// drains (the kernel waits for it before reading anything)
+	cudaLaunchConfig_t cfg{};
+	cfg.gridDim = dim3(grid);
+	cfg.blockDim = dim3(threads);
+	cfg.dynamicSmemBytes = 0;
+	cfg.stream = s;
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	attr[0].val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
 	if (d + 1 == tv.levels && tv.last_par)
-		k_bfs_level<T, true><<<grid, threads, 0, s>>>(tv, qd, w, d);
+		PST_CUDA(cudaLaunchKernelEx(&cfg, k_bfs_level<T, true>, tv, qd, w, d));
 	else
-		k_bfs_level<T, false><<<grid, threads, 0, s>>>(tv, qd, w, d);
+		PST_CUDA(cudaLaunchKernelEx(&cfg, k_bfs_level<T, false>, tv, qd, w, d));
 }
 
 template <typename T>
