@@ -132,8 +132,9 @@ pst_status pst_info(const pst_tree *tree, uint64_t *n, uint32_t *levels, uint64_
 pst_status pst_export(const pst_tree *tree, void *dim1, void *dim2, void *med, uint32_t *ids,
                       uint8_t *bitcodes);
 
-/* One query, drop-in mode: allocates the result with cudaMalloc (exactly *count
- * records; the caller frees it with cudaFree), blocks until the result is
+/* One query, drop-in mode: allocates the result (exactly *count records, from the
+ * library's stream-ordered result pool; the caller frees it with cudaFree, which
+ * accepts pool memory without synchronising), blocks until the result is
  * complete, and sets *out_d = NULL, *count = 0 for an empty tree or an empty
  * result.  Replaces StaticPSTGPU::threeSidedSearch / twoSidedLeftSearch /
  * twoSidedRightSearch (pst/static-pst-gpu.h:103-128, pst/static-pst-gpu.tu:496-642)
@@ -277,8 +278,9 @@ pst_status pst_server_destroy(pst_server *srv);
 
 /* ------------------------------------------------------------------------- */
 /* Interval parallel search: every point with dim1 <= v <= dim2, by a full scan.
- * Drop-in mode: like the reference, the result buffer is cudaMalloc'd with room
- * for all n points (the caller frees it) and *count records are valid; it is
+ * Drop-in mode: like the reference, the result buffer has room for all n points
+ * (allocated from the library's result pool; the caller frees it with cudaFree)
+ * and *count records are valid; it is
  * NULL for n == 0.  Blocks until complete.
  * Replaces intervalParallelSearch (interval-parallel-search/interval-parallel-search.h:29-66);
  * num_blocks is a launch hint (0 = automatic), threads_per_block is ignored. */

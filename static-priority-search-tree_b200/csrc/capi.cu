@@ -3,6 +3,7 @@
 #include <cstdio>
 #include <functional>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 
@@ -102,12 +103,44 @@ static pst_status guarded(F &&f)
 
 pst_status guarded_call(const std::function<void()> &f) { return guarded(f); }
 
-static void malloc_result(void **out, uint64_t bytes)
+// Results handed to the caller (the drop-in searches' cudaMalloc'd arrays) come
+// from a stream-ordered pool per device that keeps up to RESULT_POOL_KEEP bytes of
+// freed memory for reuse, instead of a cudaMalloc per call (which, with the
+// caller's cudaFree, costs more than the search itself).  The caller still frees a
+// result with cudaFree, which accepts pool memory and does not synchronise for it:
+// the call has waited for every write to the result before returning.
+constexpr uint64_t RESULT_POOL_KEEP = 1ull << 30;
+
+static cudaMemPool_t result_pool()
 {
-	cudaError_t e = cudaMalloc(out, bytes);
+	static std::mutex mu;
+	static cudaMemPool_t pools[64] = {};
+	const int dev = device_info().device;
+	std::lock_guard<std::mutex> lk(mu);
+	if (!pools[dev]) {
+		cudaMemPoolProps p{};
+		p.allocType = cudaMemAllocationTypePinned;
+		p.location.type = cudaMemLocationTypeDevice;
+		p.location.id = dev;
+		cudaMemPool_t pool = nullptr;
+		check_cuda(cudaMemPoolCreate(&pool, &p), "cudaMemPoolCreate(results)");
+		uint64_t keep = RESULT_POOL_KEEP;
+		check_cuda(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
+		pools[dev] = pool;
+	}
+	return pools[dev];
+}
+
+static void malloc_result(void **out, uint64_t bytes, cudaStream_t s)
+{
+	cudaError_t e = cudaMallocFromPoolAsync(out, bytes, result_pool(), s);
 	if (e != cudaSuccess) {
 		*out = nullptr;
-		check_cuda(e, "cudaMalloc(result)");
+		if (e == cudaErrorMemoryAllocation) {
+			cudaGetLastError();
+			fail(PST_ERR_NOMEM, "result allocation of " + std::to_string(bytes) + " B failed");
+		}
+		check_cuda(e, "cudaMallocFromPoolAsync(result)");
 	}
 }
 
@@ -153,7 +186,7 @@ static uint64_t run_single(pst_tree *tr, const pst_query *q, pst_ret ret, void *
 	if (total == 0)
 		return 0;
 	if (alloc) {
-		malloc_result(out_d, total * b.record_size(ret));
+		malloc_result(out_d, total * b.record_size(ret), s);
 	} else if (total > capacity) {
 		return total;
 	}
@@ -162,7 +195,7 @@ static uint64_t run_single(pst_tree *tr, const pst_query *q, pst_ret ret, void *
 	const pst_status st = b.read_ctl(s, &t2);
 	if (st != PST_OK) {
 		if (alloc) {
-			cudaFree(*out_d);
+			cudaFreeAsync(*out_d, s);  // after whatever the stream still holds
 			*out_d = nullptr;
 		}
 		fail(st, "search emit failed");
@@ -607,12 +640,12 @@ pst_status pst_ips_search(pst_dtype dtype, pst_idtype idtype, const void *pts_d,
 		require_device();
 		const uint64_t rs = ret == PST_RET_IDS ? 4 : point_size(dtype, idtype);
 		// The reference allocates room for every point (interval-parallel-search.h:35).
-		malloc_result(out_d, n * rs);
+		malloc_result(out_d, n * rs, reinterpret_cast<cudaStream_t>(stream));
 		try {
 			*count = ips_common(dtype, idtype, pts_d, n, v, ret, *out_d, n, num_blocks,
 			                    reinterpret_cast<cudaStream_t>(stream));
 		} catch (...) {
-			cudaFree(*out_d);
+			cudaFreeAsync(*out_d, reinterpret_cast<cudaStream_t>(stream));  // after the stream's work
 			*out_d = nullptr;
 			throw;
 		}
