@@ -356,39 +356,15 @@ __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__r
 	__syncwarp();  // the stage is reused by the warp's next batch
 }
 
-// LAST: the expansion into the last level of a tree with TreeDev::last_par (its own
-// instantiation, so the other levels keep their register budget).
+// One tree level of the search (the body of k_bfs_level): the boundary paths, the
+// seeds and the expansion of the previous level's records, spread over `gwarps`
+// warps (of the grid, or of the one CTA of k_bfs_cta).
 template <typename T, bool LAST>
-__global__ void __launch_bounds__(BFS_THREADS, 4) k_bfs_level(TreeDev<T> t, QDev<T> qd, WorkDev w, uint32_t d)
+__device__ __forceinline__ void level_body(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev &w, uint32_t d,
+                                           uint64_t gwarp, uint64_t gwarps, uint64_t base_prev, uint64_t base_cur,
+                                           uint64_t n_prev, WarpStage<T> &stage)
 {
-	// Launched as a programmatic dependent of the previous level: its CTAs may be
-	// scheduled while that level drains, and wait here until it has completed and
-	// its writes are visible (a no-op for an ordinary launch).
-	asm volatile("griddepcontrol.wait;" ::: "memory");
-	// Once the frontier has overflowed, the reservation that crossed the capacity
-	// left some slots below it unwritten, so nothing of the previous level may be
-	// read: the pass stops here and the host repeats it with a larger buffer.
-	if (w.ctl->flags & BATCH_FLAG_TASK_OVERFLOW)
-		return;
-	__shared__ uint64_t s_base[2];
-	__shared__ WarpStage<T> s_stage[BFS_THREADS / 32];
-	if (threadIdx.x == 0) {
-		uint64_t b = 0;  // start of the previous level's records
-		for (uint32_t e = 0; e + 1 < d; e++)
-			b += w.ctl->lvl_cnt[e];
-		s_base[0] = b;
-		s_base[1] = b + (d ? w.ctl->lvl_cnt[d - 1] : 0u);
-	}
-	__syncthreads();
-	const uint64_t base_prev = s_base[0], base_cur = s_base[1];
-	// after a frontier overflow the counters run past what was stored: never read beyond it
-	const uint64_t end_prev = min(base_cur, w.rec_cap);
-	const uint64_t n_prev = end_prev > base_prev ? end_prev - base_prev : 0;
-	const uint64_t gthreads = (uint64_t) gridDim.x * blockDim.x;
-	const uint64_t gtid = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
-	const uint64_t gwarps = gthreads / 32, gwarp = gtid / 32;
 	const uint32_t lane = lane_id();
-
 	// The level's three kinds of work go to disjoint sets of warps so that their
 	// dependent-load chains overlap instead of adding up: a few warps take the
 	// boundary paths, a few the seeds, the rest the records.
@@ -448,11 +424,94 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) k_bfs_level(TreeDev<T> t, QDev
 			const uint4 mine = valid ? w.rec[base_prev + wb + lane] : make_uint4(0, 0, 0, 0);
 			uint4 child[2];
 			uint32_t pts;
-			expand_records<T, LAST>(t, qd.min2, mine, valid, !LAST && d + 1 < t.levels, s_stage[threadIdx.x >> 5],
+			expand_records<T, LAST>(t, qd.min2, mine, valid, !LAST && d + 1 < t.levels, stage,
 			                        child, pts);
 			add_counts(w, mine.y, pts, valid);
 			append_blocks<2>(w, d, base_cur, child);
 		}
+	}
+}
+
+// LAST: the expansion into the last level of a tree with TreeDev::last_par (its own
+// instantiation, so the other levels keep their register budget).
+template <typename T, bool LAST>
+__global__ void __launch_bounds__(BFS_THREADS, 4) k_bfs_level(TreeDev<T> t, QDev<T> qd, WorkDev w, uint32_t d)
+{
+	// Launched as a programmatic dependent of the previous level: its CTAs may be
+	// scheduled while that level drains, and wait here until it has completed and
+	// its writes are visible (a no-op for an ordinary launch).
+	asm volatile("griddepcontrol.wait;" ::: "memory");
+	// Once the frontier has overflowed, the reservation that crossed the capacity
+	// left some slots below it unwritten, so nothing of the previous level may be
+	// read: the pass stops here and the host repeats it with a larger buffer.
+	if (w.ctl->flags & BATCH_FLAG_TASK_OVERFLOW)
+		return;
+	__shared__ uint64_t s_base[2];
+	__shared__ WarpStage<T> s_stage[BFS_THREADS / 32];
+	if (threadIdx.x == 0) {
+		uint64_t b = 0;  // start of the previous level's records
+		for (uint32_t e = 0; e + 1 < d; e++)
+			b += w.ctl->lvl_cnt[e];
+		s_base[0] = b;
+		s_base[1] = b + (d ? w.ctl->lvl_cnt[d - 1] : 0u);
+	}
+	__syncthreads();
+	const uint64_t base_prev = s_base[0], base_cur = s_base[1];
+	// after a frontier overflow the counters run past what was stored: never read beyond it
+	const uint64_t end_prev = min(base_cur, w.rec_cap);
+	const uint64_t n_prev = end_prev > base_prev ? end_prev - base_prev : 0;
+	const uint64_t gthreads = (uint64_t) gridDim.x * blockDim.x;
+	const uint64_t gtid = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
+	const uint64_t gwarps = gthreads / 32, gwarp = gtid / 32;
+	level_body<T, LAST>(t, qd, w, d, gwarp, gwarps, base_prev, base_cur, n_prev, s_stage[threadIdx.x >> 5]);
+}
+
+// Single queries: one CTA takes the tree from the top, level by level with a CTA
+// barrier in place of a kernel boundary, while the records to expand stay few
+// enough for it (at most CTA_REC_CAP); it leaves ctl->cta_levels = the levels done
+// and the host launches the per-level kernels for the rest only.  When it reaches
+// the bottom it also writes the query's offsets and total, so no scan is needed.
+constexpr uint32_t CTA_REC_CAP = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(BFS_THREADS) k_bfs_cta(TreeDev<T> t, QDev<T> qd, WorkDev w)
+{
+	__shared__ WarpStage<T> s_stage[BFS_THREADS / 32];
+	__shared__ uint64_t s_base[2];
+	__shared__ uint32_t s_go;
+	const uint64_t gwarps = BFS_THREADS / 32, gwarp = threadIdx.x >> 5;
+	uint64_t acc_prev = 0, acc = 0;  // (thread 0) start of the previous level's records, and of this level's
+	uint32_t d = 0;
+	for (; d < t.levels; d++) {
+		if (threadIdx.x == 0) {
+			const uint32_t prev = d ? w.ctl->lvl_cnt[d - 1] : 0u;
+			if (d) {
+				acc_prev = acc;
+				acc += prev;
+			}
+			s_base[0] = acc_prev;
+			s_base[1] = acc;
+			s_go = !(w.ctl->flags & BATCH_FLAG_TASK_OVERFLOW) && prev <= CTA_REC_CAP;
+		}
+		__syncthreads();
+		if (!s_go)
+			break;
+		const uint64_t base_prev = s_base[0], base_cur = s_base[1];
+		const uint64_t end_prev = min(base_cur, w.rec_cap);
+		const uint64_t n_prev = end_prev > base_prev ? end_prev - base_prev : 0;
+		if (d + 1 == t.levels && t.last_par)
+			level_body<T, true>(t, qd, w, d, gwarp, gwarps, base_prev, base_cur, n_prev, s_stage[gwarp]);
+		else
+			level_body<T, false>(t, qd, w, d, gwarp, gwarps, base_prev, base_cur, n_prev, s_stage[gwarp]);
+		__syncthreads();  // the level's records, paths and seeds are visible to the CTA
+		if (threadIdx.x == 0)
+			w.ctl->cta_levels = d + 1;
+	}
+	if (threadIdx.x == 0 && d == t.levels && !(w.ctl->flags & BATCH_FLAG_TASK_OVERFLOW)) {
+		const uint64_t c = w.counts[0];
+		const_cast<uint64_t *>(w.offsets)[0] = 0;
+		const_cast<uint64_t *>(w.offsets)[1] = c;
+		w.ctl->total = c;
 	}
 }
 
@@ -817,6 +876,35 @@ void Batch::enqueue_count(cudaStream_t s)
 	PST_CUDA(cudaGetLastError());
 }
 
+template <typename T>
+void Batch::enqueue_count_single_head(cudaStream_t s)
+{
+	TreeDev<T> tv = tree->view<T>();
+	QDev<T> qd{kind, static_cast<const T *>(min1), static_cast<const T *>(max1), static_cast<const T *>(min2)};
+	PST_WORKDEV;
+	PST_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
+	PST_CUDA(cudaMemsetAsync(counts, 0, (size_t) max_q * 8, s));
+	PST_CUDA(cudaMemsetAsync(cursor, 0, (size_t) max_q * 8, s));
+	k_check_kinds<<<1, 32, 0, s>>>(q_raw, ctl);
+	k_unpack_queries<T><<<1, 32, 0, s>>>(q_raw, ctl, kind, static_cast<T *>(min1), static_cast<T *>(max1),
+	                                     static_cast<T *>(min2), path0);
+	k_bfs_cta<T><<<1, BFS_THREADS, 0, s>>>(tv, qd, w);
+	PST_CUDA(cudaGetLastError());
+}
+
+template <typename T>
+void Batch::enqueue_count_single_tail(uint32_t from, cudaStream_t s)
+{
+	TreeDev<T> tv = tree->view<T>();
+	QDev<T> qd{kind, static_cast<const T *>(min1), static_cast<const T *>(max1), static_cast<const T *>(min2)};
+	PST_WORKDEV;
+	for (uint32_t d = from; d < tv.levels; d++)
+		launch_level<T>(tv, qd, w, d, grid, threads, s);
+	exclusive_scan<uint64_t>(counts, offsets, max_q, scan_tmp, &ctl->total, s);
+	PST_CUDA(cudaMemcpyAsync(offsets + max_q, &ctl->total, 8, cudaMemcpyDeviceToDevice, s));
+	PST_CUDA(cudaGetLastError());
+}
+
 template <typename T, bool HAS_ID, bool POINTS>
 void Batch::enqueue_emit_t(void *out, uint64_t capacity, cudaStream_t s)
 {
@@ -934,6 +1022,47 @@ void Batch::count_sync(cudaStream_t s, uint64_t *total)
 		BatchCtl h;
 		PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
 		PST_CUDA(cudaStreamSynchronize(s));
+		last = h;
+		if (h.flags & BATCH_FLAG_BAD_QUERY)
+			fail(PST_ERR_INVALID, "query kind must be PST_Q_THREE, PST_Q_LEFT or PST_Q_RIGHT");
+		if (h.flags & BATCH_FLAG_INTERNAL)
+			fail(PST_ERR_INTERNAL, "search consistency check failed");
+		if (!(h.flags & BATCH_FLAG_TASK_OVERFLOW)) {
+			*total = h.total;
+			return;
+		}
+		if (attempt > 8)
+			fail(PST_ERR_INTERNAL, "frontier did not fit after growth");
+		grow_tasks(std::max<uint64_t>(h.need_tasks + h.need_tasks / 4, task_cap * 2), s);
+	}
+}
+
+// Count pass of a single query (max_q == 1): the one-CTA top pass, then, if it
+// stopped above the bottom, the per-level kernels for the rest and the scan; with
+// automatic growth of the frontier buffer as in count_sync.
+void Batch::count_single_sync(cudaStream_t s, uint64_t *total)
+{
+	if (max_q != 1)
+		fail(PST_ERR_INTERNAL, "single-query count pass on a batch engine");
+	for (int attempt = 0;; attempt++) {
+		switch (tree->dtype) {
+		case PST_F32: enqueue_count_single_head<float>(s); break;
+		case PST_F64: enqueue_count_single_head<double>(s); break;
+		case PST_I32: enqueue_count_single_head<int32_t>(s); break;
+		}
+		BatchCtl h;
+		PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
+		PST_CUDA(cudaStreamSynchronize(s));
+		if (!(h.flags & (BATCH_FLAG_BAD_QUERY | BATCH_FLAG_INTERNAL | BATCH_FLAG_TASK_OVERFLOW)) &&
+		    h.cta_levels < tree->levels) {
+			switch (tree->dtype) {
+			case PST_F32: enqueue_count_single_tail<float>(h.cta_levels, s); break;
+			case PST_F64: enqueue_count_single_tail<double>(h.cta_levels, s); break;
+			case PST_I32: enqueue_count_single_tail<int32_t>(h.cta_levels, s); break;
+			}
+			PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
+			PST_CUDA(cudaStreamSynchronize(s));
+		}
 		last = h;
 		if (h.flags & BATCH_FLAG_BAD_QUERY)
 			fail(PST_ERR_INVALID, "query kind must be PST_Q_THREE, PST_Q_LEFT or PST_Q_RIGHT");

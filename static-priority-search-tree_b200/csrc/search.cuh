@@ -23,7 +23,7 @@ struct BatchCtl {
 	uint32_t rec_cnt;       // reported boundary nodes
 	uint32_t nq;
 	uint32_t flags;
-	uint32_t pad;
+	uint32_t cta_levels;    // levels already done by the one-CTA top pass (single queries)
 	uint64_t need_tasks;
 	uint64_t total;
 };
@@ -62,6 +62,7 @@ struct Batch {
 	void stage_queries(const pst_query *q, uint32_t nq, bool on_device, cudaStream_t s);
 	void launch_count(cudaStream_t s);
 	void count_sync(cudaStream_t s, uint64_t *total);
+	void count_single_sync(cudaStream_t s, uint64_t *total);
 	void enqueue_counting(cudaStream_t s);
 	void enqueue_emit(pst_ret ret, void *out, uint64_t capacity, cudaStream_t s);
 	pst_status read_ctl(cudaStream_t s, uint64_t *total);
@@ -70,6 +71,10 @@ struct Batch {
   private:
 	template <typename T>
 	void enqueue_count(cudaStream_t s);
+	template <typename T>
+	void enqueue_count_single_head(cudaStream_t s);
+	template <typename T>
+	void enqueue_count_single_tail(uint32_t from, cudaStream_t s);
 	template <typename T>
 	void enqueue_emit_v(pst_ret ret, void *out, uint64_t capacity, cudaStream_t s);
 	template <typename T, bool HAS_ID, bool POINTS>
