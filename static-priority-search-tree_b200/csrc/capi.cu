@@ -182,7 +182,7 @@ static uint64_t run_single(pst_tree *tr, const pst_query *q, pst_ret ret, void *
 	Batch &b = single_engine(tr);
 	b.stage_queries(q, 1, false, s);
 	uint64_t total = 0;
-	b.count_single_sync(s, &total);
+	b.count_sync(s, &total);
 	if (total == 0)
 		return 0;
 	if (alloc) {

@@ -466,18 +466,20 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) k_bfs_level(TreeDev<T> t, QDev
 	level_body<T, LAST>(t, qd, w, d, gwarp, gwarps, base_prev, base_cur, n_prev, s_stage[threadIdx.x >> 5]);
 }
 
-// Single queries: one CTA takes the tree from the top, level by level with a CTA
-// barrier in place of a kernel boundary, while the records to expand stay few
-// enough for it (at most CTA_REC_CAP); it leaves ctl->cta_levels = the levels done
-// and the host launches the per-level kernels for the rest only.  When it reaches
-// the bottom it also writes the query's offsets and total, so no scan is needed.
+// Small batches (a single query, or a few): one CTA takes the tree from the top,
+// level by level with a CTA barrier in place of a kernel boundary, while the
+// records to expand stay few enough for it (at most CTA_REC_CAP); it leaves
+// ctl->cta_levels = the levels done and the host launches the per-level kernels
+// for the rest only.  When it reaches the bottom it also scans the queries'
+// counts into offsets[0..max_q] and total, so no scan pass is needed.
 constexpr uint32_t CTA_REC_CAP = 256;
 
 template <typename T>
-__global__ void __launch_bounds__(BFS_THREADS) k_bfs_cta(TreeDev<T> t, QDev<T> qd, WorkDev w)
+__global__ void __launch_bounds__(BFS_THREADS) k_bfs_cta(TreeDev<T> t, QDev<T> qd, WorkDev w, uint32_t max_q)
 {
 	__shared__ WarpStage<T> s_stage[BFS_THREADS / 32];
 	__shared__ uint64_t s_base[2];
+	__shared__ uint64_t s_wsum[BFS_THREADS / 32];
 	__shared__ uint32_t s_go;
 	const uint64_t gwarps = BFS_THREADS / 32, gwarp = threadIdx.x >> 5;
 	uint64_t acc_prev = 0, acc = 0;  // (thread 0) start of the previous level's records, and of this level's
@@ -503,15 +505,41 @@ __global__ void __launch_bounds__(BFS_THREADS) k_bfs_cta(TreeDev<T> t, QDev<T> q
 			level_body<T, true>(t, qd, w, d, gwarp, gwarps, base_prev, base_cur, n_prev, s_stage[gwarp]);
 		else
 			level_body<T, false>(t, qd, w, d, gwarp, gwarps, base_prev, base_cur, n_prev, s_stage[gwarp]);
-		__syncthreads();  // the level's records, paths and seeds are visible to the CTA
+		__syncthreads();  // the level's records, paths, seeds and counts are visible to the CTA
 		if (threadIdx.x == 0)
 			w.ctl->cta_levels = d + 1;
 	}
-	if (threadIdx.x == 0 && d == t.levels && !(w.ctl->flags & BATCH_FLAG_TASK_OVERFLOW)) {
-		const uint64_t c = w.counts[0];
-		const_cast<uint64_t *>(w.offsets)[0] = 0;
-		const_cast<uint64_t *>(w.offsets)[1] = c;
-		w.ctl->total = c;
+	if (threadIdx.x == 0)
+		s_go = d == t.levels && !(w.ctl->flags & BATCH_FLAG_TASK_OVERFLOW);
+	__syncthreads();
+	if (!s_go)
+		return;
+	// exclusive scan of counts[0..max_q) in chunks of one count per thread
+	const uint32_t nq = w.ctl->nq, lane = lane_id();
+	uint64_t *offsets = const_cast<uint64_t *>(w.offsets);
+	uint64_t carry = 0;
+	for (uint32_t b = 0; b < max_q; b += BFS_THREADS) {
+		const uint32_t q = b + threadIdx.x;
+		const uint64_t c = q < nq ? w.counts[q] : 0;
+		const uint64_t inc = warp_incl_scan(c);
+		if (lane == 31)
+			s_wsum[gwarp] = inc;
+		__syncthreads();
+		if (gwarp == 0) {
+			uint64_t v = lane < BFS_THREADS / 32 ? s_wsum[lane] : 0;
+			v = warp_incl_scan(v);
+			if (lane < BFS_THREADS / 32)
+				s_wsum[lane] = v;
+		}
+		__syncthreads();
+		if (q < max_q)
+			offsets[q] = carry + (gwarp ? s_wsum[gwarp - 1] : 0) + inc - c;
+		carry += s_wsum[BFS_THREADS / 32 - 1];
+		__syncthreads();  // s_wsum is rewritten by the next chunk
+	}
+	if (threadIdx.x == 0) {
+		offsets[max_q] = carry;
+		w.ctl->total = carry;
 	}
 }
 
@@ -756,11 +784,17 @@ const void *bfs_kernel_ptr()
 
 Batch::~Batch() { release(); }
 
+void Batch::Graph::drop()
+{
+	if (exec)
+		cudaGraphExecDestroy(exec);
+	exec = nullptr;
+}
+
 void Batch::release()
 {
-	if (graph_exec)
-		cudaGraphExecDestroy(graph_exec);
-	graph_exec = nullptr;
+	full_graph.drop();
+	top_graph.drop();
 	for (void *p : {(void *) q_raw, (void *) kind, min1, max1, min2, (void *) path0, (void *) path1, (void *) seed0,
 	                (void *) seed1, (void *) ro, (void *) counts, (void *) cursor, (void *) offsets, (void *) scan_tmp,
 	                (void *) ctl, (void *) rec})
@@ -847,10 +881,9 @@ void Batch::grow_tasks(uint64_t cap, cudaStream_t s)
 	}
 	check_cuda(e, "cudaMallocAsync(frontier)");
 	task_cap = cap;
-	if (graph_exec) {
-		cudaGraphExecDestroy(graph_exec);
-		graph_exec = nullptr;
-	}
+	// the captured passes hold the old frontier's address
+	full_graph.drop();
+	top_graph.drop();
 }
 
 #define PST_WORKDEV                                                                                                   \
@@ -877,23 +910,24 @@ void Batch::enqueue_count(cudaStream_t s)
 }
 
 template <typename T>
-void Batch::enqueue_count_single_head(cudaStream_t s)
+void Batch::enqueue_count_top(cudaStream_t s)
 {
 	TreeDev<T> tv = tree->view<T>();
 	QDev<T> qd{kind, static_cast<const T *>(min1), static_cast<const T *>(max1), static_cast<const T *>(min2)};
 	PST_WORKDEV;
+	const unsigned qt = (unsigned) std::min<uint32_t>((max_q + 31) / 32 * 32, SMALL_BATCH_Q);
 	PST_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
 	PST_CUDA(cudaMemsetAsync(counts, 0, (size_t) max_q * 8, s));
 	PST_CUDA(cudaMemsetAsync(cursor, 0, (size_t) max_q * 8, s));
-	k_check_kinds<<<1, 32, 0, s>>>(q_raw, ctl);
-	k_unpack_queries<T><<<1, 32, 0, s>>>(q_raw, ctl, kind, static_cast<T *>(min1), static_cast<T *>(max1),
+	k_check_kinds<<<1, qt, 0, s>>>(q_raw, ctl);
+	k_unpack_queries<T><<<1, qt, 0, s>>>(q_raw, ctl, kind, static_cast<T *>(min1), static_cast<T *>(max1),
 	                                     static_cast<T *>(min2), path0);
-	k_bfs_cta<T><<<1, BFS_THREADS, 0, s>>>(tv, qd, w);
+	k_bfs_cta<T><<<1, BFS_THREADS, 0, s>>>(tv, qd, w, max_q);
 	PST_CUDA(cudaGetLastError());
 }
 
 template <typename T>
-void Batch::enqueue_count_single_tail(uint32_t from, cudaStream_t s)
+void Batch::enqueue_count_rest(uint32_t from, cudaStream_t s)
 {
 	TreeDev<T> tv = tree->view<T>();
 	QDev<T> qd{kind, static_cast<const T *>(min1), static_cast<const T *>(max1), static_cast<const T *>(min2)};
@@ -938,6 +972,15 @@ void Batch::enqueue_counting(cudaStream_t s)
 	}
 }
 
+void Batch::enqueue_counting_top(cudaStream_t s)
+{
+	switch (tree->dtype) {
+	case PST_F32: enqueue_count_top<float>(s); break;
+	case PST_F64: enqueue_count_top<double>(s); break;
+	case PST_I32: enqueue_count_top<int32_t>(s); break;
+	}
+}
+
 void Batch::enqueue_emit(pst_ret ret, void *out, uint64_t capacity, cudaStream_t s)
 {
 	switch (tree->dtype) {
@@ -947,34 +990,50 @@ void Batch::enqueue_emit(pst_ret ret, void *out, uint64_t capacity, cudaStream_t
 	}
 }
 
-void Batch::launch_count(cudaStream_t s)
+void Batch::launch_graph(Graph &g, void (Batch::*enqueue)(cudaStream_t), cudaStream_t s)
 {
 	if (!use_graph) {
-		enqueue_counting(s);
+		(this->*enqueue)(s);
 		return;
 	}
-	if (!graph_exec || graph_stream_key != s) {
-		if (graph_exec)
-			cudaGraphExecDestroy(graph_exec);
-		graph_exec = nullptr;
+	if (!g.exec || g.stream != s) {
+		g.drop();
 		cudaStream_t cs;
 		PST_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-		cudaGraph_t g;
+		cudaGraph_t gr;
 		PST_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
 		try {
-			enqueue_counting(cs);
+			(this->*enqueue)(cs);
 		} catch (...) {
-			cudaStreamEndCapture(cs, &g);
+			cudaStreamEndCapture(cs, &gr);
 			cudaStreamDestroy(cs);
 			throw;
 		}
-		PST_CUDA(cudaStreamEndCapture(cs, &g));
-		PST_CUDA(cudaGraphInstantiate(&graph_exec, g, 0));
-		cudaGraphDestroy(g);
+		PST_CUDA(cudaStreamEndCapture(cs, &gr));
+		PST_CUDA(cudaGraphInstantiate(&g.exec, gr, 0));
+		cudaGraphDestroy(gr);
 		cudaStreamDestroy(cs);
-		graph_stream_key = s;
+		g.stream = s;
 	}
-	PST_CUDA(cudaGraphLaunch(graph_exec, s));
+	PST_CUDA(cudaGraphLaunch(g.exec, s));
+}
+
+void Batch::launch_count(cudaStream_t s) { launch_graph(full_graph, &Batch::enqueue_counting, s); }
+
+void Batch::launch_count_top(cudaStream_t s)
+{
+	if (ctl_host->nq > SMALL_BATCH_Q)
+		fail(PST_ERR_INTERNAL, "top pass on a batch of more than " + std::to_string(SMALL_BATCH_Q) + " queries");
+	launch_graph(top_graph, &Batch::enqueue_counting_top, s);
+}
+
+void Batch::launch_count_rest(uint32_t from, cudaStream_t s)
+{
+	switch (tree->dtype) {
+	case PST_F32: enqueue_count_rest<float>(from, s); break;
+	case PST_F64: enqueue_count_rest<double>(from, s); break;
+	case PST_I32: enqueue_count_rest<int32_t>(from, s); break;
+	}
 }
 
 void Batch::stage_queries(const pst_query *q, uint32_t nq, bool on_device, cudaStream_t s)
@@ -1014,67 +1073,65 @@ pst_status Batch::read_ctl(cudaStream_t s, uint64_t *total)
 	return PST_OK;
 }
 
-// Count pass with automatic growth of the frontier buffer.
+// Count pass with the host waiting for it.
 void Batch::count_sync(cudaStream_t s, uint64_t *total)
+{
+	if (ctl_host->nq <= SMALL_BATCH_Q)
+		count_small_sync(s, total);
+	else
+		count_full_sync(s, total);
+}
+
+// Reads the control block after a pass; true when it is complete, false when the
+// frontier overflowed (and has been grown for another attempt).
+static bool settle(Batch &b, const BatchCtl &h, int attempt, cudaStream_t s, uint64_t *total)
+{
+	b.last = h;
+	if (h.flags & BATCH_FLAG_BAD_QUERY)
+		fail(PST_ERR_INVALID, "query kind must be PST_Q_THREE, PST_Q_LEFT or PST_Q_RIGHT");
+	if (h.flags & BATCH_FLAG_INTERNAL)
+		fail(PST_ERR_INTERNAL, "search consistency check failed");
+	if (!(h.flags & BATCH_FLAG_TASK_OVERFLOW)) {
+		*total = h.total;
+		return true;
+	}
+	if (attempt > 8)
+		fail(PST_ERR_INTERNAL, "frontier did not fit after growth");
+	b.grow_tasks(std::max<uint64_t>(h.need_tasks + h.need_tasks / 4, b.task_cap * 2), s);
+	return false;
+}
+
+// The whole pass, with automatic growth of the frontier buffer.
+void Batch::count_full_sync(cudaStream_t s, uint64_t *total)
 {
 	for (int attempt = 0;; attempt++) {
 		launch_count(s);
 		BatchCtl h;
 		PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
 		PST_CUDA(cudaStreamSynchronize(s));
-		last = h;
-		if (h.flags & BATCH_FLAG_BAD_QUERY)
-			fail(PST_ERR_INVALID, "query kind must be PST_Q_THREE, PST_Q_LEFT or PST_Q_RIGHT");
-		if (h.flags & BATCH_FLAG_INTERNAL)
-			fail(PST_ERR_INTERNAL, "search consistency check failed");
-		if (!(h.flags & BATCH_FLAG_TASK_OVERFLOW)) {
-			*total = h.total;
+		if (settle(*this, h, attempt, s, total))
 			return;
-		}
-		if (attempt > 8)
-			fail(PST_ERR_INTERNAL, "frontier did not fit after growth");
-		grow_tasks(std::max<uint64_t>(h.need_tasks + h.need_tasks / 4, task_cap * 2), s);
 	}
 }
 
-// Count pass of a single query (max_q == 1): the one-CTA top pass, then, if it
-// stopped above the bottom, the per-level kernels for the rest and the scan; with
-// automatic growth of the frontier buffer as in count_sync.
-void Batch::count_single_sync(cudaStream_t s, uint64_t *total)
+// A small batch: the one-CTA top pass, then, if it stopped above the bottom, the
+// per-level kernels for the rest and the scan; with automatic growth of the
+// frontier buffer as in count_full_sync.
+void Batch::count_small_sync(cudaStream_t s, uint64_t *total)
 {
-	if (max_q != 1)
-		fail(PST_ERR_INTERNAL, "single-query count pass on a batch engine");
 	for (int attempt = 0;; attempt++) {
-		switch (tree->dtype) {
-		case PST_F32: enqueue_count_single_head<float>(s); break;
-		case PST_F64: enqueue_count_single_head<double>(s); break;
-		case PST_I32: enqueue_count_single_head<int32_t>(s); break;
-		}
+		launch_count_top(s);
 		BatchCtl h;
 		PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
 		PST_CUDA(cudaStreamSynchronize(s));
 		if (!(h.flags & (BATCH_FLAG_BAD_QUERY | BATCH_FLAG_INTERNAL | BATCH_FLAG_TASK_OVERFLOW)) &&
 		    h.cta_levels < tree->levels) {
-			switch (tree->dtype) {
-			case PST_F32: enqueue_count_single_tail<float>(h.cta_levels, s); break;
-			case PST_F64: enqueue_count_single_tail<double>(h.cta_levels, s); break;
-			case PST_I32: enqueue_count_single_tail<int32_t>(h.cta_levels, s); break;
-			}
+			launch_count_rest(h.cta_levels, s);
 			PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
 			PST_CUDA(cudaStreamSynchronize(s));
 		}
-		last = h;
-		if (h.flags & BATCH_FLAG_BAD_QUERY)
-			fail(PST_ERR_INVALID, "query kind must be PST_Q_THREE, PST_Q_LEFT or PST_Q_RIGHT");
-		if (h.flags & BATCH_FLAG_INTERNAL)
-			fail(PST_ERR_INTERNAL, "search consistency check failed");
-		if (!(h.flags & BATCH_FLAG_TASK_OVERFLOW)) {
-			*total = h.total;
+		if (settle(*this, h, attempt, s, total))
 			return;
-		}
-		if (attempt > 8)
-			fail(PST_ERR_INTERNAL, "frontier did not fit after growth");
-		grow_tasks(std::max<uint64_t>(h.need_tasks + h.need_tasks / 4, task_cap * 2), s);
 	}
 }
 
@@ -1186,11 +1243,18 @@ uint64_t noalloc_run(TreeStorage &t, const pst_query &q, pst_ret ret, void *out,
 	WorkDev w{rec, NA_REC_CAP, path0, path1, seed0, seed1, 2u, ro, NA_RO_CAP, counts, cursor, offsets, ctl};
 	k_check_kinds<<<1, 32, 0, s>>>(qraw, ctl);
 	k_unpack_queries<T><<<1, 32, 0, s>>>(qraw, ctl, kind, min1, max1, min2, path0);
-	for (uint32_t d = 0; d < tv.levels; d++)
-		launch_level<T>(tv, qd, w, d, grid, BFS_THREADS, s);
-	exclusive_scan<uint64_t>(counts, offsets, 1, scan, &ctl->total, s);
+	// the one-CTA top pass, then the per-level kernels for whatever it left
+	k_bfs_cta<T><<<1, BFS_THREADS, 0, s>>>(tv, qd, w, 1u);
 	PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
 	PST_CUDA(cudaStreamSynchronize(s));
+	if (!(h.flags & (BATCH_FLAG_BAD_QUERY | BATCH_FLAG_INTERNAL | BATCH_FLAG_TASK_OVERFLOW)) &&
+	    h.cta_levels < tv.levels) {
+		for (uint32_t d = h.cta_levels; d < tv.levels; d++)
+			launch_level<T>(tv, qd, w, d, grid, BFS_THREADS, s);
+		exclusive_scan<uint64_t>(counts, offsets, 1, scan, &ctl->total, s);
+		PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
+		PST_CUDA(cudaStreamSynchronize(s));
+	}
 	if (h.flags & BATCH_FLAG_BAD_QUERY)
 		fail(PST_ERR_INVALID, "query kind must be PST_Q_THREE, PST_Q_LEFT or PST_Q_RIGHT");
 	if (h.flags & (BATCH_FLAG_TASK_OVERFLOW | BATCH_FLAG_INTERNAL))

@@ -6,6 +6,9 @@
 namespace pst {
 
 constexpr int BFS_THREADS = 256;
+// Batches of at most this many queries start with the one-CTA top pass, which walks
+// the upper levels without a kernel boundary between them.
+constexpr uint32_t SMALL_BATCH_Q = 32;
 
 enum : uint32_t {
 	BATCH_FLAG_TASK_OVERFLOW = 1u,  // frontier buffer too small (results incomplete)
@@ -23,7 +26,7 @@ struct BatchCtl {
 	uint32_t rec_cnt;       // reported boundary nodes
 	uint32_t nq;
 	uint32_t flags;
-	uint32_t cta_levels;    // levels already done by the one-CTA top pass (single queries)
+	uint32_t cta_levels;    // levels already done by the one-CTA top pass (small batches)
 	uint64_t need_tasks;
 	uint64_t total;
 };
@@ -52,18 +55,33 @@ struct Batch {
 	BatchCtl *ctl = nullptr;
 	BatchCtl *ctl_host = nullptr;  // pinned, zeroed except nq
 	BatchCtl last{};
-	cudaGraphExec_t graph_exec = nullptr;
-	cudaStream_t graph_stream_key = nullptr;
+	// captured passes, each for the stream it was captured for: the whole count pass,
+	// and the top pass of small batches
+	struct Graph {
+		cudaGraphExec_t exec = nullptr;
+		cudaStream_t stream = nullptr;
+		void drop();
+	};
+	Graph full_graph, top_graph;
 
 	~Batch();
 	void init(TreeStorage *t, const pst_batch_opts &o);
 	void release();
 	void grow_tasks(uint64_t cap, cudaStream_t s);
 	void stage_queries(const pst_query *q, uint32_t nq, bool on_device, cudaStream_t s);
+	// Whole count pass (every level kernel and the scan), asynchronous.
 	void launch_count(cudaStream_t s);
+	// Top pass of a small batch (nq <= SMALL_BATCH_Q), asynchronous: when it stops
+	// above the bottom (ctl->cta_levels < tree levels), launch_count_rest finishes it.
+	void launch_count_top(cudaStream_t s);
+	void launch_count_rest(uint32_t from, cudaStream_t s);
+	// Count pass with the host waiting for it: the top pass for small batches, the
+	// whole pass otherwise; grows the frontier buffer until the pass fits.
 	void count_sync(cudaStream_t s, uint64_t *total);
-	void count_single_sync(cudaStream_t s, uint64_t *total);
+	void count_full_sync(cudaStream_t s, uint64_t *total);
+	void count_small_sync(cudaStream_t s, uint64_t *total);
 	void enqueue_counting(cudaStream_t s);
+	void enqueue_counting_top(cudaStream_t s);
 	void enqueue_emit(pst_ret ret, void *out, uint64_t capacity, cudaStream_t s);
 	pst_status read_ctl(cudaStream_t s, uint64_t *total);
 	uint64_t record_size(pst_ret ret) const;
@@ -72,9 +90,10 @@ struct Batch {
 	template <typename T>
 	void enqueue_count(cudaStream_t s);
 	template <typename T>
-	void enqueue_count_single_head(cudaStream_t s);
+	void enqueue_count_top(cudaStream_t s);
 	template <typename T>
-	void enqueue_count_single_tail(uint32_t from, cudaStream_t s);
+	void enqueue_count_rest(uint32_t from, cudaStream_t s);
+	void launch_graph(Graph &g, void (Batch::*enqueue)(cudaStream_t), cudaStream_t s);
 	template <typename T>
 	void enqueue_emit_v(pst_ret ret, void *out, uint64_t capacity, cudaStream_t s);
 	template <typename T, bool HAS_ID, bool POINTS>

@@ -107,7 +107,9 @@ struct Arena {
 	}
 };
 
-enum SlotPhase { SLOT_IDLE, SLOT_COUNTING, SLOT_EMITTING };
+// A small batch counts in two steps: its top pass (SLOT_TOP), then, only when that
+// stopped above the bottom of the tree, the per-level kernels for the rest.
+enum SlotPhase { SLOT_IDLE, SLOT_TOP, SLOT_COUNTING, SLOT_EMITTING };
 
 struct Slot {
 	Batch eng;
@@ -231,6 +233,17 @@ struct Server {
 			return false;
 		check_cuda(cudaGetLastError(), "slot event");
 		const uint32_t n = (uint32_t) sl.reqs.size();
+		if (sl.phase == SLOT_TOP) {
+			const BatchCtl &c = *sl.ctl_h;
+			sl.phase = SLOT_COUNTING;
+			if (!(c.flags & (BATCH_FLAG_TASK_OVERFLOW | BATCH_FLAG_BAD_QUERY | BATCH_FLAG_INTERNAL)) &&
+			    c.cta_levels < sl.eng.tree->levels) {
+				sl.eng.launch_count_rest(c.cta_levels, sl.stream);
+				copy_count_results(sl, n);
+				return true;
+			}
+			// the top pass reached the bottom (or failed): its results are final
+		}
 		if (sl.phase == SLOT_COUNTING) {
 			const BatchCtl &c = *sl.ctl_h;
 			if (c.flags & BATCH_FLAG_TASK_OVERFLOW) {
@@ -323,13 +336,25 @@ struct Server {
 	{
 		const uint32_t n = (uint32_t) sl.reqs.size();
 		sl.eng.stage_queries(sl.qhost.data(), n, false, sl.stream);
-		sl.eng.launch_count(sl.stream);
+		if (n <= SMALL_BATCH_Q) {
+			sl.eng.launch_count_top(sl.stream);
+			sl.phase = SLOT_TOP;
+		} else {
+			sl.eng.launch_count(sl.stream);
+			sl.phase = SLOT_COUNTING;
+		}
+		copy_count_results(sl, n);
+	}
+
+	// Control block and per-query counts back to the slot's pinned buffers, then the
+	// slot's event.
+	void copy_count_results(Slot &sl, uint32_t n)
+	{
 		check_cuda(cudaMemcpyAsync(sl.ctl_h, sl.eng.ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, sl.stream),
 		           "copy control");
 		check_cuda(cudaMemcpyAsync(sl.counts_h, sl.eng.counts, (size_t) n * 8, cudaMemcpyDeviceToHost, sl.stream),
 		           "copy counts");
 		check_cuda(cudaEventRecord(sl.ev, sl.stream), "event");
-		sl.phase = SLOT_COUNTING;
 	}
 
 	void fail_all(Slot &sl, pst_status status)
@@ -371,9 +396,18 @@ struct Server {
 					for (auto &sl : ts->slots)
 						progress |= step(*ts, *sl);
 				if (!progress) {
-					std::unique_lock<std::mutex> lk(mu);
-					if (inbox.empty() && !stop)
-						cv_work.wait_for(lk, inflight ? std::chrono::microseconds(20) : std::chrono::milliseconds(5));
+					if (inflight) {
+						// GPU steps in flight: poll their events again right away.  A timed
+						// wait here would add its whole sleep, rounded up by the OS timer
+						// slack (about 100 us for a 20 us wait), to every step of every
+						// request; a stream host function to wake this thread costs more
+						// still, as it holds back the stream's next work.
+						std::this_thread::yield();
+					} else {
+						std::unique_lock<std::mutex> lk(mu);
+						if (inbox.empty() && !stop)
+							cv_work.wait_for(lk, std::chrono::milliseconds(5));
+					}
 				}
 			}
 		} catch (const Error &e) {
@@ -434,7 +468,8 @@ uint32_t server_add_tree(Server *s, TreeStorage *t)
 		bo.task_capacity = std::max<uint64_t>(1ull << 16, t->n / 8);
 		sl->eng.init(t, bo);
 		check_cuda(cudaStreamCreateWithFlags(&sl->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-		// warm-up pass: captures the slot's graph now rather than under the first request
+		// warm-up passes: capture the slot's graphs (the whole count pass, and the top pass
+		// of small batches) now rather than under the first requests
 		{
 			// an inverted 3-sided range walks one path and reports nothing
 			pst_query q{};
@@ -451,7 +486,8 @@ uint32_t server_add_tree(Server *s, TreeStorage *t)
 			}
 			sl->eng.stage_queries(&q, 1, false, sl->stream);
 			uint64_t total = 0;
-			sl->eng.count_sync(sl->stream, &total);
+			sl->eng.count_full_sync(sl->stream, &total);
+			sl->eng.count_small_sync(sl->stream, &total);
 		}
 		check_cuda(cudaEventCreateWithFlags(&sl->ev, cudaEventDisableTiming), "cudaEventCreate");
 		check_cuda(cudaMallocHost((void **) &sl->ctl_h, sizeof(BatchCtl)), "cudaMallocHost");

@@ -135,3 +135,62 @@ def test_batch_bad_kind_and_capacity(pst):
         eng.count(bad)
     eng.close()
     tr.close()
+
+
+def _narrow_queries(pts, k, seed):
+    """k queries of a few results each: a 3-sided range around one point's dim1 with
+    that point's dim2 as bound, and 2-sided ranges cut at the 6th smallest / largest
+    dim1.  Their searches reach the bottom of the tree with a small frontier."""
+    rng = np.random.default_rng(seed)
+    d1, d2 = pts["dim1"], pts["dim2"]
+    s1 = np.sort(d1)
+    out = []
+    for j in range(k):
+        i = int(rng.integers(0, len(pts)))
+        kind = ["three", "left", "right"][j % 3]
+        if kind == "three":
+            out.append(("three", d1[i], d1[i], d2[i]))
+        elif kind == "left":
+            out.append(("left", 0, s1[5], rng.choice(d2)))
+        else:
+            out.append(("right", s1[-6], 0, rng.choice(d2)))
+    return out
+
+
+@pytest.mark.parametrize("dt", ["f32", "f64", "i32"])
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_small_batches(pst, oracle, dt, use_graph):
+    """Batches of 1 to 33 queries (the top pass, which takes the upper levels in one
+    CTA, serves batches of at most 32) into engines of 1 to 1024 queries: narrow
+    queries whose frontier stays small to the bottom, wide ones that leave the lower
+    levels to the per-level kernels, a mix of both, and a frontier buffer so small
+    that the top pass overflows it and the engine grows it."""
+    pts = rand_points(200003, dt, ids="random", dup=(dt == "i32"), seed=31)
+    ref = oracle.Orc.build(pts, dt)
+    tr = pst.StaticPSTGPU.from_numpy(pts, dt)
+    narrow = _narrow_queries(pts, 33, seed=32)
+    wide = rand_queries(pts, 33, seed=33)
+    mixed = [narrow[i] if i % 2 else wide[i] for i in range(33)]
+    want = {}
+    for qs in (narrow, wide, mixed):
+        for x in qs:
+            if x not in want:
+                want[x] = _oracle_set(oracle, ref, *x, False)
+    for max_q, cap in ((1, 0), (32, 0), (33, 0), (1024, 0), (64, 64)):
+        eng = pst.BatchEngine(tr, max_queries=max_q, task_capacity=cap, use_graph=use_graph)
+        for qs in (narrow, wide, mixed):
+            for nq in sorted({1, 2, 7, 31, 32, 33}):
+                if nq > max_q:
+                    continue
+                sub = qs[:nq]
+                q = pst.make_queries([pst.pst.KIND[k] for k, *_ in sub], [x[1] for x in sub], [x[2] for x in sub],
+                                     [x[3] for x in sub], dt)
+                counts, total = eng.count(q)
+                offs, res = eng.search(q)
+                assert offs[0] == 0 and int(offs[nq]) == total == len(res) == int(counts.sum().item())
+                for i, x in enumerate(sub):
+                    got = res[offs[i]:offs[i + 1]]
+                    assert int(counts[i].item()) == len(got)
+                    assert np.array_equal(oracle.canon(got), want[x]), (max_q, nq, i, x)
+        eng.close()
+    tr.close()
