@@ -183,6 +183,8 @@ pst_status pst_search_noalloc(pst_tree *tree, const pst_query *query, pst_ret re
 /* ------------------------------------------------------------------------- */
 /* Batched queries: many queries of mixed kinds in one level-synchronous pass
  * (count prepass, exact offsets, emit), replayed from a captured CUDA graph.
+ * Waiting calls with at most 32 queries start with a one-CTA pass over the upper
+ * levels and launch per-level kernels only below where it stopped.
  * The reference has one query per launch (pst/static-pst-gpu.tu:496-642); this
  * is the batched form of the same searches. */
 

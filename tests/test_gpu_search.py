@@ -194,3 +194,32 @@ def test_small_batches(pst, oracle, dt, use_graph):
                     assert np.array_equal(oracle.canon(got), want[x]), (max_q, nq, i, x)
         eng.close()
     tr.close()
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_batch_async_run(pst, oracle, use_graph):
+    """pst_batch_run with sync = 0 (everything enqueued, nothing waited for; small
+    batches take the whole pass there) gives the offsets and results of the
+    waiting run, for a small and a large batch."""
+    import torch
+    pts = rand_points(100000, "f32", ids="random", seed=41)
+    ref = oracle.Orc.build(pts, "f32")
+    tr = pst.StaticPSTGPU.from_numpy(pts, "f32")
+    eng = pst.BatchEngine(tr, max_queries=512, use_graph=use_graph)
+    for nq in (5, 300):
+        qs = rand_queries(pts, nq, seed=42 + nq)
+        q = pst.make_queries([pst.pst.KIND[k] for k, *_ in qs], [x[1] for x in qs], [x[2] for x in qs],
+                             [x[3] for x in qs], "f32")
+        offs, res = eng.search(q)
+        out = torch.empty(max(len(res) * 4, 16), dtype=torch.uint8, device="cuda")
+        offs_d = torch.empty(nq + 1, dtype=torch.int64, device="cuda")
+        st, tot = eng.run(q, out, offs_d, sync=False)
+        torch.cuda.synchronize()
+        assert st == 0 and tot == len(res)
+        assert np.array_equal(offs_d.cpu().numpy().astype(np.uint64), offs)
+        got_all = out[: tot * 4].cpu().numpy().view(np.uint32)
+        for i, x in enumerate(qs):
+            got = got_all[offs[i]:offs[i + 1]]
+            assert np.array_equal(oracle.canon(got), _oracle_set(oracle, ref, *x, False)), (nq, i)
+    eng.close()
+    tr.close()
