@@ -595,10 +595,23 @@ __device__ __forceinline__ uint64_t claim_output(const WorkDev &w, uint32_t q, u
 	return (valid && pc) ? w.offsets[q] + rb + run - pc : 0;
 }
 
+// Output range check of one lane's record, made once where the lane claims it: a
+// record whose claimed range would end past the output's capacity is cleared (it
+// writes nothing) and flagged.  Counts and claims come from the same masks, so this
+// never fires; it keeps the warp-wide store loop of emit_blocks free of per-store
+// checks (a 64-bit compare at every 4-byte store cost 8 % of a batched step).
+__device__ __forceinline__ void guard_claim(const WorkDev &w, uint4 &rec, uint64_t out_base, uint64_t capacity)
+{
+	if (out_base + __popc(rec.z) + __popc(rec.w) > capacity) {
+		atomicOr(&w.ctl->flags, BATCH_FLAG_INTERNAL);
+		rec.z = rec.w = 0;
+	}
+}
+
 // Writes the results of the warp's records (lane k owns record `mine`, whose results
-// start at out_base; the valid lanes are a prefix): the lanes stage their records
-// and offsets, then the warp writes U records at a time, each by the whole warp,
-// lane l taking slots 2l and 2l + 1 of the 64-slot block.
+// start at out_base, checked by guard_claim; the valid lanes are a prefix): the
+// lanes stage their records and offsets, then the warp writes U records at a time,
+// each by the whole warp, lane l taking slots 2l and 2l + 1 of the 64-slot block.
 struct EmitStage {
 	uint4 rec[32];
 	unsigned long long ob[32];
@@ -606,7 +619,7 @@ struct EmitStage {
 
 template <typename T, bool HAS_ID, bool POINTS>
 __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mine, uint64_t out_base, bool valid,
-                                            EmitStage &st, void *__restrict__ out, uint64_t capacity)
+                                            EmitStage &st, void *__restrict__ out)
 {
 	using Pt = Point<T, HAS_ID>;
 	constexpr int U = POINTS ? 4 : 8;  // records in flight
@@ -657,25 +670,22 @@ __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mi
 		}
 #pragma unroll
 		for (int u = 0; u < U; u++) {
-			uint64_t oo = o[u];
 #pragma unroll
 			for (int j = 0; j < 2; j++) {
 				if ((b2[u] >> j) & 1u) {
-					if (oo < capacity) {
-						if constexpr (POINTS) {
-							Pt rec;
-							rec.dim1 = d1[u][j];
-							rec.dim2 = d2[u][j];
-							if constexpr (HAS_ID)
-								rec.id = j ? idv[u].y : idv[u].x;
-							static_cast<Pt *>(out)[oo] = rec;
-						} else {
-							// evict-first: the output streams through L2 once and should not push
-							// out tree rows that other queries' records read again
-							__stcs(static_cast<uint32_t *>(out) + oo, j ? idv[u].y : idv[u].x);
-						}
+					const uint64_t oo = o[u] + (j & b2[u]);  // the second slot follows a reported first
+					if constexpr (POINTS) {
+						Pt rec;
+						rec.dim1 = d1[u][j];
+						rec.dim2 = d2[u][j];
+						if constexpr (HAS_ID)
+							rec.id = j ? idv[u].y : idv[u].x;
+						static_cast<Pt *>(out)[oo] = rec;
+					} else {
+						// evict-first: the output streams through L2 once and should not push
+						// out tree rows that other queries' records read again
+						__stcs(static_cast<uint32_t *>(out) + oo, j ? idv[u].y : idv[u].x);
 					}
-					oo++;
 				}
 			}
 		}
@@ -713,12 +723,14 @@ __global__ void __launch_bounds__(BFS_THREADS) k_emit(TreeDev<T> t, WorkDev w, v
 	bool v0 = wb + lane < total;
 	uint4 m0 = v0 ? w.rec[wb + lane] : make_uint4(0, 0, 0, 0);
 	uint64_t ob0 = wb < total ? claim_output(w, m0.y, __popc(m0.z) + __popc(m0.w), v0) : 0;
+	guard_claim(w, m0, ob0, capacity);
 	while (wb < total) {
 		const uint64_t nb = wb + stride;
 		const bool v1 = nb + lane < total;
-		const uint4 m1 = v1 ? w.rec[nb + lane] : make_uint4(0, 0, 0, 0);
+		uint4 m1 = v1 ? w.rec[nb + lane] : make_uint4(0, 0, 0, 0);
 		const uint64_t ob1 = nb < total ? claim_output(w, m1.y, __popc(m1.z) + __popc(m1.w), v1) : 0;
-		emit_blocks<T, HAS_ID, POINTS>(t, m0, ob0, v0, s_stage[threadIdx.x >> 5], out, capacity);
+		guard_claim(w, m1, ob1, capacity);
+		emit_blocks<T, HAS_ID, POINTS>(t, m0, ob0, v0, s_stage[threadIdx.x >> 5], out);
 		wb = nb;
 		v0 = v1;
 		m0 = m1;
@@ -726,9 +738,10 @@ __global__ void __launch_bounds__(BFS_THREADS) k_emit(TreeDev<T> t, WorkDev w, v
 	}
 	for (uint64_t wb = gwarp * 32; wb < nro; wb += gwarps * 32) {
 		const bool valid = wb + lane < nro;
-		const uint4 mine = valid ? w.ro[wb + lane] : make_uint4(0, 0, 0, 0);
+		uint4 mine = valid ? w.ro[wb + lane] : make_uint4(0, 0, 0, 0);
 		const uint64_t ob = claim_output(w, mine.y, __popc(mine.z) + __popc(mine.w), valid);
-		emit_blocks<T, HAS_ID, POINTS>(t, mine, ob, valid, s_stage[threadIdx.x >> 5], out, capacity);
+		guard_claim(w, mine, ob, capacity);
+		emit_blocks<T, HAS_ID, POINTS>(t, mine, ob, valid, s_stage[threadIdx.x >> 5], out);
 	}
 }
 

@@ -144,6 +144,7 @@ def _narrow_queries(pts, k, seed):
     rng = np.random.default_rng(seed)
     d1, d2 = pts["dim1"], pts["dim2"]
     s1 = np.sort(d1)
+    c = min(5, len(s1) - 1)
     out = []
     for j in range(k):
         i = int(rng.integers(0, len(pts)))
@@ -151,9 +152,9 @@ def _narrow_queries(pts, k, seed):
         if kind == "three":
             out.append(("three", d1[i], d1[i], d2[i]))
         elif kind == "left":
-            out.append(("left", 0, s1[5], rng.choice(d2)))
+            out.append(("left", 0, s1[c], rng.choice(d2)))
         else:
-            out.append(("right", s1[-6], 0, rng.choice(d2)))
+            out.append(("right", s1[-1 - c], 0, rng.choice(d2)))
     return out
 
 
@@ -221,5 +222,27 @@ def test_batch_async_run(pst, oracle, use_graph):
         for i, x in enumerate(qs):
             got = got_all[offs[i]:offs[i + 1]]
             assert np.array_equal(oracle.canon(got), _oracle_set(oracle, ref, *x, False)), (nq, i)
+    eng.close()
+    tr.close()
+
+
+@pytest.mark.parametrize("dt", ["f32", "i32"])
+@pytest.mark.parametrize("n", [3, 63, 64, 65, 255, 256, 257, 511, 512, 513, 4095, 4096, 4097, 65535, 65536, 65537])
+def test_batch_tree_sizes(pst, oracle, dt, n):
+    """Batched search on trees whose last level is full, holds one node, or is
+    missing (n = 2^k - 1, 2^k, 2^k + 1; the last-level parent bitmap exists from
+    n = 256 on): a batch of 32 (top pass) and one of 60 (whole pass)."""
+    pts = rand_points(n, dt, ids="random", dup=(dt == "i32"), seed=n + 77)
+    ref = oracle.Orc.build(pts, dt)
+    tr = pst.StaticPSTGPU.from_numpy(pts, dt)
+    qs = rand_queries(pts, 30, seed=n) + _narrow_queries(pts, 30, seed=n + 1)
+    eng = pst.BatchEngine(tr, max_queries=64)
+    for sub in (qs[:32], qs):
+        q = pst.make_queries([pst.pst.KIND[k] for k, *_ in sub], [x[1] for x in sub], [x[2] for x in sub],
+                             [x[3] for x in sub], dt)
+        offs, res = eng.search(q)
+        for i, x in enumerate(sub):
+            got = res[offs[i]:offs[i + 1]]
+            assert np.array_equal(oracle.canon(got), _oracle_set(oracle, ref, *x, False)), (n, i, x)
     eng.close()
     tr.close()
