@@ -623,6 +623,7 @@ __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mi
 {
 	using Pt = Point<T, HAS_ID>;
 	constexpr int U = POINTS ? 4 : 8;  // records in flight
+	static_assert(32 % U == 0, "a batch of records ends inside the 32 staged ones");
 	const uint32_t lane = lane_id();
 	const uint32_t psh = (2 * lane) & 31;
 	st.rec[lane] = mine;
@@ -636,13 +637,15 @@ __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mi
 		T d1[POINTS ? U : 1][2], d2[POINTS ? U : 1][2];
 #pragma unroll
 		for (int u = 0; u < U; u++) {
+			// every lane staged a record, and those past nrec are empty (zero masks), so
+			// a batch that runs past nrec reads them and writes nothing: no bound test
+			// per record (U divides 32, so k < 32)
 			const int k = k0 + u;
-			const int src = k < nrec ? k : 0;
-			const uint4 rc = st.rec[src];
-			b2[u] = k < nrec ? ((lane < 16 ? rc.z : rc.w) >> psh) & 3u : 0u;
+			const uint4 rc = st.rec[k];
+			b2[u] = ((lane < 16 ? rc.z : rc.w) >> psh) & 3u;
 			const uint32_t before = lane < 16 ? __popc(rc.z & ((1u << psh) - 1u))
 			                                  : __popc(rc.z) + __popc(rc.w & ((1u << psh) - 1u));
-			o[u] = st.ob[src] + before;
+			o[u] = st.ob[k] + before;
 			hb[u] = rc.x + 2 * lane;
 			if constexpr (!POINTS || HAS_ID)
 				idv[u] = b2[u] ? *reinterpret_cast<const uint2 *>(t.id + hb[u]) : make_uint2(0, 0);
