@@ -626,6 +626,9 @@ __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mi
 	static_assert(32 % U == 0, "a batch of records ends inside the 32 staged ones");
 	const uint32_t lane = lane_id();
 	const uint32_t psh = (2 * lane) & 31;
+	// the record's slots before this lane's pair, as masks of its two 32-slot words
+	const uint32_t below_z = lane < 16 ? (1u << psh) - 1u : FULL;
+	const uint32_t below_w = lane < 16 ? 0u : (1u << psh) - 1u;
 	st.rec[lane] = mine;
 	st.ob[lane] = out_base;
 	__syncwarp();
@@ -643,8 +646,7 @@ __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mi
 			const int k = k0 + u;
 			const uint4 rc = st.rec[k];
 			b2[u] = ((lane < 16 ? rc.z : rc.w) >> psh) & 3u;
-			const uint32_t before = lane < 16 ? __popc(rc.z & ((1u << psh) - 1u))
-			                                  : __popc(rc.z) + __popc(rc.w & ((1u << psh) - 1u));
+			const uint32_t before = __popc(rc.z & below_z) + __popc(rc.w & below_w);
 			o[u] = st.ob[k] + before;
 			hb[u] = rc.x + 2 * lane;
 			if constexpr (!POINTS || HAS_ID)
