@@ -332,11 +332,13 @@ __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__r
 #pragma unroll
 		for (int u = 0; u < U; u++) {
 			const T m2 = st.m2[kk[u]];
-			uint32_t bits = 0;
+			// all four slots are compared (values of slots without a candidate are zero or
+			// loaded anyway) and the candidates masked once, not tested slot by slot
+			uint32_t ge = 0;
 #pragma unroll
 			for (int j = 0; j < 4; j++)
-				bits |= (((cn[u] >> j) & 1u) && m2 <= v[u][j]) ? 1u << j : 0u;
-			uint32_t row = bits << (4 * qd);
+				ge |= (m2 <= v[u][j]) ? 1u << j : 0u;
+			uint32_t row = (ge & cn[u]) << (4 * qd);
 			row |= __shfl_xor_sync(FULL, row, 1);
 			row |= __shfl_xor_sync(FULL, row, 2);
 			row |= __shfl_xor_sync(FULL, row, 4);
