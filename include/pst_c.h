@@ -235,8 +235,11 @@ pst_status pst_batch_last_stats(pst_batch *batch, pst_batch_stats *stats, uint32
  * exact output bytes that pass predicts fit the free result arena.  Batches of
  * different trees and slots run on separate streams and overlap on the device.
  * Latency is measured from each request's arrival time to the moment its result
- * is in host memory.  The reference has no serving layer; each request is the
- * search of pst/static-pst-gpu.tu:496-642. */
+ * is in host memory.  One worker thread per server drives every batch: while
+ * any batch is on the device it polls their events without sleeping (one CPU
+ * core busy), and with nothing in flight it sleeps until a submission.  The
+ * reference has no serving layer; each request is the search of
+ * pst/static-pst-gpu.tu:496-642. */
 
 typedef struct pst_server pst_server;
 
