@@ -1,0 +1,47 @@
+"""The batched bench's workload, checked on the CPU: the query plan has the stated
+kind mix and selectivity range, and the bisection that sets each query's free
+bound reaches its target count (measured here by brute force over the points)."""
+import sys
+from pathlib import Path
+
+import numpy as np
+
+sys.path.insert(0, str(Path(__file__).resolve().parent.parent))
+import bench  # noqa: E402
+
+
+def test_query_plan_mix_and_selectivities():
+    kinds, sel, anchor = bench.query_plan(bench.NQ, 7)
+    assert len(kinds) == len(sel) == len(anchor) == 4096
+    assert np.bincount(kinds, minlength=3).tolist() == [2048, 1024, 1024]  # 50 % three, 25 % left, 25 % right
+    assert sel.min() >= bench.SEL_LO and sel.max() <= bench.SEL_HI
+    # log-uniform: the mean of log(sel) sits at the middle of the log range
+    mid = (np.log(bench.SEL_LO) + np.log(bench.SEL_HI)) / 2
+    assert abs(np.log(sel).mean() - mid) < 0.2
+    assert anchor.min() >= 0 and anchor.max() < 1 << 24
+    k2, s2, a2 = bench.query_plan(bench.NQ, 7)
+    assert np.array_equal(kinds, k2) and np.array_equal(sel, s2) and np.array_equal(anchor, a2)
+
+
+def _brute_counts(pts, kinds, min1, max1, min2):
+    d1 = pts["dim1"][None, :]
+    d2 = pts["dim2"][None, :]
+    ok2 = d2 >= min2[:, None]
+    three = (d1 >= min1[:, None]) & (d1 <= max1[:, None])
+    left = d1 <= max1[:, None]
+    right = d1 >= min1[:, None]
+    k = kinds[:, None]
+    hit = ok2 & np.where(k == 0, three, np.where(k == 1, left, right))
+    return hit.sum(axis=1)
+
+
+def test_calibration_reaches_targets():
+    n = 1 << 16
+    pts = bench.gen_points_host(n, 1)
+    kinds, _, anchor = bench.query_plan(48, 3)
+    # targets of 100 to 650 points: large enough that one point is within 1 %
+    sel = np.exp(np.random.default_rng(4).uniform(np.log(1.5e-3), np.log(1e-2), 48))
+    min1, max1, min2 = bench.calibrate(lambda k, a, b, c: _brute_counts(pts, k, a, b, c), kinds, sel, anchor, n)
+    got = _brute_counts(pts, kinds, min1, max1, min2)
+    err = np.abs(got - sel * n) / (sel * n)
+    assert err.max() < 0.01, err  # every query within 1 % of its target count
