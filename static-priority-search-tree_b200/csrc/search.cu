@@ -935,7 +935,9 @@ void Batch::enqueue_count_top(cudaStream_t s)
 	TreeDev<T> tv = tree->view<T>();
 	QDev<T> qd{kind, static_cast<const T *>(min1), static_cast<const T *>(max1), static_cast<const T *>(min2)};
 	PST_WORKDEV;
-	const unsigned qt = (unsigned) std::min<uint32_t>((max_q + 31) / 32 * 32, SMALL_BATCH_Q);
+	// one thread per query of the batch (at most SMALL_BATCH_Q; the loops are grid-strided)
+	static_assert(SMALL_BATCH_Q % 32 == 0 && SMALL_BATCH_Q <= 1024, "one CTA of whole warps");
+	const unsigned qt = SMALL_BATCH_Q;
 	PST_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
 	PST_CUDA(cudaMemsetAsync(counts, 0, (size_t) max_q * 8, s));
 	PST_CUDA(cudaMemsetAsync(cursor, 0, (size_t) max_q * 8, s));
