@@ -96,3 +96,22 @@ def test_recursive_reference_drops_points_under_ties(oracle):
         short += len(got) < len(want)
     assert short > 0
     rec.close()
+
+
+@pytest.mark.parametrize("dt", ["f32", "f64", "i32"])
+@pytest.mark.parametrize("dup", [False, True])
+def test_ips_equals_two_sided_left(oracle, dt, dup):
+    """The interval scan's stabbing query dim1 <= v <= dim2
+    (interval-parallel-search/interval-parallel-search.h:94-96) is the PST's
+    2-sided-left search (v, v): the oracle's two answers and brute force agree,
+    at values drawn from the points' own bounds (ties on both sides)."""
+    pts = rand_points(5000, dt, ids="arange", dup=dup, seed=61)
+    tree = oracle.Orc.build(pts, dt)
+    rng = np.random.default_rng(62)
+    vals = list(rng.choice(pts["dim1"], 8)) + list(rng.choice(pts["dim2"], 8))
+    for v in vals:
+        ips = np.sort(oracle.Orc.ips(pts, dt, v))
+        pst = np.sort(oracle.Orc.search_ids(tree, "left", 0, v, v).astype(np.uint64))
+        brute = np.sort(oracle.Orc.brute(pts, dt, "left", 0, v, v))
+        assert np.array_equal(ips, pst) and np.array_equal(ips, brute), v
+        assert len(ips) > 0  # v is some point's bound, so that point is reported
