@@ -3,7 +3,7 @@
 Workload (one "step" = one batched launch): 4096 queries (50% 3-sided, 25% 2-sided
 left, 25% 2-sided right) with target selectivities log-uniform in [1e-7, 1e-2], on
 a resident tree of 2^28 float32 points with uint32 ids, dim1 ~ U[0, 2^24) and
-dim2 = dim1 + U[0, 2^16) (seeded synthetic data; the tree alone is ~9 GB, far
+dim2 = dim1 + U[0, 2^16) (seeded synthetic data; the tree alone is 7.1 GiB, far
 larger than L2, so no flush is needed between steps).  Query bounds are fixed
 once by bisection on exact counts.
 
@@ -781,7 +781,7 @@ def main():
                 "config": {"workload": "batched-4096-mixed-queries-2^28-f32", "n_points": n, "ids": "u32",
                            "queries_per_step": NQ, "mix": "50% three / 25% left / 25% right",
                            "selectivity": [SEL_LO, SEL_HI], "results": "ids",
-                           "l2": "inputs larger than L2 (tree ~9 GB)", "parallelism": f"{world} independent shards"},
+                           "l2": "inputs larger than L2 (tree 7.1 GiB)", "parallelism": f"{world} independent shards"},
                 "queries_per_s": qps, "points_per_step": total,
                 "frontier": {k: frontier[k] for k in ("records", "seeds", "boundary")},
                 "plain_queries_per_s": plain_qps, "batched_vs_plain_qps": qps / world / plain_qps,

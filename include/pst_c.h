@@ -133,8 +133,9 @@ pst_status pst_export(const pst_tree *tree, void *dim1, void *dim2, void *med, u
                       uint8_t *bitcodes);
 
 /* One query, drop-in mode: allocates the result (exactly *count records, from the
- * library's stream-ordered result pool; the caller frees it with cudaFree, which
- * accepts pool memory without synchronising), blocks until the result is
+ * library's stream-ordered result pool; the caller frees it with cudaFree as the
+ * reference's callers do, or with cudaFreeAsync on a stream to avoid the
+ * device-wide synchronisation cudaFree may take), blocks until the result is
  * complete, and sets *out_d = NULL, *count = 0 for an empty tree or an empty
  * result.  Replaces StaticPSTGPU::threeSidedSearch / twoSidedLeftSearch /
  * twoSidedRightSearch (pst/static-pst-gpu.h:103-128, pst/static-pst-gpu.tu:496-642)
@@ -170,13 +171,15 @@ pst_status pst_search_into(pst_tree *tree, const pst_query *query, pst_ret ret, 
  * synchronisation of cudaMalloc/cudaFree.  Its working memory is a static 8 MiB
  * device array in the library (held by every GPU that loads it until the process
  * exits), which bounds the tree: at most 2^22 - 1 = 4,194,303 points, larger trees
- * are rejected with PST_ERR_CAPACITY before any work.  The result contract is
+ * are rejected with PST_ERR_CAPACITY before any work.  The tree must live on the
+ * current device (PST_ERR_INVALID otherwise).  The result contract is
  * pst_search_into's: *count is the full size, PST_ERR_CAPACITY (nothing written)
  * when it exceeds `capacity`.  Blocks until complete.  The first call on a device
- * looks up the array's device address; make that first call before any stream
- * capture.  All calls on a device share the array, so calls whose GPU work
- * overlapped would race; calls from one process are serialised (each holds a lock
- * until its work has completed). */
+ * (and the first after a cudaDeviceReset) looks up the array's device address;
+ * make that first call before any stream capture begins.  All calls on a device
+ * share the array, so calls whose GPU work overlapped would race; calls from one
+ * process are serialised (each holds a lock until its work has completed, also
+ * when it fails). */
 pst_status pst_search_noalloc(pst_tree *tree, const pst_query *query, pst_ret ret, void *out_d,
                               uint64_t capacity, uint64_t *count, pst_stream_t stream);
 

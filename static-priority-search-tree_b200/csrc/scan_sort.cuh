@@ -128,8 +128,10 @@ void exclusive_scan(const T *in, U *out, uint64_t n, T *tmp, T *total_d, cudaStr
 }
 
 // ---------------------------------------------------------------------------
-// LSD radix sort, 8-bit digits, 4096-key tiles, one kernel per digit pass
-// ("onesweep"): a first kernel histograms the digits of every pass at once; in a
+// LSD radix sort, 8-bit digits, 4096-key tiles, one kernel per digit pass: the
+// single-pass scheme of Adinets and Merrill, "Onesweep: A Faster Least Significant
+// Digit Radix Sort for GPUs" (2022), written for this library.  A first kernel
+// histograms the digits of every pass at once; in a
 // pass, each tile ranks its keys stably (warp-private digit counters; the lanes of
 // a warp holding the same digit are found with eight ballots, one per digit bit),
 // publishes its digit counts, and finds the counts of all earlier tiles by walking

@@ -27,6 +27,8 @@
 #include <type_traits>
 #include <vector>
 
+#include <cuda.h>
+
 #include "scan_sort.cuh"
 #include "search.cuh"
 
@@ -1210,21 +1212,70 @@ static_assert(NA_RECS + NA_REC_CAP * sizeof(uint4) <= NOALLOC_SCRATCH_BYTES, "sc
 static_assert((1ull << NOALLOC_MAX_LEVELS) / 32 + 14 * NOALLOC_MAX_LEVELS + 64 <= NA_REC_CAP, "frontier bound");
 
 std::mutex g_noalloc_mu;
-unsigned char *g_noalloc_ptr[64] = {};
 
-// Device address of the scratch array for the current device, looked up once per
-// device with that device current (the host-side name of a __device__ array is only
-// a stand-in for it).
+// The scratch array's device address per device, with the id of the context it was
+// looked up in.  cudaDeviceReset ends that context (and the array with it); the next
+// call on the device, in the new context, looks the address up again.
+struct NoallocSlot {
+	unsigned long long ctx = 0;
+	unsigned char *ptr = nullptr;
+};
+NoallocSlot g_noalloc_slot[64];
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+
+// Unique id of the calling thread's current context, made current first for device
+// `dev` when the thread has none yet (the library does not link the driver library
+// itself: the two driver calls come from the runtime's entry points).
+unsigned long long current_context_id(int dev)
+{
+	static CtxGetCurrentFn get_cur = nullptr;
+	static CtxGetIdFn get_id = nullptr;
+	static std::once_flag once;
+	std::call_once(once, [] {
+		void *p = nullptr;
+		cudaDriverEntryPointQueryResult q{};
+		if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+		    q == cudaDriverEntryPointSuccess)
+			get_cur = reinterpret_cast<CtxGetCurrentFn>(p);
+		p = nullptr;
+		if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+		    q == cudaDriverEntryPointSuccess)
+			get_id = reinterpret_cast<CtxGetIdFn>(p);
+		cudaGetLastError();
+	});
+	if (!get_cur || !get_id)
+		fail(PST_ERR_CUDA, "driver entry points cuCtxGetCurrent / cuCtxGetId are unavailable");
+	CUcontext c = nullptr;
+	if (get_cur(&c) == CUDA_SUCCESS && !c) {
+		// a thread that has made no other CUDA call: cudaSetDevice makes the device's
+		// primary context current on it
+		check_cuda(cudaSetDevice(dev), "cudaSetDevice");
+		get_cur(&c);
+	}
+	unsigned long long id = 0;
+	if (!c || get_id(c, &id) != CUDA_SUCCESS)
+		fail(PST_ERR_CUDA, "no current CUDA context");
+	return id;
+}
+
+// Device address of the scratch array for device `dev`, which must be current
+// (the host-side name of a __device__ array is only a stand-in for it): looked up
+// once per device and context.
 unsigned char *noalloc_scratch(int dev)
 {
 	if (dev < 0 || dev >= 64)
 		fail(PST_ERR_CUDA, "device index out of range");
-	if (!g_noalloc_ptr[dev]) {
+	const unsigned long long ctx = current_context_id(dev);
+	NoallocSlot &slot = g_noalloc_slot[dev];
+	if (!slot.ptr || slot.ctx != ctx) {
 		void *p = nullptr;
 		check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(no-alloc scratch)");
-		g_noalloc_ptr[dev] = static_cast<unsigned char *>(p);
+		slot.ptr = static_cast<unsigned char *>(p);
+		slot.ctx = ctx;
 	}
-	return g_noalloc_ptr[dev];
+	return slot.ptr;
 }
 
 template <typename T>
@@ -1309,15 +1360,26 @@ uint64_t search_noalloc(TreeStorage &t, const pst_query &q, pst_ret ret, void *o
 		                           std::to_string(t.n));
 	int dev = 0;
 	PST_CUDA(cudaGetDevice(&dev));
+	if (t.device != dev)
+		fail(PST_ERR_INVALID, "the tree lives on device " + std::to_string(t.device) + " but device " +
+		                          std::to_string(dev) + " is current");
 	// Every call on a device shares the one array, so two calls whose GPU work
 	// overlapped would race on it; within this process the lock, held until the
 	// call's work has completed, keeps calls from overlapping.
 	std::lock_guard<std::mutex> lk(g_noalloc_mu);
 	unsigned char *base = noalloc_scratch(dev);
-	switch (t.dtype) {
-	case PST_F32: return noalloc_run<float>(t, q, ret, out, capacity, s, base);
-	case PST_F64: return noalloc_run<double>(t, q, ret, out, capacity, s, base);
-	case PST_I32: return noalloc_run<int32_t>(t, q, ret, out, capacity, s, base);
+	try {
+		switch (t.dtype) {
+		case PST_F32: return noalloc_run<float>(t, q, ret, out, capacity, s, base);
+		case PST_F64: return noalloc_run<double>(t, q, ret, out, capacity, s, base);
+		case PST_I32: return noalloc_run<int32_t>(t, q, ret, out, capacity, s, base);
+		}
+	} catch (...) {
+		// kernels enqueued before the failure may still be using the array: let them
+		// finish before the lock is released and another call rewrites it
+		cudaStreamSynchronize(s);
+		cudaGetLastError();
+		throw;
 	}
 	fail(PST_ERR_INVALID, "bad dtype");
 }

@@ -1,9 +1,9 @@
 """pst_search_noalloc: the single-query search that allocates nothing (its working
 memory is the library's static 8 MiB device array), for callers that cannot
 allocate device memory while they search.  Checked through the C ABI against the
-existing pst_search_into on the same tree and queries, two calls in a row each
-(the array keeps the previous call's contents, so the second call checks that
-everything that must start at zero is reset)."""
+existing pst_search_into on the same tree and queries and against the CPU oracle,
+two calls in a row each (the array keeps the previous call's contents, so the
+second call checks that everything that must start at zero is reset)."""
 import ctypes as C
 
 import numpy as np
@@ -44,8 +44,11 @@ def test_noalloc_equals_search_into(pst, oracle, dt):
     noalloc, into = _entry_points(pst)
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     n = len(pts)
+    ref = oracle.Orc.build(pts, dt)
     for kind, a, b, m2 in rand_queries(pts, 6, seed=32):
         q = _query(pst, dt, kind, a, b, m2)
+        expect = {"ids": oracle.canon(oracle.Orc.search_ids(ref, kind, a, b, m2)),
+                  "points": oracle.canon(oracle.Orc.search_points(ref, kind, a, b, m2))}
         for ret, rec in (("ids", np.dtype(np.uint32)), ("points", pts.dtype)):
             rsz = rec.itemsize
             buf = torch.empty(n * rsz + 16, dtype=torch.uint8, device="cuda")
@@ -53,6 +56,7 @@ def test_noalloc_equals_search_into(pst, oracle, dt):
             assert into(tree.handle, C.byref(q), pst.pst.RET[ret], C.c_void_p(buf.data_ptr()), n, C.byref(cnt),
                         stream) == PST_OK
             want = _canon(oracle, buf[: cnt.value * rsz].cpu().numpy(), rec)
+            assert np.array_equal(want, expect[ret]), (kind, ret)
             for _ in range(2):
                 out = torch.full((n * rsz + 16,), 0xAB, dtype=torch.uint8, device="cuda")
                 c2 = C.c_uint64()
