@@ -39,7 +39,11 @@ UNIT = "pts/s"
 N_POINTS = 1 << 28
 NQ = 4096
 SEL_LO, SEL_HI = 1e-7, 1e-2
-BYTES_PER_PT = 12  # dim2 tested (4) + id read (4) + id written (4), float32 tree returning ids
+# Algorithmic bytes per reported point, float32 tree returning ids: dim1 and dim2
+# read (4 + 4), id read (4), id written (4).  A point inside a report-above subtree
+# needs no dim1 test, so the search can move as little as 12 B per point.
+BYTES_PER_PT = 16
+BYTES_PER_PT_MIN = 12
 
 
 _T0 = time.perf_counter()
@@ -88,6 +92,23 @@ def gen_points_device(n, seed, torch):
     return rec
 
 
+def gen_points_exp_device(n, seed, torch, mean_gap=0.01):
+    """(n, 3) int32 tensor of PointStruct<float, uint32_t, 1> records of the
+    batched-queries distribution: dim1 ~ U[0, 1), dim2 = dim1 + Exp(mean 0.01)
+    (float32 add, rounded once), ids 0..n-1."""
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    d1 = torch.rand(n, generator=g, device="cuda", dtype=torch.float32)
+    gap = torch.empty(n, device="cuda", dtype=torch.float32).exponential_(1.0 / mean_gap, generator=g)
+    d2 = d1 + gap
+    rec = torch.empty((n, 3), dtype=torch.int32, device="cuda")
+    rec[:, 0] = d1.view(torch.int32)
+    rec[:, 1] = d2.view(torch.int32)
+    rec[:, 2] = torch.arange(n, device="cuda", dtype=torch.int32)
+    del d1, d2, gap
+    return rec
+
+
 def gen_points_host(n, seed):
     rng = np.random.default_rng(seed)
     d1 = (rng.random(n, dtype=np.float32) * np.float32(1 << 24)).astype(np.float32)
@@ -108,22 +129,24 @@ def query_plan(nq, seed):
     return kinds, sel, anchor
 
 
-def calibrate(count_fn, kinds, sel, anchor, n, iters=24, domain=float(1 << 24)):
+def calibrate(count_fn, kinds, sel, anchor, n, iters=24, domain=float(1 << 24), spread=float(1 << 16)):
     """Bisection of each query's free bound so that its exact count is ~sel * n,
     over brackets that keep every trial count within ~4x of the target (a trial
-    never asks for a large fraction of the tree).  dim1 ~ U[0, domain),
-    dim2 = dim1 + U[0, 2^16).
+    never asks for a large fraction of the tree).  dim1 ~ U[0, domain) and
+    dim2 - dim1 in [0, spread) (U[0, 2^16) for the large random trees; for the
+    exponential gaps of the batched-queries distribution, a bound its largest gap
+    stays below):
       3-sided [a, a + W] with min2 = a: W free in [0, 4 s domain];
-      left (b, c): dim2 bound c free in [b - 2 s domain - 2^16, b + 2^16];
-      right (a, c): c free in [max(a, domain - 2 s domain - 2^16), domain + 2^16].
+      left (b, c): dim2 bound c free in [b - 2 s domain - spread, b + spread];
+      right (a, c): c free in [max(a, domain - 2 s domain - spread), domain + spread].
     count_fn(kinds, min1, max1, min2) -> exact counts."""
     nq = len(kinds)
     target = sel * n
     three, left, right = kinds == 0, kinds == 1, kinds == 2
-    w = 1 << 16
+    w = spread
     lo = np.where(three, 0.0, np.where(left, anchor - 2 * sel * domain - w,
                                         np.maximum(anchor, domain - 2 * sel * domain - w)))
-    hi = np.where(three, 4 * sel * domain + 64, np.where(left, anchor + w, domain + w))
+    hi = np.where(three, 4 * sel * domain + 64 * domain / (1 << 24), np.where(left, anchor + w, domain + w))
     best = (lo + hi) / 2
     best_err = np.full(nq, np.inf)
 
@@ -144,6 +167,110 @@ def calibrate(count_fn, kinds, sel, anchor, n, iters=24, domain=float(1 << 24)):
         lo = np.where(grow, mid, lo)
         hi = np.where(grow, hi, mid)
     return bounds(best)
+
+
+def disjoint_plan(nq, seed, domain=float(1 << 24)):
+    """nq 3-sided queries over consecutive, disjoint dim1 ranges that cover the whole
+    domain, with min2 = the range's lower bound, so every point is reported by
+    exactly one query (dim2 >= dim1 >= the bound): no point is read for two queries.
+    Range widths are proportional to log-uniform weights on [1e-7, 1e-2], so the
+    output sizes are as uneven as in the mixed plan.  Returns (kinds, min1, max1,
+    min2) in float32."""
+    rng = np.random.default_rng(seed)
+    w = np.exp(rng.uniform(np.log(SEL_LO), np.log(SEL_HI), nq))
+    edges = (np.concatenate([[0.0], np.cumsum(w / w.sum())]) * domain).astype(np.float32)
+    edges[0] = np.float32(-np.inf)
+    a = edges[:-1]
+    # each range ends just below where the next one starts (bounds are inclusive)
+    b = np.nextafter(edges[1:], np.float32(-np.inf)).astype(np.float32)
+    b[-1] = np.float32(np.inf)
+    return np.zeros(nq, np.int32), a, b, a.copy()
+
+
+def time_pass(eng, q_dev, out, offs, steps, warmup, stream, torch):
+    """Mean device time (CUDA events on the launching stream) of `steps` batched
+    passes over device-resident queries, after `warmup` untimed ones."""
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for _ in range(warmup):
+        eng.run(q_dev, out, offs, queries_on_device=True, sync=False)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(steps):
+        ev[0].record(stream)
+        eng.run(q_dev, out, offs, queries_on_device=True, sync=False)
+        ev[1].record(stream)
+        ev[1].synchronize()
+        ms.append(ev[0].elapsed_time(ev[1]))
+    return statistics.mean(ms)
+
+
+def construct_roofline(n, ms, peak, peak_kind, val_bytes=4, id_bytes=4, key_bits=32, digit_bits=8):
+    """Construction against HBM with the algorithmic bytes of the path's definition:
+    the index sorts, ceil(key_bits / digit_bits) radix passes of n (key + u32 index)
+    pairs read and written (16 B per point and pass for 4-byte keys), plus population,
+    ceil(log2(n + 1)) levels of an index read and written per point and one write
+    of every slot (three values, id, bitcode)."""
+    levels = int(n).bit_length()
+    slots = (1 << levels) - 1
+    passes = -(-key_bits // digit_bits)
+    sort_b = passes * n * 2 * (val_bytes + 4)
+    pop_b = levels * 8 * n + slots * (3 * val_bytes + id_bytes + 1)
+    ach = (sort_b + pop_b) / (ms / 1000.0) / 1e9
+    return {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+            "traffic": None, "algorithmic_bytes": sort_b + pop_b, "sort_bytes": sort_b, "populate_bytes": pop_b,
+            "peak_source": f"{peak_kind} hbm_gbs"}
+
+
+def batched_queries_config(pst, torch, stream, steps, warmup, n=1 << 26, seed=3, plain_n=NQ):
+    """The batched-queries configuration: one tree of 2^26 float32 points, dim1 ~
+    U[0,1), dim2 = dim1 + Exp(mean 0.01); 4096 queries per pass (50 % 3-sided, 25 %
+    left, 25 % right, selectivities log-uniform in [1e-7, 1e-2], bounds bisected on
+    exact counts); the batched pass against the same 4096 queries as plain drop-in
+    launches, one blocking call each."""
+    rec = gen_points_exp_device(n, seed, torch)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    tree = pst.StaticPSTGPU(rec, n, "f32", True)
+    torch.cuda.synchronize()
+    build_ms = 1000 * (time.perf_counter() - t0)
+    del rec
+    eng = pst.BatchEngine(tree, max_queries=NQ, task_capacity=n >> 2)
+    kinds, sel, anchor = query_plan(NQ, 9)
+    anchor = anchor / float(1 << 24)
+
+    def count_fn(k, a, b, c):
+        return eng.count(pst.make_queries(k, a, b, c, "f32"))[0].cpu().numpy()
+    min1, max1, min2 = calibrate(count_fn, kinds, sel, anchor, n, domain=1.0, spread=0.25)
+    q_host = pst.make_queries(kinds, min1, max1, min2, "f32")
+    _, total = eng.count(q_host)
+    q_dev = torch.from_numpy(q_host.view(np.uint8).copy()).to("cuda")
+    out = torch.empty(total * 4 + 16, dtype=torch.uint8, device="cuda")
+    offs = torch.empty(NQ + 1, dtype=torch.int64, device="cuda")
+    st, tot = eng.run(q_dev, out, offs, queries_on_device=True, sync=True)
+    assert st == 0 and tot == total
+    ms = time_pass(eng, q_dev, out, offs, steps, warmup, stream, torch)
+    names = {0: "three", 1: "left", 2: "right"}
+    m = min(plain_n, NQ)
+    pst.free_device(tree.search_device(names[int(kinds[0])], min1[0], max1[0], min2[0])[0])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain_pts = 0
+    for i in range(m):
+        ptr, c = tree.search_device(names[int(kinds[i])], min1[i], max1[i], min2[i])
+        pst.free_device(ptr)
+        plain_pts += c
+    plain_s = time.perf_counter() - t0
+    eng.close()
+    tree.close()
+    del out, q_dev
+    torch.cuda.empty_cache()
+    return {"workload": "batched-4096-mixed-queries-2^26-f32-exp", "n_points": n,
+            "distribution": "dim1 ~ U[0,1), dim2 = dim1 + Exp(mean 0.01)", "queries_per_pass": NQ,
+            "points_per_pass": int(total), "batched_ms": ms, "batched_pts_per_s": total / (ms / 1000.0),
+            "batched_queries_per_s": NQ / (ms / 1000.0), "plain_queries": m, "plain_s": plain_s,
+            "plain_queries_per_s": m / plain_s, "plain_points": int(plain_pts),
+            "batched_vs_plain_qps": (NQ / (ms / 1000.0)) / (m / plain_s), "build_ms": build_ms,
+            "bytes_per_pt": BYTES_PER_PT}
 
 
 def blob_volume_device(px, py, pz, seed, torch, nblobs=32, noise=0.01):
@@ -589,6 +716,7 @@ def main():
     ap.add_argument("--points-log2", type=int, default=28)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the 2^26 batched-queries configuration")
     ap.add_argument("--plain-queries", type=int, default=256)
     ap.add_argument("--sweep", action="store_true", help="also run every value type x kind x selectivity")
     ap.add_argument("--isosurface", action="store_true", help="also run the 512^3 isosurface pipeline")
@@ -721,20 +849,52 @@ def main():
     plain_qps = plain_n / plain_s
     log(f"plain per-query path: {plain_qps:.1f} queries/s")
 
+    # ---- the same tree, queries over disjoint dim1 ranges: every point reported
+    # exactly once per pass, so no row is read for two queries (no L2 reuse between
+    # queries); the pass's HBM efficiency without overlap
+    dk, da, db, dc = disjoint_plan(NQ, 13)
+    dq_host = pst.make_queries(dk, da, db, dc, "f32")
+    dq_dev = torch.from_numpy(dq_host.view(np.uint8).copy()).to("cuda")
+    st_d, tot_d = eng.run(dq_dev, out, offs, queries_on_device=True, sync=True)
+    assert st_d == 0 and tot_d == n, (st_d, tot_d)  # each point exactly once
+    dis_ms = time_pass(eng, dq_dev, out, offs, max(3, args.steps // 2), args.warmup, stream, torch)
+    log(f"disjoint ranges: {dis_ms:.3f} ms/pass for {tot_d} points")
+
     # ---- roofline of the batched search pass
     peak, peak_kind = measured_peak()
     achieved = total * BYTES_PER_PT / (my_ms / 1000.0) / 1e9
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None, "kernel": "batched search pass (k_bfs_level x levels + scan + k_emit)",
-            "bytes_per_unit": BYTES_PER_PT, "units_per_launch": total, "peak_source": f"{peak_kind} hbm_gbs"}
+            "bytes_per_unit": BYTES_PER_PT, "units_per_launch": total, "peak_source": f"{peak_kind} hbm_gbs",
+            "frac_at_min_bytes": total * BYTES_PER_PT_MIN / (my_ms / 1000.0) / 1e9 / peak,
+            "min_bytes_per_unit": BYTES_PER_PT_MIN}
+    dis_ach = tot_d * BYTES_PER_PT / (dis_ms / 1000.0) / 1e9
+    disjoint = {"workload": "batched-4096-disjoint-3-sided-2^28-f32", "points_per_pass": int(tot_d),
+                "ms_per_pass": dis_ms, "pts_per_s": tot_d / (dis_ms / 1000.0),
+                "roofline": {"bound": "hbm", "achieved": dis_ach, "peak": peak, "unit": "GB/s",
+                             "frac": dis_ach / peak, "traffic": None, "bytes_per_unit": BYTES_PER_PT,
+                             "units_per_launch": int(tot_d),
+                             "frac_at_min_bytes": tot_d * BYTES_PER_PT_MIN / (dis_ms / 1000.0) / 1e9 / peak,
+                             "peak_source": f"{peak_kind} hbm_gbs"}}
     prof = ROOT / "profiles" / "search_traffic.json"
     if prof.exists() and n == N_POINTS:
         try:
             tr = json.loads(prof.read_text())
             roof["traffic"] = tr["search_bytes_per_step"]
             roof["traffic_source"] = f"ncu dram bytes on {tr['measured_on']}, scaled to {tr['scaled_to']}"
+            if "disjoint_bytes_per_pass" in tr:
+                disjoint["roofline"]["traffic"] = tr["disjoint_bytes_per_pass"]
+                disjoint["roofline"]["traffic_source"] = tr["disjoint_source"]
         except Exception:
             pass
+    del dq_dev
+
+    batched_cfg = None
+    if rank == 0 and not args.no_extra:
+        batched_cfg = batched_queries_config(pst, torch, stream, max(3, args.steps // 2), args.warmup)
+        log("batched-queries configuration (2^26, exponential gaps): {:.3f} ms/pass, {:.3g} pts/s, "
+            "{:.0f}x the plain launches in queries/s".format(batched_cfg["batched_ms"], batched_cfg["batched_pts_per_s"],
+                                                            batched_cfg["batched_vs_plain_qps"]))
 
     sweep_rows = None
     if rank == 0 and args.sweep:
@@ -786,6 +946,9 @@ def main():
                 "frontier": {k: frontier[k] for k in ("records", "seeds", "boundary")},
                 "plain_queries_per_s": plain_qps, "batched_vs_plain_qps": qps / world / plain_qps,
                 "construct_ms": construct_ms, "construct_first_ms": construct_cold_ms, "construct_pts_per_s": n / (construct_ms / 1000.0),
+                "construct": {"ms": construct_ms, "points": n,
+                              "roofline": construct_roofline(n, construct_ms, peak, peak_kind)},
+                "disjoint": disjoint, "batched_queries_config": batched_cfg,
                 "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(q_host.nbytes),
                         "d2h_bytes_per_step": int(total * 4 + (NQ + 1) * 8)},
                 "gpu_launches": None, "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),

@@ -113,6 +113,10 @@ class Orc:
                 f = getattr(lib, f"orc_ips_{sfx}")
                 f.restype = C.c_int64
                 f.argtypes = [C.c_void_p, C.c_size_t, C.c_uint64, ct, C.c_void_p]
+                f = getattr(lib, f"orc_brute_multi_{sfx}")
+                f.restype = C.c_int64
+                f.argtypes = [C.c_void_p, C.c_size_t, C.c_uint64, C.c_uint32] + [C.c_void_p] * 4 + \
+                    [C.c_int, C.c_void_p, C.c_void_p]
                 f = getattr(lib, f"orc_metacells_{sfx}")
                 f.restype = C.c_int64
                 f.argtypes = [C.c_void_p] + [C.c_uint32] * 6 + [C.c_void_p] * 3
@@ -162,6 +166,30 @@ class Orc:
         cnt = getattr(cls.lib(), f"orc_brute_{dt}")(
             _ptr(pts), pts.dtype.itemsize, len(pts), KINDS[kind], min1, max1, min2, _ptr(out))
         return out[:cnt]
+
+    @classmethod
+    def brute_multi(cls, pts: np.ndarray, dt: str, kinds, min1, max1, min2, threads: int | None = None):
+        """Brute force of many queries in one threaded pass over the points (for large
+        point sets): returns (offsets[nq + 1], input indices), each query's indices in
+        index order."""
+        pts = np.ascontiguousarray(pts)
+        t = DTYPES[dt]
+        k = np.ascontiguousarray(np.asarray(kinds, np.int32))
+        a, b, c = (np.ascontiguousarray(np.asarray(x, t)) for x in (min1, max1, min2))
+        nq = len(k)
+        th = threads or os.cpu_count() or 1
+        off = np.zeros(nq + 1, np.uint64)
+        fn = getattr(cls.lib(), f"orc_brute_multi_{dt}")
+        tot = fn(_ptr(pts), pts.dtype.itemsize, len(pts), nq, _ptr(k), _ptr(a), _ptr(b), _ptr(c), th, _ptr(off),
+                 None)
+        if tot < 0:
+            raise RuntimeError("oracle brute_multi failed")
+        idx = np.zeros(max(int(tot), 1), np.uint64)
+        tot2 = fn(_ptr(pts), pts.dtype.itemsize, len(pts), nq, _ptr(k), _ptr(a), _ptr(b), _ptr(c), th, _ptr(off),
+                  _ptr(idx))
+        if tot2 != tot:
+            raise RuntimeError("oracle brute_multi failed")
+        return off, idx[:tot]
 
     @classmethod
     def ips(cls, pts: np.ndarray, dt: str, v) -> np.ndarray:

@@ -26,6 +26,7 @@
  * The "address" tiebreak of the reference (comparisonTiebreaker compares
  * this-pointers inside one contiguous array) is the input index here.
  */
+#include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -389,3 +390,116 @@ int64_t orc_metacells_##SFX(const T *vol, uint32_t px, uint32_t py, uint32_t pz,
 ORACLE_DEFINE(f32, float)
 ORACLE_DEFINE(f64, double)
 ORACLE_DEFINE(i32, int32_t)
+
+/*
+ * Brute force of many queries over one point set at once (the same predicates as
+ * orc_brute_*), for checking large trees: the points are read once per pass
+ * instead of once per query.  Threads take contiguous point ranges; pass 1 counts
+ * each (thread, query) pair over blocks of BRUTE_BLOCK points, pass 2 writes the
+ * input indices of each query's hits, in index order, at out_off[q].
+ * out_off receives nq + 1 offsets (exclusive scan of the per-query counts);
+ * out_idx (may be NULL: counts only) must hold out_off[nq] entries.
+ * Returns the total number of hits, or -1 when a thread or buffer cannot be had.
+ */
+#define BRUTE_BLOCK 2048
+
+#define BRUTE_MULTI_DEFINE(SFX, T)                                                             \
+typedef struct {                                                                               \
+	const unsigned char *pts; size_t stride; uint64_t lo, hi;                                  \
+	uint32_t nq; const int32_t *kinds; const T *min1, *max1, *min2;                           \
+	uint64_t *cnt;        /* nq counts of this thread (pass 1) */                               \
+	uint64_t *pos;        /* nq write positions of this thread (pass 2) */                      \
+	uint64_t *out_idx;                                                                         \
+	int pass;                                                                                  \
+} bm_##SFX;                                                                                    \
+                                                                                               \
+static void *bm_run_##SFX(void *arg)                                                           \
+{                                                                                              \
+	bm_##SFX *a = (bm_##SFX *) arg;                                                            \
+	T v1[BRUTE_BLOCK], v2[BRUTE_BLOCK];                                                        \
+	for (uint64_t b = a->lo; b < a->hi; b += BRUTE_BLOCK) {                                    \
+		const uint64_t m = a->hi - b < BRUTE_BLOCK ? a->hi - b : BRUTE_BLOCK;                  \
+		for (uint64_t i = 0; i < m; i++) {                                                     \
+			memcpy(&v1[i], a->pts + (b + i) * a->stride, sizeof(T));                           \
+			memcpy(&v2[i], a->pts + (b + i) * a->stride + sizeof(T), sizeof(T));               \
+		}                                                                                      \
+		for (uint32_t q = 0; q < a->nq; q++) {                                                 \
+			const int k = a->kinds[q];                                                         \
+			const T m2 = a->min2[q];                                                           \
+			const int use_lo = k != ORC_Q_LEFT, use_hi = k != ORC_Q_RIGHT;                     \
+			if (a->pass == 1) {                                                                \
+				uint64_t c = 0;                                                                \
+				for (uint64_t i = 0; i < m; i++)                                               \
+					c += (m2 <= v2[i]) & (!use_lo | (a->min1[q] <= v1[i]))                     \
+					     & (!use_hi | (v1[i] <= a->max1[q]));                                  \
+				a->cnt[q] += c;                                                                \
+			} else {                                                                           \
+				uint64_t w = a->pos[q];                                                        \
+				for (uint64_t i = 0; i < m; i++)                                               \
+					if ((m2 <= v2[i]) & (!use_lo | (a->min1[q] <= v1[i]))                      \
+					    & (!use_hi | (v1[i] <= a->max1[q])))                                   \
+						a->out_idx[w++] = b + i;                                               \
+				a->pos[q] = w;                                                                 \
+			}                                                                                  \
+		}                                                                                      \
+	}                                                                                          \
+	return NULL;                                                                               \
+}                                                                                              \
+                                                                                               \
+int64_t orc_brute_multi_##SFX(const void *pts, size_t stride, uint64_t n, uint32_t nq,        \
+                              const int32_t *kinds, const T *min1, const T *max1,              \
+                              const T *min2, int threads, uint64_t *out_off,                   \
+                              uint64_t *out_idx)                                               \
+{                                                                                              \
+	if (threads < 1) threads = 1;                                                              \
+	if ((uint64_t) threads > n / BRUTE_BLOCK + 1) threads = (int) (n / BRUTE_BLOCK + 1);       \
+	bm_##SFX *job = calloc((size_t) threads, sizeof(bm_##SFX));                                \
+	pthread_t *th = calloc((size_t) threads, sizeof(pthread_t));                               \
+	uint64_t *cnt = calloc((size_t) threads * (nq ? nq : 1), sizeof(uint64_t));                \
+	uint64_t *pos = calloc((size_t) threads * (nq ? nq : 1), sizeof(uint64_t));                \
+	int64_t total = -1;                                                                        \
+	if (!job || !th || !cnt || !pos)                                                           \
+		goto done;                                                                             \
+	const uint64_t per = (n + (uint64_t) threads - 1) / (uint64_t) threads;                    \
+	for (int t = 0; t < threads; t++) {                                                        \
+		uint64_t lo = per * (uint64_t) t, hi = lo + per;                                       \
+		if (lo > n) lo = n;                                                                    \
+		if (hi > n) hi = n;                                                                    \
+		job[t] = (bm_##SFX) { (const unsigned char *) pts, stride, lo, hi, nq, kinds, min1,    \
+		                      max1, min2, cnt + (size_t) t * nq, pos + (size_t) t * nq,        \
+		                      out_idx, 1 };                                                    \
+	}                                                                                          \
+	for (int pass = 1; pass <= (out_idx ? 2 : 1); pass++) {                                    \
+		int started = 0;                                                                       \
+		for (int t = 0; t < threads; t++) {                                                    \
+			job[t].pass = pass;                                                                \
+			if (pthread_create(&th[t], NULL, bm_run_##SFX, &job[t]) != 0)                      \
+				break;                                                                         \
+			started++;                                                                         \
+		}                                                                                      \
+		for (int t = 0; t < started; t++)                                                      \
+			pthread_join(th[t], NULL);                                                         \
+		if (started < threads)                                                                 \
+			goto done;                                                                         \
+		if (pass == 1) {                                                                       \
+			/* query q's hits: thread 0's, then thread 1's, ... (index order) */              \
+			uint64_t acc = 0;                                                                  \
+			for (uint32_t q = 0; q < nq; q++) {                                                \
+				out_off[q] = acc;                                                              \
+				for (int t = 0; t < threads; t++) {                                            \
+					pos[(size_t) t * nq + q] = acc;                                            \
+					acc += cnt[(size_t) t * nq + q];                                           \
+				}                                                                              \
+			}                                                                                  \
+			out_off[nq] = acc;                                                                 \
+			total = (int64_t) acc;                                                             \
+		}                                                                                      \
+	}                                                                                          \
+done:                                                                                          \
+	free(job); free(th); free(cnt); free(pos);                                                 \
+	return total;                                                                              \
+}
+
+BRUTE_MULTI_DEFINE(f32, float)
+BRUTE_MULTI_DEFINE(f64, double)
+BRUTE_MULTI_DEFINE(i32, int32_t)

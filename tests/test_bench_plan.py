@@ -45,3 +45,17 @@ def test_calibration_reaches_targets():
     got = _brute_counts(pts, kinds, min1, max1, min2)
     err = np.abs(got - sel * n) / (sel * n)
     assert err.max() < 0.01, err  # every query within 1 % of its target count
+
+
+def test_disjoint_plan_reports_every_point_once(oracle):
+    """The disjoint-range workload: 4096 3-sided queries whose results partition the
+    point set (every point reported by exactly one query)."""
+    n = 1 << 16
+    pts = bench.gen_points_host(n, 1)
+    kinds, a, b, c = bench.disjoint_plan(bench.NQ, 13)
+    assert (kinds == 0).all() and np.all(a[1:] > b[:-1])
+    off, idx = oracle.Orc.brute_multi(pts, "f32", kinds, a, b, c)
+    assert int(off[-1]) == n
+    assert np.array_equal(np.sort(idx), np.arange(n, dtype=np.uint64))
+    sizes = np.diff(off.astype(np.int64))
+    assert sizes.max() > 100 * max(np.median(sizes), 1)  # uneven output sizes
