@@ -92,6 +92,58 @@ def gen_points_device(n, seed, torch):
     return rec
 
 
+SLAB = float(1 << 24)  # dim1 width of one shard's slab
+
+
+def slab_points_device(n, rank, torch):
+    """Shard `rank` of the sharded point set (weak scaling: every shard holds 2^28
+    points): the large-random-tree distribution with dim1 ~ U[r 2^24, (r + 1) 2^24)
+    (float32, shifted after drawing), dim2 = dim1 + U[0, 2^16), ids r n ..
+    (r + 1) n - 1.  Shard 0 is the one-GPU workload itself."""
+    rec = gen_points_device(n, seed=1 + rank, torch=torch)
+    if rank:
+        vals = rec[:, :2].view(torch.float32)
+        vals += float(rank) * SLAB
+        rec[:, 2] += rank * n
+    return rec
+
+
+def slab_bounds(rec, torch):
+    """(min dim1, max dim1, max dim2, nonempty) of a (n, 3) float32-with-id slab."""
+    v = rec[:, :2].view(torch.float32)
+    return (float(v[:, 0].min().item()), float(v[:, 0].max().item()), float(v[:, 1].max().item()), 1.0)
+
+
+def sharded_block(count_fn, rank, world, n, seed_base=7):
+    """This shard's block of the global query list: the mixed plan of the one-GPU
+    workload inside the shard's slab, bisected on the shard's own counts.  A
+    2-sided-right query of small selectivity reports a suffix of the dim1 order, so
+    only the last shard keeps its right queries as they are; on every other shard
+    they become 3-sided queries clipped at the slab's top (the same points the right
+    query finds on that shard's slab).  Returns (kinds, min1, max1, min2, sel)."""
+    kinds, sel, anchor = query_plan(NQ, seed_base + rank)
+    origin = float(rank) * SLAB
+    min1, max1, min2 = calibrate(count_fn, kinds, sel, anchor + origin, n, origin=origin)
+    if rank < world - 1:
+        clip = kinds == 2
+        kinds = kinds.copy()
+        kinds[clip] = 0
+        max1 = max1.copy()
+        max1[clip] = np.nextafter(np.float32(origin + SLAB), np.float32(-np.inf))
+    return kinds, min1, max1, min2, sel
+
+
+def query_fields(q, dt="f32"):
+    """(kinds, min1, max1, min2) of a pst_query array, bounds in the value type."""
+    t = {"f32": np.float32, "f64": np.float64, "i32": np.int32}[dt]
+    sz = np.dtype(t).itemsize
+    out = [np.asarray(q["kind"])]
+    for f in ("min1", "max1", "min2"):
+        raw = np.ascontiguousarray(q[f]).view(np.uint8).reshape(-1, 8)[:, :sz]
+        out.append(np.ascontiguousarray(raw).view(t)[:, 0])
+    return out
+
+
 def gen_points_exp_device(n, seed, torch, mean_gap=0.01):
     """(n, 3) int32 tensor of PointStruct<float, uint32_t, 1> records of the
     batched-queries distribution: dim1 ~ U[0, 1), dim2 = dim1 + Exp(mean 0.01)
@@ -129,13 +181,14 @@ def query_plan(nq, seed):
     return kinds, sel, anchor
 
 
-def calibrate(count_fn, kinds, sel, anchor, n, iters=24, domain=float(1 << 24), spread=float(1 << 16)):
+def calibrate(count_fn, kinds, sel, anchor, n, iters=24, domain=float(1 << 24), spread=float(1 << 16), origin=0.0):
     """Bisection of each query's free bound so that its exact count is ~sel * n,
     over brackets that keep every trial count within ~4x of the target (a trial
     never asks for a large fraction of the tree).  dim1 ~ U[0, domain) and
     dim2 - dim1 in [0, spread) (U[0, 2^16) for the large random trees; for the
     exponential gaps of the batched-queries distribution, a bound its largest gap
-    stays below):
+    stays below; a dim1 range that starts at `origin` shifts the brackets of the
+    right queries with it):
       3-sided [a, a + W] with min2 = a: W free in [0, 4 s domain];
       left (b, c): dim2 bound c free in [b - 2 s domain - spread, b + spread];
       right (a, c): c free in [max(a, domain - 2 s domain - spread), domain + spread].
@@ -144,9 +197,10 @@ def calibrate(count_fn, kinds, sel, anchor, n, iters=24, domain=float(1 << 24), 
     target = sel * n
     three, left, right = kinds == 0, kinds == 1, kinds == 2
     w = spread
+    top = origin + domain
     lo = np.where(three, 0.0, np.where(left, anchor - 2 * sel * domain - w,
-                                        np.maximum(anchor, domain - 2 * sel * domain - w)))
-    hi = np.where(three, 4 * sel * domain + 64 * domain / (1 << 24), np.where(left, anchor + w, domain + w))
+                                        np.maximum(anchor, top - 2 * sel * domain - w)))
+    hi = np.where(three, 4 * sel * domain + 64 * domain / (1 << 24), np.where(left, anchor + w, top + w))
     best = (lo + hi) / 2
     best_err = np.full(nq, np.inf)
 
@@ -740,7 +794,8 @@ def main():
     stream = torch.cuda.current_stream()
 
     # ---- construction (timed separately, reported as extra keys)
-    pts_d = gen_points_device(n, seed=1 + rank, torch=torch)
+    pts_d = slab_points_device(n, rank, torch)
+    bounds = slab_bounds(pts_d, torch)
     torch.cuda.synchronize()
     c0 = time.perf_counter()
     tree = pst.StaticPSTGPU(pts_d, n, "f32", True)  # first build: allocator and module warm-up
@@ -757,21 +812,44 @@ def main():
     del pts_d
     torch.cuda.empty_cache()
 
-    # ---- queries
+    # ---- queries: this shard's block of the global list (bisected on its own
+    # counts); with several shards every rank routes the whole list by the shards'
+    # bounds and runs the queries that can meet its slab
     eng = pst.BatchEngine(tree, max_queries=NQ, task_capacity=max(1 << 20, n >> 2))
-    kinds, sel, anchor = query_plan(NQ, 7 + rank)
 
     def count_fn(k, a, b, c):
         q = pst.make_queries(k, a, b, c, "f32")
         counts, _ = eng.count(q)
         return counts.cpu().numpy()
-    min1, max1, min2 = calibrate(count_fn, kinds, sel, anchor, n)
+    kinds, min1, max1, min2, sel = sharded_block(count_fn, rank, world, n)
     log("calibrated query bounds")
     q_host = pst.make_queries(kinds, min1, max1, min2, "f32")
+    routed_n = NQ
+    if world > 1:
+        import importlib.util as _ilu
+        _spec = _ilu.spec_from_file_location("pst_sharded", PKG_DIR / "sharded.py")
+        sharded = _ilu.module_from_spec(_spec)
+        _spec.loader.exec_module(sharded)
+        qb = torch.from_numpy(q_host.view(np.uint8).copy()).to("cuda")
+        blocks = [torch.empty_like(qb) for _ in range(world)]
+        dist.all_gather(blocks, qb)
+        rb = [torch.zeros(4, dtype=torch.float64, device="cuda") for _ in range(world)]
+        dist.all_gather(rb, torch.tensor(bounds, dtype=torch.float64, device="cuda"))
+        ranges = torch.stack(rb).cpu().numpy()
+        q_all = torch.cat(blocks).cpu().numpy().view(pst.pst.QUERY_NP)
+        ak, a1, a2, a3 = query_fields(q_all)
+        routed = np.nonzero(sharded.route_many(ak, a1, a2, a3, ranges)[:, rank])[0]
+        q_host = np.ascontiguousarray(q_all[routed])
+        kinds, min1, max1, min2 = query_fields(q_host)
+        routed_n = len(routed)
+        if routed_n > NQ:
+            eng.close()
+            eng = pst.BatchEngine(tree, max_queries=routed_n, task_capacity=max(1 << 20, n >> 2))
+        log(f"shard {rank}: {routed_n} of {world * NQ} queries routed here")
     counts, total = eng.count(q_host)
     q_dev = torch.from_numpy(q_host.view(np.uint8).copy()).to("cuda")
     out = torch.empty(total * 4 + 16, dtype=torch.uint8, device="cuda")
-    offs = torch.empty(NQ + 1, dtype=torch.int64, device="cuda")
+    offs = torch.empty(max(routed_n, NQ) + 1, dtype=torch.int64, device="cuda")
     st, tot = eng.run(q_dev, out, offs, queries_on_device=True, sync=True)
     assert st == 0 and tot == total
     frontier = eng.last_stats()
@@ -815,7 +893,7 @@ def main():
     # ---- end to end through the public call with host buffers
     q_pin = torch.from_numpy(q_host.view(np.uint8).copy()).pin_memory()
     out_pin = torch.empty(total * 4 + 16, dtype=torch.uint8).pin_memory()
-    offs_pin = torch.empty(NQ + 1, dtype=torch.int64).pin_memory()
+    offs_pin = torch.empty(offs.numel(), dtype=torch.int64).pin_memory()
     e2e_ms = []
     for i in range(args.warmup + max(3, args.steps // 4)):
         torch.cuda.synchronize()
@@ -834,7 +912,7 @@ def main():
     # ---- plain per-query drop-in path on a sample of the same queries: the blocking
     # call that hands back a device array of exactly `count` ids (as the reference's
     # searches do), released after each call
-    plain_n = min(args.plain_queries, NQ)
+    plain_n = min(args.plain_queries, len(q_host))
     names = {0: "three", 1: "left", 2: "right"}
     ptr, _ = tree.search_device(names[int(kinds[0])], float(min1[0]), float(max1[0]), float(min2[0]))
     pst.free_device(ptr)
@@ -941,7 +1019,11 @@ def main():
                 "config": {"workload": "batched-4096-mixed-queries-2^28-f32", "n_points": n, "ids": "u32",
                            "queries_per_step": NQ, "mix": "50% three / 25% left / 25% right",
                            "selectivity": [SEL_LO, SEL_HI], "results": "ids",
-                           "l2": "inputs larger than L2 (tree 7.1 GiB)", "parallelism": f"{world} independent shards"},
+                           "l2": "inputs larger than L2 (tree 7.1 GiB)", "parallelism": (f"{world} dim1 shards of one point set (weak scaling: 2^28 points "
+                                           f"and a block of 4096 queries per shard, every query routed to the "
+                                           f"shards its bounds meet; no data-path collective)"
+                                           if world > 1 else "one shard")},
+                "routed_queries": routed_n,
                 "queries_per_s": qps, "points_per_step": total,
                 "frontier": {k: frontier[k] for k in ("records", "seeds", "boundary")},
                 "plain_queries_per_s": plain_qps, "batched_vs_plain_qps": qps / world / plain_qps,
@@ -950,7 +1032,7 @@ def main():
                               "roofline": construct_roofline(n, construct_ms, peak, peak_kind)},
                 "disjoint": disjoint, "batched_queries_config": batched_cfg,
                 "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(q_host.nbytes),
-                        "d2h_bytes_per_step": int(total * 4 + (NQ + 1) * 8)},
+                        "d2h_bytes_per_step": int(total * 4 + offs.numel() * 8)},
                 "gpu_launches": None, "roofline": roof, "cpu_baseline": cpu, "clocks": clk.summary(),
                 "serving": serving}
         if sweep_rows is not None:

@@ -168,10 +168,11 @@ class Orc:
         return out[:cnt]
 
     @classmethod
-    def brute_multi(cls, pts: np.ndarray, dt: str, kinds, min1, max1, min2, threads: int | None = None):
+    def brute_multi(cls, pts: np.ndarray, dt: str, kinds, min1, max1, min2, threads: int | None = None,
+                    counts_only: bool = False):
         """Brute force of many queries in one threaded pass over the points (for large
         point sets): returns (offsets[nq + 1], input indices), each query's indices in
-        index order."""
+        index order (only the offsets, and no indices, with counts_only)."""
         pts = np.ascontiguousarray(pts)
         t = DTYPES[dt]
         k = np.ascontiguousarray(np.asarray(kinds, np.int32))
@@ -184,6 +185,8 @@ class Orc:
                  None)
         if tot < 0:
             raise RuntimeError("oracle brute_multi failed")
+        if counts_only:
+            return off, None
         idx = np.zeros(max(int(tot), 1), np.uint64)
         tot2 = fn(_ptr(pts), pts.dtype.itemsize, len(pts), nq, _ptr(k), _ptr(a), _ptr(b), _ptr(c), th, _ptr(off),
                   _ptr(idx))

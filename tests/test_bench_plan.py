@@ -59,3 +59,45 @@ def test_disjoint_plan_reports_every_point_once(oracle):
     assert np.array_equal(np.sort(idx), np.arange(n, dtype=np.uint64))
     sizes = np.diff(off.astype(np.int64))
     assert sizes.max() > 100 * max(np.median(sizes), 1)  # uneven output sizes
+
+
+def test_sharded_plan_routes_every_result(oracle):
+    """The sharded (weak-scaling) workload on the CPU, 3 shards of 2^14 points: each
+    shard's block of queries starts in its slab (right queries clipped to 3-sided
+    except on the last shard), and routing by the shards' bounds loses no result:
+    the routed shards' brute-force answers add up to the answer over all points."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("sh", bench.PKG_DIR / "sharded.py")
+    sh = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(sh)
+    world, n = 3, 1 << 14
+    slabs = []
+    for r in range(world):
+        p = bench.gen_points_host(n, 1 + r)
+        p["dim1"] += np.float32(r * bench.SLAB)
+        p["dim2"] += np.float32(r * bench.SLAB)
+        p["id"] += np.uint32(r * n)
+        slabs.append(p)
+    def counts(p, k, x, y, z):
+        off, _ = oracle.Orc.brute_multi(p, "f32", k, x, y, z, counts_only=True)
+        return np.diff(off.astype(np.int64))
+    blocks = []
+    for r in range(world):
+        kinds, a, b, c, sel = bench.sharded_block(lambda k, x, y, z, s=slabs[r]: counts(s, k, x, y, z), r, world, n)
+        if r < world - 1:
+            assert not (kinds == 2).any()
+        else:
+            assert (kinds == 2).sum() == bench.NQ // 4
+        three = kinds == 0
+        # every 3-sided range starts in the slab (one near its top may run into the next)
+        assert (a[three] >= r * bench.SLAB).all() and (a[three] < (r + 1) * bench.SLAB).all()
+        blocks.append((kinds, a, b, c))
+    k, a, b, c = (np.concatenate([blk[i] for blk in blocks]) for i in range(4))
+    ranges = np.array([sh.shard_ranges(s) for s in slabs])
+    route = sh.route_many(k, a, b, c, ranges)
+    allpts = np.concatenate(slabs)
+    want = counts(allpts, k, a, b, c)
+    got = sum(np.where(route[:, r], counts(slabs[r], k, a, b, c), 0) for r in range(world))
+    assert np.array_equal(got, want)
+    # most queries stay on one shard
+    assert (route.sum(axis=1) <= 1).mean() > 0.9
