@@ -771,6 +771,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the 2^26 batched-queries configuration")
+    ap.add_argument("--no-tune", action="store_true", help="the default launch shape instead of the autotuner's")
     ap.add_argument("--plain-queries", type=int, default=256)
     ap.add_argument("--sweep", action="store_true", help="also run every value type x kind x selectivity")
     ap.add_argument("--isosurface", action="store_true", help="also run the 512^3 isosurface pipeline")
@@ -842,10 +843,23 @@ def main():
         q_host = np.ascontiguousarray(q_all[routed])
         kinds, min1, max1, min2 = query_fields(q_host)
         routed_n = len(routed)
-        if routed_n > NQ:
-            eng.close()
-            eng = pst.BatchEngine(tree, max_queries=routed_n, task_capacity=max(1 << 20, n >> 2))
         log(f"shard {rank}: {routed_n} of {world * NQ} queries routed here")
+    # ---- launch shape: the project's autotuner times its candidates on these
+    # queries (not cached across runs: every box times them afresh)
+    tuned = None
+    if not args.no_tune:
+        import importlib
+        autotune = importlib.import_module("pst_b200.autotune")
+        tuned = autotune.tune(tree, q_host, repeats=5, cache_path=None, task_capacity=max(1 << 20, n >> 2))
+        dflt = [ms for sh, ms in tuned["tried"] if sh["block_threads"] == 256 and sh["blocks_per_sm"] == 0
+                and sh["emit_records"] == 8]
+        tuned["default_ms"] = dflt[0] if dflt else None
+        for sh, ms in tuned["tried"]:
+            log("  shape " + " ".join(f"{k}={sh[k]}" for k in pst.pst.TUNING_FIELDS) + f": {ms:.3f} ms")
+        log("autotuned launch shape: " + ", ".join(f"{k}={tuned[k]}" for k in pst.pst.TUNING_FIELDS) +
+            f" ({tuned['ms']:.3f} ms per pass; default shape {tuned['default_ms']:.3f} ms)")
+    eng.close()
+    eng = pst.BatchEngine(tree, max_queries=max(routed_n, NQ), task_capacity=max(1 << 20, n >> 2), tuning=tuned)
     counts, total = eng.count(q_host)
     q_dev = torch.from_numpy(q_host.view(np.uint8).copy()).to("cuda")
     out = torch.empty(total * 4 + 16, dtype=torch.uint8, device="cuda")
@@ -935,7 +949,9 @@ def main():
     dq_dev = torch.from_numpy(dq_host.view(np.uint8).copy()).to("cuda")
     st_d, tot_d = eng.run(dq_dev, out, offs, queries_on_device=True, sync=True)
     assert st_d == 0 and tot_d == n, (st_d, tot_d)  # each point exactly once
+    torch.cuda.nvtx.range_push("disjoint")
     dis_ms = time_pass(eng, dq_dev, out, offs, max(3, args.steps // 2), args.warmup, stream, torch)
+    torch.cuda.nvtx.range_pop()
     log(f"disjoint ranges: {dis_ms:.3f} ms/pass for {tot_d} points")
 
     # ---- roofline of the batched search pass
@@ -1024,6 +1040,9 @@ def main():
                                            f"shards its bounds meet; no data-path collective)"
                                            if world > 1 else "one shard")},
                 "routed_queries": routed_n,
+                "autotune": None if tuned is None else {
+                    "chosen": {k: tuned[k] for k in pst.pst.TUNING_FIELDS}, "ms": tuned["ms"],
+                    "default_shape_ms": tuned["default_ms"], "candidates": len(tuned["tried"])},
                 "queries_per_s": qps, "points_per_step": total,
                 "frontier": {k: frontier[k] for k in ("records", "seeds", "boundary")},
                 "plain_queries_per_s": plain_qps, "batched_vs_plain_qps": qps / world / plain_qps,

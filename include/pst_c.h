@@ -191,12 +191,20 @@ pst_status pst_search_noalloc(pst_tree *tree, const pst_query *query, pst_ret re
  * The reference has one query per launch (pst/static-pst-gpu.tu:496-642); this
  * is the batched form of the same searches. */
 
+/* Launch shape of an engine.  The zero values are the library's defaults; the
+ * project's autotuner (static-priority-search-tree_b200/autotune.py) times the
+ * choices on the caller's own queries and caches the fastest per tree shape and
+ * batch size (the reference launches one block of warp_multiplier x 32 threads per
+ * query, pst/static-pst-gpu.tu:525-529). */
 typedef struct pst_batch_opts {
 	uint32_t max_queries;      /* capacity of the query buffer */
-	uint64_t task_capacity;    /* initial frontier capacity in 32-slot chunks (0 = auto) */
-	uint32_t block_threads;    /* 0 = autotuned */
-	uint32_t blocks_per_sm;    /* 0 = autotuned */
+	uint64_t task_capacity;    /* initial frontier capacity in 64-slot block records (0 = auto) */
+	uint32_t block_threads;    /* CTA size of the level and emit kernels: 128, 256 or 512 (0 = 256) */
+	uint32_t blocks_per_sm;    /* level-kernel CTAs per SM (0 = as many as fit) */
 	int32_t use_graph;         /* replay the pass from a captured CUDA graph */
+	uint32_t emit_records;     /* records in flight per warp when ids are emitted: 4, 8 or 16 (0 = 8) */
+	uint32_t top_pass_queries; /* largest waiting batch that starts with the one-CTA top pass, at
+	                              most 1024 (0 = 32) */
 } pst_batch_opts;
 
 pst_status pst_batch_create(pst_batch **out, pst_tree *tree, const pst_batch_opts *opts);
@@ -230,6 +238,13 @@ typedef struct pst_batch_stats {
 	uint32_t levels;
 } pst_batch_stats;
 pst_status pst_batch_last_stats(pst_batch *batch, pst_batch_stats *stats, uint32_t *per_level);
+
+/* The engine's launch shape as resolved on its device: CTA size, level-kernel CTAs
+ * per SM and grid, emit records in flight, top-pass batch limit (any pointer may be
+ * NULL).  No reference counterpart (its launch shape is fixed per call,
+ * pst/static-pst-gpu.tu:525-529). */
+pst_status pst_batch_launch_shape(pst_batch *batch, uint32_t *block_threads, uint32_t *blocks_per_sm,
+                                  uint32_t *grid, uint32_t *emit_records, uint32_t *top_pass_queries);
 
 /* ------------------------------------------------------------------------- */
 /* Serving: a request loop over several resident trees with continuous batching.
@@ -266,6 +281,12 @@ typedef struct pst_server_stats {
 pst_status pst_server_create(pst_server **out, const pst_server_opts *opts);
 /* Registers a resident tree (it must outlive the server); returns its index. */
 pst_status pst_server_add_tree(pst_server *srv, pst_tree *tree, uint32_t *tree_index);
+/* The same with the launch shape of the tree's batch engines taken from `tuning`
+ * (block_threads, blocks_per_sm, emit_records, top_pass_queries; its other fields
+ * are ignored: the server's opts set the batch size and graph replay), e.g. the
+ * autotuner's choice for the tree (NULL = the defaults). */
+pst_status pst_server_add_tree_tuned(pst_server *srv, pst_tree *tree, const pst_batch_opts *tuning,
+                                     uint32_t *tree_index);
 /* Queues n requests.  arrival_ns (CLOCK_MONOTONIC, may be NULL = now) is the
  * arrival time latency is measured from.  ids receives request ids. */
 pst_status pst_server_submit(pst_server *srv, uint32_t n, const uint32_t *tree_index, const pst_query *queries,

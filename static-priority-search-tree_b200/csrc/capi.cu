@@ -572,6 +572,26 @@ pst_status pst_batch_last_stats(pst_batch *batch, pst_batch_stats *stats, uint32
 	});
 }
 
+pst_status pst_batch_launch_shape(pst_batch *batch, uint32_t *block_threads, uint32_t *blocks_per_sm, uint32_t *grid,
+                                  uint32_t *emit_records, uint32_t *top_pass_queries)
+{
+	return guarded([&] {
+		if (!batch)
+			fail(PST_ERR_INVALID, "null argument");
+		const Batch &b = batch->b;
+		if (block_threads)
+			*block_threads = b.threads;
+		if (blocks_per_sm)
+			*blocks_per_sm = b.blocks_per_sm;
+		if (grid)
+			*grid = b.grid;
+		if (emit_records)
+			*emit_records = b.emit_u;
+		if (top_pass_queries)
+			*top_pass_queries = b.top_q;
+	});
+}
+
 // The result counter of an interval search: one device word and one pinned host
 // word per calling thread and device, made on first use and kept (a call waits for
 // its count before it returns, so a thread's calls never overlap).

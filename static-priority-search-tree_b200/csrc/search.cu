@@ -11,10 +11,10 @@
 //   - every subtree the reference would "report above" is scanned by level.  In a
 //     max-heap on dim2 a node of such a subtree is reported exactly when its own
 //     dim2 passes (its ancestors' dim2 are at least as large), so the work unit is a
-//     chunk: 32 consecutive slots of one level, tested by one warp with one coalesced
-//     load.  The frontier is kept as "alive records" only — (chunk, query, mask of
+//     block: 64 consecutive slots of one level, tested by one warp with coalesced
+//     loads.  The frontier is kept as "alive records" only — (block, query, mask of
 //     reported slots) — and the next level expands each record into its two child
-//     chunks (spread16), masked by occupancy before anything is loaded.  Every
+//     blocks, loading only the children of reported slots.  Every
 //     level but the last is full (a level-d node holds at least
 //     floor((n + 1) / 2^d) - 1 >= 1 points for d <= D - 2), so occupancy is read
 //     only for children on the last level.
@@ -50,7 +50,10 @@ struct QDev {
 
 // Alive records cover a "block" of 64 consecutive slots of one level (two
 // 128-byte rows of a 4-byte field): (block base position, query, mask of reported
-// slots, low and high word).  Block bases are multiples of 64.
+// slots in pair order).  Block bases are multiples of 64.  Pair order: bit m of the
+// first mask word is slot 2m of the block, bit m of the second word slot 2m + 1, so
+// lane m of a warp owns the slot pair (2m, 2m + 1) and a warp-wide ballot of one
+// test per lane is one mask word.
 struct WorkDev {
 	uint4 *rec;            // alive records of every level, level regions in order
 	uint64_t rec_cap;
@@ -65,11 +68,22 @@ struct WorkDev {
 	BatchCtl *ctl;
 };
 
-// The block record of a 32-slot chunk (base pos32, a multiple of 32) and its mask.
+// The even-indexed bits of x, packed into the low 16 bits.
+__device__ __forceinline__ uint32_t even_bits(uint32_t x)
+{
+	x &= 0x55555555u;
+	x = (x | (x >> 1)) & 0x33333333u;
+	x = (x | (x >> 2)) & 0x0F0F0F0Fu;
+	x = (x | (x >> 4)) & 0x00FF00FFu;
+	return (x | (x >> 8)) & 0x0000FFFFu;
+}
+
+// The block record of a 32-slot chunk (base pos32, a multiple of 32) and its mask
+// (bit i = slot pos32 + i), converted to pair order.
 __device__ __forceinline__ uint4 block_record(uint32_t pos32, uint32_t q, uint32_t bits32)
 {
-	const bool upper = (pos32 & 32u) != 0;
-	return make_uint4(pos32 & ~63u, q, upper ? 0u : bits32, upper ? bits32 : 0u);
+	const uint32_t sh = (pos32 & 32u) ? 16u : 0u;  // the upper chunk holds pairs 16..31
+	return make_uint4(pos32 & ~63u, q, even_bits(bits32) << sh, even_bits(bits32 >> 1) << sh);
 }
 
 template <typename T>
@@ -181,38 +195,6 @@ __device__ __forceinline__ void path_step(const TreeDev<T> &t, const QDev<T> &qd
 	}
 }
 
-template <typename T>
-struct Vec4;
-template <>
-struct Vec4<float> {
-	using V = float4;
-};
-template <>
-struct Vec4<int32_t> {
-	using V = int4;
-};
-
-// Four consecutive values from a 16-byte aligned address (two loads for doubles).
-template <typename T>
-__device__ __forceinline__ void load_quad(const T *__restrict__ p, T (&v)[4])
-{
-	if constexpr (sizeof(T) == 4) {
-		using V = typename Vec4<T>::V;
-		const V x = *reinterpret_cast<const V *>(p);
-		v[0] = x.x;
-		v[1] = x.y;
-		v[2] = x.z;
-		v[3] = x.w;
-	} else {
-		const double2 a = reinterpret_cast<const double2 *>(p)[0];
-		const double2 b = reinterpret_cast<const double2 *>(p)[1];
-		v[0] = a.x;
-		v[1] = a.y;
-		v[2] = b.x;
-		v[3] = b.y;
-	}
-}
-
 // Appends each lane's non-empty records (at most K) to the level region (one atomic
 // per warp).
 template <int K>
@@ -257,28 +239,40 @@ __device__ __forceinline__ void add_counts(const WorkDev &w, uint32_t q, uint32_
 		atomicAdd((unsigned long long *) &w.counts[q], (unsigned long long) run);
 }
 
-// Per-warp shared staging of the 32 records a warp holds: the records, the
-// candidate masks of their four child rows (parents' bits spread to their children,
-// ANDed with the occupancy), their queries' min2, the child rows found, and the
-// list of records that have any candidate at all.
+// Per-warp shared staging of the 32 records a warp holds: the records, their
+// queries' min2 and the list of records that can have children at all.
 template <typename T>
 struct WarpStage {
 	uint4 rec[32];
-	uint4 cand[32];
-	uint4 rows[32];
 	T m2[32];
 	uint32_t live[32];
 };
 
+// Two consecutive values from an 8-byte (16 for doubles) aligned address.
+template <typename T>
+__device__ __forceinline__ void load_pair(const T *__restrict__ p, T (&v)[2])
+{
+	if constexpr (sizeof(T) == 4) {
+		const uint2 x = *reinterpret_cast<const uint2 *>(p);
+		memcpy(&v[0], &x.x, 4);
+		memcpy(&v[1], &x.y, 4);
+	} else {
+		const double2 x = *reinterpret_cast<const double2 *>(p);
+		v[0] = x.x;
+		v[1] = x.y;
+	}
+}
+
 // Expands the records held by the warp (lane k owns record `mine`; the valid lanes
-// are a prefix) into their child records.  Each lane first stages its record's
-// candidate child slots (`full`: the children's level is full, so the candidates
-// are the spread parent bits with no occupancy read); records without any (all
-// children absent, e.g. above a sparse last level) cost nothing more.  Then the whole warp takes the live records
-// U at a time: lane l tests the child slots [2b + 4l, 2b + 4l + 4) with one 16-byte
-// load (two for doubles), issued only where it has candidates; each 8-lane group
-// ORs its nibbles into one 32-slot child row, and the owner reads the four rows as
-// its two child records (blocks 2b and 2b + 64).
+// are a prefix) into their child records.  The whole warp takes the live records U
+// at a time.  A record's block [b, b + 64) has the children [2b, 2b + 128), the
+// blocks A = [2b, 2b + 64) and B = [2b + 64, 2b + 128): lane m tests the pair
+// (2b + 2m, 2b + 2m + 1) of A, the children of parent b + m, and the same pair of
+// B, the children of parent b + 32 + m, with one 8-byte load each (16 for doubles),
+// issued only where the parent was reported (and, for children on the last level,
+// the child exists).  The four ballots of those tests are the two child records'
+// masks in pair order, taken by the record's owner lane: no shuffles, no staging of
+// rows.  Children on a full level (every level but the last) need no occupancy read.
 template <typename T, bool LAST>
 __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__restrict__ min2s, const uint4 &mine,
                                                bool valid, bool full, WarpStage<T> &st, uint4 (&child)[2],
@@ -286,78 +280,72 @@ __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__r
 {
 	constexpr int U = sizeof(T) == 4 ? 4 : 2;  // records in flight
 	const uint32_t lane = lane_id();
-	const uint32_t r = lane >> 3, qd = lane & 7;
-	uint4 cand = make_uint4(0, 0, 0, 0);
-	bool has_children = valid;
-	if (LAST && valid) {
+	bool live = valid && (mine.z | mine.w) != 0;
+	if (LAST && live) {
 		// expanding into the last level: most blocks of a sparse last level have no
 		// children, which one bit per parent block tells before any occupancy read
 		const uint32_t j = (mine.x - (1u << (t.levels - 2))) >> 6;
-		has_children = (t.last_par[j >> 5] >> (j & 31)) & 1u;
+		live = (t.last_par[j >> 5] >> (j & 31)) & 1u;
 	}
-	if (has_children) {
-		// children on a full level (every level but the last) need no occupancy read
-		const uint4 occ = full ? make_uint4(FULL, FULL, FULL, FULL)
-		                       : *reinterpret_cast<const uint4 *>(t.occ + ((2 * mine.x) >> 5));
-		cand = make_uint4(spread16(mine.z) & occ.x, spread16(mine.z >> 16) & occ.y, spread16(mine.w) & occ.z,
-		                  spread16(mine.w >> 16) & occ.w);
-	}
-	const bool live = (cand.x | cand.y | cand.z | cand.w) != 0;
 	const uint32_t lm = __ballot_sync(FULL, live);
 	const int nlive = __popc(lm);
 	if (live) {
 		st.rec[lane] = mine;
-		st.cand[lane] = cand;
 		st.m2[lane] = min2s[mine.y];
 		st.live[__popc(lm & lanemask_lt())] = lane;
 	}
 	__syncwarp();
-	const uint32_t *candw = reinterpret_cast<const uint32_t *>(st.cand);
+	// parent slot b + m is pair m >> 1, word m & 1 of the record's mask; b + 32 + m is
+	// pair 16 + (m >> 1)
+	const uint32_t psh = lane >> 1;
+	uint4 rows = make_uint4(0, 0, 0, 0);
 	for (int k0 = 0; k0 < nlive; k0 += U) {
-		uint32_t cn[U], kk[U];
-		T v[U][4];
+		uint32_t kk[U], ca[U], cb[U];
+		T va[U][2], vb[U][2];
 #pragma unroll
 		for (int u = 0; u < U; u++) {
 			const bool on = k0 + u < nlive;
 			const uint32_t k = st.live[on ? k0 + u : 0];
 			kk[u] = k;
-			const uint32_t c4 = on ? (candw[4 * k + r] >> (4 * qd)) & 0xFu : 0u;
-			cn[u] = c4;
-			if (c4) {
-				load_quad(t.dim2 + 2 * st.rec[k].x + 4 * lane, v[u]);
-			} else {
-#pragma unroll
-				for (int j = 0; j < 4; j++)
-					v[u][j] = T(0);
+			const uint4 rc = st.rec[k];
+			const uint32_t pw = (lane & 1) ? rc.w : rc.z;
+			// candidate pairs of A and B: both children of a reported parent (bits 0, 1)
+			uint32_t a = on ? ((pw >> psh) & 1u) * 3u : 0u;
+			uint32_t b = on ? ((pw >> (16 + psh)) & 1u) * 3u : 0u;
+			const uint32_t cbase = 2 * rc.x;  // a multiple of 128
+			if (!full) {
+				if (a)
+					a &= t.occ[(cbase >> 5) + (lane >> 4)] >> ((2 * lane) & 31);
+				if (b)
+					b &= t.occ[(cbase >> 5) + 2 + (lane >> 4)] >> ((2 * lane) & 31);
 			}
+			ca[u] = a & 3u;
+			cb[u] = b & 3u;
+			va[u][0] = va[u][1] = vb[u][0] = vb[u][1] = T(0);
+			if (ca[u])
+				load_pair(t.dim2 + cbase + 2 * lane, va[u]);
+			if (cb[u])
+				load_pair(t.dim2 + cbase + 64 + 2 * lane, vb[u]);
 		}
 #pragma unroll
 		for (int u = 0; u < U; u++) {
 			const T m2 = st.m2[kk[u]];
-			// all four slots are compared (values of slots without a candidate are zero or
-			// loaded anyway) and the candidates masked once, not tested slot by slot
-			uint32_t ge = 0;
-#pragma unroll
-			for (int j = 0; j < 4; j++)
-				ge |= (m2 <= v[u][j]) ? 1u << j : 0u;
-			uint32_t row = (ge & cn[u]) << (4 * qd);
-			row |= __shfl_xor_sync(FULL, row, 1);
-			row |= __shfl_xor_sync(FULL, row, 2);
-			row |= __shfl_xor_sync(FULL, row, 4);
-			if (qd == 0 && k0 + u < nlive)
-				reinterpret_cast<uint32_t *>(st.rows)[4 * kk[u] + r] = row;
+			const uint32_t a0 = __ballot_sync(FULL, (ca[u] & 1u) && m2 <= va[u][0]);
+			const uint32_t a1 = __ballot_sync(FULL, (ca[u] & 2u) && m2 <= va[u][1]);
+			const uint32_t b0 = __ballot_sync(FULL, (cb[u] & 1u) && m2 <= vb[u][0]);
+			const uint32_t b1 = __ballot_sync(FULL, (cb[u] & 2u) && m2 <= vb[u][1]);
+			if (k0 + u < nlive && lane == kk[u])
+				rows = make_uint4(a0, a1, b0, b1);
 		}
 	}
-	__syncwarp();
+	__syncwarp();  // the stage is reused by the warp's next batch
 	child[0] = child[1] = make_uint4(0, 0, 0, 0);
 	pts = 0;
 	if (live) {
-		const uint4 rw = st.rows[lane];
-		child[0] = make_uint4(2 * mine.x, mine.y, rw.x, rw.y);
-		child[1] = make_uint4(2 * mine.x + 64, mine.y, rw.z, rw.w);
-		pts = __popc(rw.x) + __popc(rw.y) + __popc(rw.z) + __popc(rw.w);
+		child[0] = make_uint4(2 * mine.x, mine.y, rows.x, rows.y);
+		child[1] = make_uint4(2 * mine.x + 64, mine.y, rows.z, rows.w);
+		pts = __popc(rows.x) + __popc(rows.y) + __popc(rows.z) + __popc(rows.w);
 	}
-	__syncwarp();  // the stage is reused by the warp's next batch
 }
 
 // One tree level of the search (the body of k_bfs_level): the boundary paths, the
@@ -437,9 +425,12 @@ __device__ __forceinline__ void level_body(const TreeDev<T> &t, const QDev<T> &q
 }
 
 // LAST: the expansion into the last level of a tree with TreeDev::last_par (its own
-// instantiation, so the other levels keep their register budget).
-template <typename T, bool LAST>
-__global__ void __launch_bounds__(BFS_THREADS, 4) k_bfs_level(TreeDev<T> t, QDev<T> qd, WorkDev w, uint32_t d)
+// instantiation, so the other levels keep their register budget).  THREADS: the
+// CTA size (128, 256 or 512, a tuning choice); every size keeps 64 registers a
+// thread, so 1024 threads of the kernel fit an SM at once.
+template <typename T, bool LAST, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_bfs_level(TreeDev<T> t, QDev<T> qd, WorkDev w,
+                                                                      uint32_t d)
 {
 	// Launched as a programmatic dependent of the previous level: its CTAs may be
 	// scheduled while that level drains, and wait here until it has completed and
@@ -451,7 +442,7 @@ __global__ void __launch_bounds__(BFS_THREADS, 4) k_bfs_level(TreeDev<T> t, QDev
 	if (w.ctl->flags & BATCH_FLAG_TASK_OVERFLOW)
 		return;
 	__shared__ uint64_t s_base[2];
-	__shared__ WarpStage<T> s_stage[BFS_THREADS / 32];
+	__shared__ WarpStage<T> s_stage[THREADS / 32];
 	if (threadIdx.x == 0) {
 		uint64_t b = 0;  // start of the previous level's records
 		for (uint32_t e = 0; e + 1 < d; e++)
@@ -621,18 +612,16 @@ struct EmitStage {
 	unsigned long long ob[32];
 };
 
-template <typename T, bool HAS_ID, bool POINTS>
+template <typename T, bool HAS_ID, bool POINTS, int U>
 __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mine, uint64_t out_base, bool valid,
                                             EmitStage &st, void *__restrict__ out)
 {
-	using Pt = Point<T, HAS_ID>;
-	constexpr int U = POINTS ? 4 : 8;  // records in flight
+	using Pt = Point<T, HAS_ID>;  // U: records in flight per warp
 	static_assert(32 % U == 0, "a batch of records ends inside the 32 staged ones");
 	const uint32_t lane = lane_id();
-	const uint32_t psh = (2 * lane) & 31;
-	// the record's slots before this lane's pair, as masks of its two 32-slot words
-	const uint32_t below_z = lane < 16 ? (1u << psh) - 1u : FULL;
-	const uint32_t below_w = lane < 16 ? 0u : (1u << psh) - 1u;
+	// pair order: this lane's slots are bit `lane` of the two mask words, and the
+	// record's reported slots before them are the lower bits of both
+	const uint32_t lt = lanemask_lt();
 	st.rec[lane] = mine;
 	st.ob[lane] = out_base;
 	__syncwarp();
@@ -649,8 +638,8 @@ __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mi
 			// per record (U divides 32, so k < 32)
 			const int k = k0 + u;
 			const uint4 rc = st.rec[k];
-			b2[u] = ((lane < 16 ? rc.z : rc.w) >> psh) & 3u;
-			const uint32_t before = __popc(rc.z & below_z) + __popc(rc.w & below_w);
+			b2[u] = ((rc.z >> lane) & 1u) | (((rc.w >> lane) & 1u) << 1);
+			const uint32_t before = __popc(rc.z & lt) + __popc(rc.w & lt);
 			o[u] = st.ob[k] + before;
 			hb[u] = rc.x + 2 * lane;
 			if constexpr (!POINTS || HAS_ID)
@@ -702,11 +691,13 @@ __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mi
 	__syncwarp();  // the stage is reused by the warp's next batch
 }
 
-template <typename T, bool HAS_ID, bool POINTS>
-__global__ void __launch_bounds__(BFS_THREADS) k_emit(TreeDev<T> t, WorkDev w, void *out, uint64_t capacity)
+// THREADS: the CTA size and U the records each warp has in flight (both tuning
+// choices; point records keep U = 4).
+template <typename T, bool HAS_ID, bool POINTS, int THREADS, int U>
+__global__ void __launch_bounds__(THREADS) k_emit(TreeDev<T> t, WorkDev w, void *out, uint64_t capacity)
 {
 	__shared__ uint64_t s_total;
-	__shared__ EmitStage s_stage[BFS_THREADS / 32];
+	__shared__ EmitStage s_stage[THREADS / 32];
 	if (threadIdx.x == 0) {
 		uint64_t b = 0;
 		for (uint32_t e = 0; e < t.levels; e++)
@@ -739,7 +730,7 @@ __global__ void __launch_bounds__(BFS_THREADS) k_emit(TreeDev<T> t, WorkDev w, v
 		uint4 m1 = v1 ? w.rec[nb + lane] : make_uint4(0, 0, 0, 0);
 		const uint64_t ob1 = nb < total ? claim_output(w, m1.y, __popc(m1.z) + __popc(m1.w), v1) : 0;
 		guard_claim(w, m1, ob1, capacity);
-		emit_blocks<T, HAS_ID, POINTS>(t, m0, ob0, v0, s_stage[threadIdx.x >> 5], out);
+		emit_blocks<T, HAS_ID, POINTS, U>(t, m0, ob0, v0, s_stage[threadIdx.x >> 5], out);
 		wb = nb;
 		v0 = v1;
 		m0 = m1;
@@ -750,18 +741,18 @@ __global__ void __launch_bounds__(BFS_THREADS) k_emit(TreeDev<T> t, WorkDev w, v
 		uint4 mine = valid ? w.ro[wb + lane] : make_uint4(0, 0, 0, 0);
 		const uint64_t ob = claim_output(w, mine.y, __popc(mine.z) + __popc(mine.w), valid);
 		guard_claim(w, mine, ob, capacity);
-		emit_blocks<T, HAS_ID, POINTS>(t, mine, ob, valid, s_stage[threadIdx.x >> 5], out);
+		emit_blocks<T, HAS_ID, POINTS, U>(t, mine, ob, valid, s_stage[threadIdx.x >> 5], out);
 	}
 }
 
 // Grid of k_emit: as many CTAs as fit on the device at once (its own occupancy,
 // which can differ from the level kernel's), so the grid-stride loop has no tail wave.
-template <typename T, bool HAS_ID, bool POINTS>
+template <typename T, bool HAS_ID, bool POINTS, int THREADS, int U>
 unsigned emit_grid()
 {
 	static const int occ = [] {
 		int o = 0;
-		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_emit<T, HAS_ID, POINTS>, BFS_THREADS, 0) !=
+		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_emit<T, HAS_ID, POINTS, THREADS, U>, THREADS, 0) !=
 		    cudaSuccess) {
 			cudaGetLastError();
 			o = 1;
@@ -787,16 +778,64 @@ void launch_level(const TreeDev<T> &tv, const QDev<T> &qd, const WorkDev &w, uin
 	attr[0].val.programmaticStreamSerializationAllowed = 1;
 	cfg.attrs = attr;
 	cfg.numAttrs = 1;
-	if (d + 1 == tv.levels && tv.last_par)
-		PST_CUDA(cudaLaunchKernelEx(&cfg, k_bfs_level<T, true>, tv, qd, w, d));
-	else
-		PST_CUDA(cudaLaunchKernelEx(&cfg, k_bfs_level<T, false>, tv, qd, w, d));
+	const bool last = d + 1 == tv.levels && tv.last_par;
+	switch (threads) {
+	case 128:
+		PST_CUDA(last ? cudaLaunchKernelEx(&cfg, k_bfs_level<T, true, 128>, tv, qd, w, d)
+		              : cudaLaunchKernelEx(&cfg, k_bfs_level<T, false, 128>, tv, qd, w, d));
+		break;
+	case 512:
+		PST_CUDA(last ? cudaLaunchKernelEx(&cfg, k_bfs_level<T, true, 512>, tv, qd, w, d)
+		              : cudaLaunchKernelEx(&cfg, k_bfs_level<T, false, 512>, tv, qd, w, d));
+		break;
+	default:
+		PST_CUDA(last ? cudaLaunchKernelEx(&cfg, k_bfs_level<T, true, BFS_THREADS>, tv, qd, w, d)
+		              : cudaLaunchKernelEx(&cfg, k_bfs_level<T, false, BFS_THREADS>, tv, qd, w, d));
+	}
 }
 
 template <typename T>
-const void *bfs_kernel_ptr()
+const void *bfs_kernel_ptr(unsigned threads)
 {
-	return reinterpret_cast<const void *>(&k_bfs_level<T, false>);
+	switch (threads) {
+	case 128: return reinterpret_cast<const void *>(&k_bfs_level<T, false, 128>);
+	case 512: return reinterpret_cast<const void *>(&k_bfs_level<T, false, 512>);
+	default: return reinterpret_cast<const void *>(&k_bfs_level<T, false, BFS_THREADS>);
+	}
+}
+
+// Launches the emit with the batch's CTA size and records in flight.
+template <typename T, bool HAS_ID, bool POINTS, int THREADS, int U>
+void launch_emit_tu(const TreeDev<T> &tv, const WorkDev &w, void *out, uint64_t capacity, cudaStream_t s)
+{
+	k_emit<T, HAS_ID, POINTS, THREADS, U><<<emit_grid<T, HAS_ID, POINTS, THREADS, U>(), THREADS, 0, s>>>(tv, w, out,
+	                                                                                                   capacity);
+}
+
+template <typename T, bool HAS_ID, bool POINTS, int THREADS>
+void launch_emit_t(const TreeDev<T> &tv, const WorkDev &w, void *out, uint64_t capacity, uint32_t u, cudaStream_t s)
+{
+	if constexpr (POINTS) {
+		(void) u;
+		launch_emit_tu<T, HAS_ID, POINTS, THREADS, 4>(tv, w, out, capacity, s);
+	} else if (u == 4) {
+		launch_emit_tu<T, HAS_ID, POINTS, THREADS, 4>(tv, w, out, capacity, s);
+	} else if (u == 16) {
+		launch_emit_tu<T, HAS_ID, POINTS, THREADS, 16>(tv, w, out, capacity, s);
+	} else {
+		launch_emit_tu<T, HAS_ID, POINTS, THREADS, 8>(tv, w, out, capacity, s);
+	}
+}
+
+template <typename T, bool HAS_ID, bool POINTS>
+void launch_emit(const TreeDev<T> &tv, const WorkDev &w, void *out, uint64_t capacity, uint32_t threads, uint32_t u,
+                 cudaStream_t s)
+{
+	switch (threads) {
+	case 128: launch_emit_t<T, HAS_ID, POINTS, 128>(tv, w, out, capacity, u, s); break;
+	case 512: launch_emit_t<T, HAS_ID, POINTS, 512>(tv, w, out, capacity, u, s); break;
+	default: launch_emit_t<T, HAS_ID, POINTS, BFS_THREADS>(tv, w, out, capacity, u, s);
+	}
 }
 
 }  // namespace
@@ -848,14 +887,20 @@ void Batch::init(TreeStorage *t, const pst_batch_opts &o)
 	max_q = std::max<uint32_t>(o.max_queries, 1);
 	use_graph = o.use_graph != 0;
 	threads = o.block_threads ? o.block_threads : BFS_THREADS;
-	if (threads != BFS_THREADS)
-		fail(PST_ERR_INVALID, "block_threads must be 0 or " + std::to_string(BFS_THREADS));
+	if (threads != 128 && threads != 256 && threads != 512)
+		fail(PST_ERR_INVALID, "block_threads must be 0, 128, 256 or 512");
+	emit_u = o.emit_records ? o.emit_records : 8;
+	if (emit_u != 4 && emit_u != 8 && emit_u != 16)
+		fail(PST_ERR_INVALID, "emit_records must be 0, 4, 8 or 16");
+	top_q = o.top_pass_queries ? o.top_pass_queries : SMALL_BATCH_Q;
+	if (top_q > MAX_TOP_PASS_Q)
+		fail(PST_ERR_INVALID, "top_pass_queries must be at most " + std::to_string(MAX_TOP_PASS_Q));
 	int occ = 0;
 	const void *kfn = nullptr;
 	switch (t->dtype) {
-	case PST_F32: kfn = bfs_kernel_ptr<float>(); break;
-	case PST_F64: kfn = bfs_kernel_ptr<double>(); break;
-	case PST_I32: kfn = bfs_kernel_ptr<int32_t>(); break;
+	case PST_F32: kfn = bfs_kernel_ptr<float>(threads); break;
+	case PST_F64: kfn = bfs_kernel_ptr<double>(threads); break;
+	case PST_I32: kfn = bfs_kernel_ptr<int32_t>(threads); break;
 	}
 	PST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, threads, 0));
 	blocks_per_sm = o.blocks_per_sm ? std::min<uint32_t>(o.blocks_per_sm, (uint32_t) std::max(occ, 1))
@@ -937,8 +982,7 @@ void Batch::enqueue_count_top(cudaStream_t s)
 	TreeDev<T> tv = tree->view<T>();
 	QDev<T> qd{kind, static_cast<const T *>(min1), static_cast<const T *>(max1), static_cast<const T *>(min2)};
 	PST_WORKDEV;
-	// one thread per query of the batch (at most SMALL_BATCH_Q; the loops are grid-strided)
-	static_assert(SMALL_BATCH_Q % 32 == 0 && SMALL_BATCH_Q <= 1024, "one CTA of whole warps");
+	// one CTA over the batch's queries (the loops are grid-strided)
 	const unsigned qt = SMALL_BATCH_Q;
 	PST_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
 	PST_CUDA(cudaMemsetAsync(counts, 0, (size_t) max_q * 8, s));
@@ -968,7 +1012,7 @@ void Batch::enqueue_emit_t(void *out, uint64_t capacity, cudaStream_t s)
 {
 	TreeDev<T> tv = tree->view<T>();
 	PST_WORKDEV;
-	k_emit<T, HAS_ID, POINTS><<<emit_grid<T, HAS_ID, POINTS>(), threads, 0, s>>>(tv, w, out, capacity);
+	launch_emit<T, HAS_ID, POINTS>(tv, w, out, capacity, threads, emit_u, s);
 	PST_CUDA(cudaGetLastError());
 }
 
@@ -1046,8 +1090,8 @@ void Batch::launch_count(cudaStream_t s) { launch_graph(full_graph, &Batch::enqu
 
 void Batch::launch_count_top(cudaStream_t s)
 {
-	if (ctl_host->nq > SMALL_BATCH_Q)
-		fail(PST_ERR_INTERNAL, "top pass on a batch of more than " + std::to_string(SMALL_BATCH_Q) + " queries");
+	if (ctl_host->nq > top_q)
+		fail(PST_ERR_INTERNAL, "top pass on a batch of more than " + std::to_string(top_q) + " queries");
 	launch_graph(top_graph, &Batch::enqueue_counting_top, s);
 }
 
@@ -1100,7 +1144,7 @@ pst_status Batch::read_ctl(cudaStream_t s, uint64_t *total)
 // Count pass with the host waiting for it.
 void Batch::count_sync(cudaStream_t s, uint64_t *total)
 {
-	if (ctl_host->nq <= SMALL_BATCH_Q)
+	if (ctl_host->nq <= top_q)
 		count_small_sync(s, total);
 	else
 		count_full_sync(s, total);
@@ -1309,7 +1353,7 @@ uint64_t noalloc_run(TreeStorage &t, const pst_query &q, pst_ret ret, void *out,
 	PST_CUDA(cudaMemsetAsync(cursor, 0, 8, s));
 
 	int occ = 0;
-	PST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bfs_kernel_ptr<T>(), BFS_THREADS, 0));
+	PST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bfs_kernel_ptr<T>(BFS_THREADS), BFS_THREADS, 0));
 	const unsigned grid = (unsigned) device_info().sms * (unsigned) std::max(occ, 1);
 	TreeDev<T> tv = t.view<T>();
 	QDev<T> qd{kind, min1, max1, min2};
@@ -1336,11 +1380,11 @@ uint64_t noalloc_run(TreeStorage &t, const pst_query &q, pst_ret ret, void *out,
 		return h.total;
 	const bool has_id = t.idtype == PST_ID_U32;
 	if (ret == PST_RET_IDS)
-		k_emit<T, true, false><<<emit_grid<T, true, false>(), BFS_THREADS, 0, s>>>(tv, w, out, capacity);
+		launch_emit<T, true, false>(tv, w, out, capacity, BFS_THREADS, 8, s);
 	else if (has_id)
-		k_emit<T, true, true><<<emit_grid<T, true, true>(), BFS_THREADS, 0, s>>>(tv, w, out, capacity);
+		launch_emit<T, true, true>(tv, w, out, capacity, BFS_THREADS, 4, s);
 	else
-		k_emit<T, false, true><<<emit_grid<T, false, true>(), BFS_THREADS, 0, s>>>(tv, w, out, capacity);
+		launch_emit<T, false, true>(tv, w, out, capacity, BFS_THREADS, 4, s);
 	PST_CUDA(cudaGetLastError());
 	PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
 	PST_CUDA(cudaStreamSynchronize(s));

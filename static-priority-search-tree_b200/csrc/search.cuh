@@ -6,9 +6,11 @@
 namespace pst {
 
 constexpr int BFS_THREADS = 256;
-// Batches of at most this many queries start with the one-CTA top pass, which walks
-// the upper levels without a kernel boundary between them.
+// Batches of at most this many queries (by default; pst_batch_opts.top_pass_queries
+// sets it per engine, up to MAX_TOP_PASS_Q) start with the one-CTA top pass, which
+// walks the upper levels without a kernel boundary between them.
 constexpr uint32_t SMALL_BATCH_Q = 32;
+constexpr uint32_t MAX_TOP_PASS_Q = 1024;
 
 enum : uint32_t {
 	BATCH_FLAG_TASK_OVERFLOW = 1u,  // frontier buffer too small (results incomplete)
@@ -35,7 +37,9 @@ struct Batch {
 	TreeStorage *tree = nullptr;
 	uint32_t max_q = 0;
 	bool use_graph = true;
-	uint32_t threads = BFS_THREADS;
+	uint32_t threads = BFS_THREADS;  // CTA size of the level and emit kernels
+	uint32_t emit_u = 8;             // records in flight per warp in the emit (ids)
+	uint32_t top_q = SMALL_BATCH_Q;  // largest batch that starts with the one-CTA top pass
 	uint32_t blocks_per_sm = 0;
 	uint32_t grid = 0;
 	// queries
@@ -71,7 +75,7 @@ struct Batch {
 	void stage_queries(const pst_query *q, uint32_t nq, bool on_device, cudaStream_t s);
 	// Whole count pass (every level kernel and the scan), asynchronous.
 	void launch_count(cudaStream_t s);
-	// Top pass of a small batch (nq <= SMALL_BATCH_Q), asynchronous: when it stops
+	// Top pass of a small batch (nq <= top_q), asynchronous: when it stops
 	// above the bottom (ctl->cta_levels < tree levels), launch_count_rest finishes it.
 	void launch_count_top(cudaStream_t s);
 	void launch_count_rest(uint32_t from, cudaStream_t s);

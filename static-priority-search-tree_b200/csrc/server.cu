@@ -336,7 +336,7 @@ struct Server {
 	{
 		const uint32_t n = (uint32_t) sl.reqs.size();
 		sl.eng.stage_queries(sl.qhost.data(), n, false, sl.stream);
-		if (n <= SMALL_BATCH_Q) {
+		if (n <= sl.eng.top_q) {
 			sl.eng.launch_count_top(sl.stream);
 			sl.phase = SLOT_TOP;
 		} else {
@@ -451,7 +451,7 @@ Server *server_create(const pst_server_opts &o)
 	return s.release();
 }
 
-uint32_t server_add_tree(Server *s, TreeStorage *t)
+uint32_t server_add_tree(Server *s, TreeStorage *t, const pst_batch_opts *tuning)
 {
 	if (t->device != s->device)
 		fail(PST_ERR_INVALID, "all trees of a server must live on the server's device");
@@ -461,6 +461,14 @@ uint32_t server_add_tree(Server *s, TreeStorage *t)
 	for (uint32_t i = 0; i < s->opts.slots_per_tree; i++) {
 		auto sl = std::make_unique<Slot>();
 		pst_batch_opts bo{};
+		if (tuning) {
+			// the tree's launch shape (the autotuner's choice); batch size and graph
+			// replay stay the server's
+			bo.block_threads = tuning->block_threads;
+			bo.blocks_per_sm = tuning->blocks_per_sm;
+			bo.emit_records = tuning->emit_records;
+			bo.top_pass_queries = tuning->top_pass_queries;
+		}
 		bo.max_queries = s->opts.max_batch;
 		bo.use_graph = s->opts.use_graph;
 		// frontier sized from the tree (one 64-slot record per 8 points) so that batches
@@ -670,12 +678,18 @@ pst_status pst_server_create(pst_server **out, const pst_server_opts *opts)
 
 pst_status pst_server_add_tree(pst_server *srv, pst_tree *tree, uint32_t *tree_index)
 {
+	return pst_server_add_tree_tuned(srv, tree, nullptr, tree_index);
+}
+
+pst_status pst_server_add_tree_tuned(pst_server *srv, pst_tree *tree, const pst_batch_opts *tuning,
+                                     uint32_t *tree_index)
+{
 	return pst::guarded_call([&] {
 		if (!srv || !tree)
 			pst::fail(PST_ERR_INVALID, "null argument");
 		if (tree->t.n == 0)
 			pst::fail(PST_ERR_INVALID, "an empty tree cannot be served");
-		const uint32_t i = pst::server_add_tree(srv->s, &tree->t);
+		const uint32_t i = pst::server_add_tree(srv->s, &tree->t, tuning);
 		if (tree_index)
 			*tree_index = i;
 	});

@@ -35,7 +35,12 @@ class Query(C.Structure):
 
 class BatchOpts(C.Structure):
     _fields_ = [("max_queries", C.c_uint32), ("task_capacity", C.c_uint64), ("block_threads", C.c_uint32),
-                ("blocks_per_sm", C.c_uint32), ("use_graph", C.c_int32)]
+                ("blocks_per_sm", C.c_uint32), ("use_graph", C.c_int32), ("emit_records", C.c_uint32),
+                ("top_pass_queries", C.c_uint32)]
+
+
+# The launch-shape fields of BatchOpts a tuning (the autotuner's choice) sets.
+TUNING_FIELDS = ("block_threads", "blocks_per_sm", "emit_records", "top_pass_queries")
 
 
 class ServerOpts(C.Structure):
@@ -97,11 +102,13 @@ def lib():
         "pst_batch_count": (i32, [vp, vp, u32, i32, vp, P(u64), vp]),
         "pst_batch_status": (i32, [vp, P(u64)]),
         "pst_batch_last_stats": (i32, [vp, P(BatchStats), vp]),
+        "pst_batch_launch_shape": (i32, [vp, P(u32), P(u32), P(u32), P(u32), P(u32)]),
         "pst_ips_search": (i32, [i32, i32, vp, u64, u64, i32, P(vp), P(u64), u32, u32, vp]),
         "pst_ips_search_into": (i32, [i32, i32, vp, u64, u64, i32, vp, u64, P(u64), vp]),
         "pst_num_metacells": (i32, [P(u32), P(u32), P(u32), P(u64)]),
         "pst_server_create": (i32, [P(vp), P(ServerOpts)]),
         "pst_server_add_tree": (i32, [vp, vp, P(u32)]),
+        "pst_server_add_tree_tuned": (i32, [vp, vp, P(BatchOpts), P(u32)]),
         "pst_server_submit": (i32, [vp, u32, vp, vp, i32, vp, vp]),
         "pst_server_wait": (i32, [vp, u64, u32, P(i32), P(u64)]),
         "pst_server_take": (i32, [vp, u64, vp, u64, P(u64)]),
@@ -384,13 +391,30 @@ class StaticPSTGPUArr(StaticPSTGPU):
 
 
 class BatchEngine:
-    """Batched queries on one resident tree (pst_batch_*)."""
+    """Batched queries on one resident tree (pst_batch_*).
+
+    The launch shape (block_threads, blocks_per_sm, emit_records,
+    top_pass_queries; 0 = the library's default) comes from the arguments, or from
+    `tuning`: a dict of those fields (what autotune.tune returns), or "cache" for the
+    autotuner's cached choice for this tree shape and batch size (the defaults when
+    it has none)."""
 
     def __init__(self, tree: StaticPSTGPU, max_queries: int, task_capacity: int = 0, use_graph: bool = True,
-                 blocks_per_sm: int = 0):
+                 blocks_per_sm: int = 0, block_threads: int = 0, emit_records: int = 0, top_pass_queries: int = 0,
+                 tuning=None):
         self.tree = tree
         self.max_queries = max_queries
-        o = BatchOpts(max_queries, task_capacity, 0, blocks_per_sm, int(use_graph))
+        shape = {"block_threads": block_threads, "blocks_per_sm": blocks_per_sm, "emit_records": emit_records,
+                 "top_pass_queries": top_pass_queries}
+        if tuning == "cache":
+            from .autotune import cached
+            tuning = cached(tree, max_queries)
+        if tuning:
+            shape.update({k: int(tuning[k]) for k in TUNING_FIELDS if k in tuning})
+            use_graph = bool(tuning.get("use_graph", use_graph))
+        self.shape = dict(shape, use_graph=bool(use_graph))
+        o = BatchOpts(max_queries, task_capacity, shape["block_threads"], shape["blocks_per_sm"], int(use_graph),
+                      shape["emit_records"], shape["top_pass_queries"])
         self._h = C.c_void_p()
         _check(lib().pst_batch_create(C.byref(self._h), tree.handle, C.byref(o)))
 
@@ -404,6 +428,13 @@ class BatchEngine:
             self.close()
         except Exception:
             pass
+
+    def launch_shape(self) -> dict:
+        """The engine's launch shape as resolved on the device (pst_batch_launch_shape)."""
+        t, b, g, e, q = (C.c_uint32() for _ in range(5))
+        _check(lib().pst_batch_launch_shape(self._h, C.byref(t), C.byref(b), C.byref(g), C.byref(e), C.byref(q)))
+        return {"block_threads": t.value, "blocks_per_sm": b.value, "grid": g.value, "emit_records": e.value,
+                "top_pass_queries": q.value}
 
     def last_stats(self) -> dict:
         st = BatchStats()
@@ -463,14 +494,25 @@ class Server:
                  keep_results=1):
         keep_results = int(keep_results)
         self.keep_results = keep_results
+        self.max_batch = max_batch or 1024
         o = ServerOpts(max_batch, slots_per_tree, out_budget_bytes, int(use_graph), int(keep_results))
         self._h = C.c_void_p()
         _check(lib().pst_server_create(C.byref(self._h), C.byref(o)))
         self.trees = []
 
-    def add_tree(self, tree: StaticPSTGPU) -> int:
+    def add_tree(self, tree: StaticPSTGPU, tuning=None) -> int:
+        """Registers a resident tree; `tuning` sets its engines' launch shape (a dict
+        of BatchOpts launch fields, or "cache" for the autotuner's cached choice)."""
         idx = C.c_uint32()
-        _check(lib().pst_server_add_tree(self._h, tree.handle, C.byref(idx)))
+        if tuning == "cache":
+            from .autotune import cached
+            tuning = cached(tree, self.max_batch)
+        if tuning:
+            o = BatchOpts(0, 0, *(int(tuning.get(k, 0)) for k in ("block_threads", "blocks_per_sm")), 0,
+                          int(tuning.get("emit_records", 0)), int(tuning.get("top_pass_queries", 0)))
+            _check(lib().pst_server_add_tree_tuned(self._h, tree.handle, C.byref(o), C.byref(idx)))
+        else:
+            _check(lib().pst_server_add_tree(self._h, tree.handle, C.byref(idx)))
         self.trees.append(tree)
         return idx.value
 
