@@ -345,7 +345,18 @@ def blob_volume_device(px, py, pz, seed, torch, nblobs=32, noise=0.01):
                                                            * g[0][None, None, :])
     gen = torch.Generator(device="cuda")
     gen.manual_seed(seed)
-    vol += noise * torch.randn(vol.shape, generator=gen, device="cuda", dtype=torch.float32)
+    if vol.numel() <= 1 << 30:
+        vol += noise * torch.randn(vol.shape, generator=gen, device="cuda", dtype=torch.float32)
+    else:
+        # large volumes: the noise in z-slabs of at most 2^28 values, through one buffer
+        per = max(1, (1 << 28) // (py * px))
+        buf = torch.empty((per, py, px), device="cuda", dtype=torch.float32)
+        for z0 in range(0, pz, per):
+            z1 = min(pz, z0 + per)
+            b = buf[: z1 - z0]
+            b.normal_(generator=gen)
+            vol[z0:z1].add_(b, alpha=noise)
+        del buf
     return vol
 
 
@@ -560,24 +571,32 @@ def isosurface_bench(pst, torch, dims=(512, 512, 512), seed=1):
     return out
 
 
-SERVING_VOLUMES = [(64, 64, 64), (128, 128, 128), (192, 192, 192), (256, 256, 256), (384, 384, 384),
-                   (512, 512, 512), (768, 768, 512), (1024, 1024, 512)]
+# Vertex grids of the 8 served volumes: 4^3 metacells give 2^16, 2^18, 2^20, 2^21,
+# 2^23, 2^24, 2^25 and 2^27 metacells (the largest volume, 2048^3 float32, is 34 GB
+# and is dropped once its metacells are formed).
+SERVING_VOLUMES = [(256, 256, 64), (256, 256, 256), (512, 512, 256), (512, 512, 512), (1024, 1024, 512),
+                   (1024, 1024, 1024), (2048, 2048, 512), (2048, 2048, 2048)]
 
 
 def serving_bench(pst, torch, rates=(1000, 10000, 100000), seconds=1.5, seed=11):
-    """8 resident trees of 4^3 metacells (2^12 .. 2^23 points) from Gaussian-blob
+    """8 resident trees of 4^3 metacells (2^16 .. 2^27 points) from Gaussian-blob
     volumes; Poisson arrivals; 90% isovalue queries (iso, iso) with iso ~ U[0,1] and
     10% 3-sided range queries [a, a + w], w ~ U[0, 0.1], min2 = a; results copied to
-    host memory.  Latency runs from the scheduled arrival to the result in host
-    memory (open loop)."""
+    host memory.  A batch is admitted by its exact result bytes (from its count
+    pass) into a 4 GiB result arena, or else into free HBM while 16 GiB stay free.
+    Latency runs from the scheduled arrival to the result in host memory (open
+    loop)."""
     trees = []
     for i, (px, py, pz) in enumerate(SERVING_VOLUMES):
         vol = blob_volume_device(px, py, pz, seed + i, torch)
         mc, n = pst.formMetacellTags(vol.reshape(-1), (px, py, pz), (4, 4, 4), "f32", True)
+        del vol
+        torch.cuda.empty_cache()
         trees.append(pst.StaticPSTGPU(mc, n, "f32", True))
-        del vol, mc
+        del mc
     torch.cuda.empty_cache()
-    srv = pst.Server(max_batch=1024, slots_per_tree=2, out_budget_bytes=2 << 30, keep_results=2)
+    srv = pst.Server(max_batch=1024, slots_per_tree=2, out_budget_bytes=4 << 30, keep_results=2,
+                     hbm_headroom_bytes=16 << 30)
     idx = [srv.add_tree(t) for t in trees]
     rng = np.random.default_rng(seed)
     out = {"trees_points": [t.n for t in trees]}
@@ -606,7 +625,8 @@ def serving_bench(pst, torch, rates=(1000, 10000, 100000), seconds=1.5, seed=11)
         st = srv.stats()
         out[f"{rate}qps"] = {"p50_ms": st["p50_ms"], "p90_ms": st["p90_ms"], "p99_ms": st["p99_ms"],
                              "mean_ms": st["mean_ms"], "completed": st["completed"], "failed": st["failed"],
-                             "batches": st["batches"], "points": st["points"],
+                             "batches": st["batches"], "points": st["points"], "spilled_batches": st["spilled"],
+                             "peak_arena_bytes": st["peak_out_bytes"],
                              "throughput_qps": st["completed"] / st["busy_s"] if st["busy_s"] else None}
     srv.close()
     for t in trees:

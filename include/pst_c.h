@@ -202,7 +202,8 @@ typedef struct pst_batch_opts {
 	uint32_t block_threads;    /* CTA size of the level and emit kernels: 128, 256 or 512 (0 = 256) */
 	uint32_t blocks_per_sm;    /* level-kernel CTAs per SM (0 = as many as fit) */
 	int32_t use_graph;         /* replay the pass from a captured CUDA graph */
-	uint32_t emit_records;     /* records in flight per warp when ids are emitted: 4, 8 or 16 (0 = 8) */
+	uint32_t emit_records;     /* records in flight per warp when ids are emitted: 4, 8 or 16 held in
+	                              registers, or 64 staged in shared memory (0 = 8) */
 	uint32_t top_pass_queries; /* largest waiting batch that starts with the one-CTA top pass, at
 	                              most 1024 (0 = 32) */
 } pst_batch_opts;
@@ -269,11 +270,18 @@ typedef struct pst_server_opts {
 	int32_t keep_results;      /* 1: results copied to host and kept for pst_server_take;
 	                              2: copied to host (latency includes it) then dropped;
 	                              0: results stay in device memory, only counts are kept */
+	uint64_t hbm_headroom_bytes; /* 0: a batch waits until its results fit the arena (a batch
+	                                larger than the arena is split, a request larger than it
+	                                fails with PST_ERR_NOMEM); > 0: a batch that does not fit
+	                                the arena is admitted into a device buffer of its own when
+	                                free HBM (cudaMemGetInfo) stays above this many bytes with
+	                                it, one such batch at a time */
 } pst_server_opts;
 
 typedef struct pst_server_stats {
 	uint64_t submitted, completed, failed, cancelled, batches, points;
 	uint64_t peak_out_bytes;   /* largest arena use seen */
+	uint64_t spilled;          /* batches admitted into free HBM beyond the arena */
 	double p50_ms, p90_ms, p99_ms, mean_ms, max_ms; /* over requests completed since the last reset */
 	double busy_s;             /* wall time from the first arrival to the last completion */
 } pst_server_stats;

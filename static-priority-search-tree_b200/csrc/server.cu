@@ -124,6 +124,10 @@ struct Slot {
 	uint64_t *offs_h = nullptr;
 	uint64_t out_off = 0, out_bytes = 0;
 	uint64_t total = 0;
+	bool spilled = false;        // results in a buffer of their own, outside the arena
+	char *spill_d = nullptr;     // that buffer (stream-ordered allocation on the slot's stream)
+	char *out_d = nullptr;       // where the emit writes this batch's results
+	unsigned char *out_h = nullptr;  // and where they are staged in host memory (kept results)
 
 	~Slot()
 	{
@@ -154,6 +158,12 @@ struct Server {
 	int device = 0;
 	std::vector<std::unique_ptr<TreeSlots>> trees;
 	Arena arena;
+	// Batches whose results do not fit the arena may take a device buffer of their own
+	// when free HBM allows (opts.hbm_headroom_bytes > 0), one such batch at a time;
+	// its host staging buffer is kept and grown as needed.
+	bool spill_busy = false;
+	unsigned char *spill_h = nullptr;
+	uint64_t spill_h_size = 0;
 	std::mutex mu;
 	std::condition_variable cv_work, cv_done;
 	std::deque<Request *> inbox;
@@ -194,6 +204,67 @@ struct Server {
 			last_done = std::max(last_done, r->done_ns);
 		} else {
 			st.failed++;
+		}
+	}
+
+	// Whether free HBM, less the headroom, would hold `bytes` of results.
+	bool could_spill(uint64_t bytes)
+	{
+		if (!opts.hbm_headroom_bytes)
+			return false;
+		size_t fr = 0, tot = 0;
+		if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+			cudaGetLastError();
+			return false;
+		}
+		return bytes + opts.hbm_headroom_bytes <= fr;
+	}
+
+	// Admits a batch whose results did not fit the arena into a device buffer of its
+	// own, if no other batch holds one and free HBM (cudaMemGetInfo) stays above the
+	// headroom with it.  The buffer is allocated on the slot's stream, so the
+	// allocation waits for nothing on the device's other streams.
+	bool try_spill(Slot &sl)
+	{
+		if (spill_busy || !could_spill(sl.out_bytes))
+			return false;
+		void *p = nullptr;
+		if (cudaMallocAsync(&p, std::max<uint64_t>(sl.out_bytes, 256), sl.stream) != cudaSuccess) {
+			cudaGetLastError();
+			return false;
+		}
+		if (opts.keep_results && spill_h_size < sl.out_bytes) {
+			if (spill_h)
+				cudaFreeHost(spill_h);
+			spill_h = nullptr;
+			spill_h_size = 0;
+			if (cudaMallocHost((void **) &spill_h, sl.out_bytes) != cudaSuccess) {
+				cudaGetLastError();
+				spill_h = nullptr;
+				cudaFreeAsync(p, sl.stream);
+				return false;
+			}
+			spill_h_size = sl.out_bytes;
+		}
+		sl.spill_d = static_cast<char *>(p);
+		sl.out_d = sl.spill_d;
+		sl.out_h = opts.keep_results ? spill_h : nullptr;
+		spill_busy = true;
+		std::lock_guard<std::mutex> lk(mu);
+		st.spilled++;
+		return true;
+	}
+
+	// Returns a finished batch's result space (arena range or spill buffer).
+	void release_out(Slot &sl)
+	{
+		if (sl.spilled) {
+			cudaFreeAsync(sl.spill_d, sl.stream);
+			sl.spill_d = nullptr;
+			sl.spilled = false;
+			spill_busy = false;
+		} else {
+			arena.release(sl.out_off, sl.out_bytes);
 		}
 	}
 
@@ -269,13 +340,22 @@ struct Server {
 				return true;
 			}
 			sl.out_bytes = sl.total * rs;
-			if (sl.out_bytes > arena.size) {
-				// Requests that can never fit fail; the others go back to the queue front
-				// and the tree's batches shrink until their results fit.
+			sl.spilled = false;
+			if (sl.out_bytes <= arena.size && arena.alloc(sl.out_bytes, &sl.out_off)) {
+				sl.out_d = arena.base + sl.out_off;
+				sl.out_h = arena.host ? arena.host + sl.out_off : nullptr;
+			} else if (try_spill(sl)) {
+				sl.spilled = true;
+			} else if (sl.out_bytes <= arena.size || (spill_busy && could_spill(sl.out_bytes))) {
+				return false;  // admitted once results in flight free the arena (or the spill)
+			} else {
+				// Requests that can never fit (neither the arena nor free HBM) fail; the
+				// others go back to the queue front and the tree's batches shrink until
+				// their results fit.
 				ts.batch_limit = std::max<uint32_t>(1, n / 2);
 				for (uint32_t i = n; i-- > 0;) {
 					Request *r = sl.reqs[i];
-					if (sl.counts_h[i] * rs > arena.size) {
+					if (sl.counts_h[i] * rs > arena.size && !could_spill(sl.counts_h[i] * rs)) {
 						std::vector<unsigned char> none;
 						finish(r, PST_ERR_NOMEM, sl.counts_h[i], std::move(none));
 					} else {
@@ -288,14 +368,12 @@ struct Server {
 				notify_done();
 				return true;
 			}
-			if (!arena.alloc(sl.out_bytes, &sl.out_off))
-				return false;  // admitted once results in flight free up
-			sl.eng.enqueue_emit(sl.ret, arena.base + sl.out_off, sl.total, sl.stream);
+			sl.eng.enqueue_emit(sl.ret, sl.out_d, sl.total, sl.stream);
 			check_cuda(cudaMemcpyAsync(sl.offs_h, sl.eng.offsets, ((size_t) n + 1) * 8, cudaMemcpyDeviceToHost,
 			                           sl.stream), "copy offsets");
 			if (opts.keep_results)
-				check_cuda(cudaMemcpyAsync(arena.host + sl.out_off, arena.base + sl.out_off, sl.out_bytes, cudaMemcpyDeviceToHost,
-				                           sl.stream), "copy results");
+				check_cuda(cudaMemcpyAsync(sl.out_h, sl.out_d, sl.out_bytes, cudaMemcpyDeviceToHost, sl.stream),
+				           "copy results");
 			check_cuda(cudaMemcpyAsync(sl.ctl_h, sl.eng.ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, sl.stream),
 			           "copy control");
 			check_cuda(cudaEventRecord(sl.ev, sl.stream), "event");
@@ -308,12 +386,12 @@ struct Server {
 		}
 		// SLOT_EMITTING done
 		if (sl.ctl_h->flags & (BATCH_FLAG_OUT_OVERFLOW | BATCH_FLAG_INTERNAL | BATCH_FLAG_TASK_OVERFLOW)) {
-			arena.release(sl.out_off, sl.out_bytes);
+			release_out(sl);
 			fail_all(sl, PST_ERR_INTERNAL);
 			return true;
 		}
 		const uint64_t rs = sl.eng.record_size(sl.ret);
-		const unsigned char *staged = arena.host ? arena.host + sl.out_off : nullptr;
+		const unsigned char *staged = sl.out_h;
 		for (uint32_t i = 0; i < n; i++) {
 			const uint64_t a = sl.offs_h[i], b = sl.offs_h[i + 1];
 			std::vector<unsigned char> res;
@@ -321,7 +399,7 @@ struct Server {
 				res.assign(staged + a * rs, staged + b * rs);
 			finish(sl.reqs[i], PST_OK, b - a, std::move(res));
 		}
-		arena.release(sl.out_off, sl.out_bytes);
+		release_out(sl);
 		{
 			std::lock_guard<std::mutex> lk(mu);
 			st.batches++;
@@ -429,6 +507,14 @@ struct Server {
 		cv_work.notify_all();
 		if (worker.joinable())
 			worker.join();
+		// the slots (and their streams) go with `trees` after this body; their spill
+		// buffers were freed on their streams when their batches finished
+		for (auto &ts : trees)
+			for (auto &sl : ts->slots)
+				if (sl->stream)
+					cudaStreamSynchronize(sl->stream);
+		if (spill_h)
+			cudaFreeHost(spill_h);
 	}
 };
 

@@ -45,13 +45,13 @@ TUNING_FIELDS = ("block_threads", "blocks_per_sm", "emit_records", "top_pass_que
 
 class ServerOpts(C.Structure):
     _fields_ = [("max_batch", C.c_uint32), ("slots_per_tree", C.c_uint32), ("out_budget_bytes", C.c_uint64),
-                ("use_graph", C.c_int32), ("keep_results", C.c_int32)]
+                ("use_graph", C.c_int32), ("keep_results", C.c_int32), ("hbm_headroom_bytes", C.c_uint64)]
 
 
 class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
                 ("cancelled", C.c_uint64), ("batches", C.c_uint64), ("points", C.c_uint64),
-                ("peak_out_bytes", C.c_uint64), ("p50_ms", C.c_double), ("p90_ms", C.c_double),
+                ("peak_out_bytes", C.c_uint64), ("spilled", C.c_uint64), ("p50_ms", C.c_double), ("p90_ms", C.c_double),
                 ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double), ("busy_s", C.c_double)]
 
 
@@ -491,11 +491,12 @@ class Server:
     """Serving loop over resident trees (pst_server_*)."""
 
     def __init__(self, max_batch=1024, slots_per_tree=2, out_budget_bytes=1 << 30, use_graph=True,
-                 keep_results=1):
+                 keep_results=1, hbm_headroom_bytes=0):
         keep_results = int(keep_results)
         self.keep_results = keep_results
         self.max_batch = max_batch or 1024
-        o = ServerOpts(max_batch, slots_per_tree, out_budget_bytes, int(use_graph), int(keep_results))
+        o = ServerOpts(max_batch, slots_per_tree, out_budget_bytes, int(use_graph), int(keep_results),
+                       int(hbm_headroom_bytes))
         self._h = C.c_void_p()
         _check(lib().pst_server_create(C.byref(self._h), C.byref(o)))
         self.trees = []

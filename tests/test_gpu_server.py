@@ -117,3 +117,27 @@ def test_open_loop_latency(pst):
     assert st["completed"] == n and 0 < st["p50_ms"] <= st["p99_ms"] < 1000
     srv.close()
     t.close()
+
+
+def test_admission_into_free_hbm(pst, oracle):
+    """With a headroom set, batches whose results do not fit a 1 MiB arena (one
+    request alone needs 2.4 MB) are admitted into free HBM, one at a time, instead
+    of waiting for the arena or failing; every result equals the oracle's."""
+    pts = rand_points(200000, "f32", ids="arange", seed=19)
+    ref = oracle.Orc.build(pts, "f32")
+    t = pst.StaticPSTGPU.from_numpy(pts, "f32")
+    srv = pst.Server(max_batch=8, slots_per_tree=2, out_budget_bytes=1 << 20, keep_results=1,
+                     hbm_headroom_bytes=1 << 30)
+    i = srv.add_tree(t)
+    qs = [("left", 0, 50 + 40 * k, 55 + 40 * k) for k in range(24)] + [("three", -1, 2000, -1)] * 3
+    ids = srv.submit(i, _queries(pst, qs, "f32"), ret="points")
+    srv.drain(60000)
+    for (kind, a, b, m2), rid in zip(qs, ids):
+        got = srv.take(int(rid), pts.dtype)
+        want = oracle.Orc.search_points(ref, kind, a, b, m2)
+        assert np.array_equal(oracle.canon(got), oracle.canon(want)), (kind, a, b, m2)
+    st = srv.stats()
+    assert st["failed"] == 0 and st["completed"] == len(qs)
+    assert st["spilled"] >= 3  # at least the three whole-tree requests went past the arena
+    srv.close()
+    t.close()
