@@ -792,6 +792,9 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the 2^26 batched-queries configuration")
     ap.add_argument("--no-tune", action="store_true", help="the default launch shape instead of the autotuner's")
+    ap.add_argument("--shape", default=None,
+                    help="a launch shape as JSON (block_threads, blocks_per_sm, emit_records, top_pass_queries) "
+                         "instead of tuning, e.g. to profile the shape a tuned run chose")
     ap.add_argument("--plain-queries", type=int, default=256)
     ap.add_argument("--sweep", action="store_true", help="also run every value type x kind x selectivity")
     ap.add_argument("--isosurface", action="store_true", help="also run the 512^3 isosurface pipeline")
@@ -867,7 +870,9 @@ def main():
     # ---- launch shape: the project's autotuner times its candidates on these
     # queries (not cached across runs: every box times them afresh)
     tuned = None
-    if not args.no_tune:
+    if args.shape:
+        tuned = dict(json.loads(args.shape), ms=None, default_ms=None, tried=[])
+    elif not args.no_tune:
         import importlib
         autotune = importlib.import_module("pst_b200.autotune")
         tuned = autotune.tune(tree, q_host, repeats=5, cache_path=None, task_capacity=max(1 << 20, n >> 2))
