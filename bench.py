@@ -426,7 +426,7 @@ def ips_scan(pst, torch, pts, n, dt, has_id, reps=5):
             "gbs": (n * pt_bytes + k * rec_bytes) / (ms / 1000) / 1e9, "bytes_per_point": pt_bytes}
 
 
-def sweep(pst, torch, n, seed=1):
+def sweep(pst, torch, n, peak, seed=1):
     """Per value type: build, then for each kind and selectivity a batch of 32 queries
     calibrated to s * n points each: batched pass time and one plain query; and one
     interval parallel search over the same points (returned as the "ips" rows)."""
@@ -441,6 +441,10 @@ def sweep(pst, torch, n, seed=1):
         torch.cuda.synchronize()
         build_ms = 1000 * (time.perf_counter() - t0)
         r = ips_scan(pst, torch, pts, n, dt, has_id)
+        # the survey's algorithmic bytes: dim1 and dim2 of every point, id and record of every hit
+        vs_ = 8 if dt == "f64" else 4
+        r["survey_bytes"] = n * 2 * vs_ + r["hits"] * ((4 if has_id else 0) + (4 if has_id else 2 * vs_))
+        r["frac"] = r["survey_bytes"] / (r["ms"] / 1000) / 1e9 / peak
         ips_rows.append(r)
         log(f"ips {dt}{'' if has_id else '-noid'}: {r['hits']} hits, {r['ms']:.3f} ms = {r['gbs']:.0f} GB/s")
         del pts
@@ -490,7 +494,8 @@ def sweep(pst, torch, n, seed=1):
                 plain_s = time.perf_counter() - t1
                 row = {"dtype": dt, "ids": has_id, "kind": name, "sel": s, "queries": SWEEP_BATCH,
                        "mean_points": total / SWEEP_BATCH, "batch_ms": ms, "pts_per_s": total / (ms / 1000),
-                       "gbs": total * bpp / (ms / 1000) / 1e9, "bytes_per_pt": bpp, "build_ms": build_ms,
+                       "gbs": total * bpp / (ms / 1000) / 1e9, "frac": total * bpp / (ms / 1000) / 1e9 / peak,
+                       "bytes_per_pt": bpp, "build_ms": build_ms,
                        "plain_query_ms": plain_s * 1000, "plain_pts_per_s": k1 / plain_s if plain_s else None}
                 out.append(row)
                 log(f"sweep {dt}{'' if has_id else '-noid'} {name:5s} s={s:g}: {total / SWEEP_BATCH:.3g} pts/query, "
@@ -506,7 +511,7 @@ def sweep(pst, torch, n, seed=1):
 # ---------------------------------------------------------------------------
 # isosurface pipeline (run with --isosurface)
 
-def isosurface_bench(pst, torch, dims=(512, 512, 512), seed=1):
+def isosurface_bench(pst, torch, dims=(512, 512, 512), seed=1, peak=None):
     """512^3 float32 blob volume -> 4^3 metacells (128^3 points) -> tree; at 16
     isovalues 0.05 + 0.06 i: the active metacells by twoSidedLeftSearch(iso, iso)
     (batched and plain) and by the interval parallel search, then marching cubes
@@ -561,7 +566,12 @@ def isosurface_bench(pst, torch, dims=(512, 512, 512), seed=1):
         rows.append({"iso": iso32, "active_metacells": int(k), "plain_query_ms": plain_ms, "ips_ms": ips_ms,
                      "triangles": int(len(tri)), "marching_cubes_ms": mc_ms_i})
         del tri, ids
-    out = {"volume": list(dims), "metacells": n, "form_metacells_ms": mc_ms, "build_ms": build_ms,
+    mc_bytes = dims[0] * dims[1] * dims[2] * 4 + n * 12  # read the volume, write (min, max, id) per metacell
+    out = {"volume": list(dims), "metacells": n, "form_metacells_ms": mc_ms,
+           "form_metacells_roofline": {"bound": "hbm", "algorithmic_bytes": mc_bytes,
+                                       "achieved": mc_bytes / (mc_ms / 1000) / 1e9, "peak": peak, "unit": "GB/s",
+                                       "frac": mc_bytes / (mc_ms / 1000) / 1e9 / peak if peak else None},
+           "build_ms": build_ms,
            "batched_16_isovalues_ms": batch_ms, "marching_cubes_triangles_per_s": tri_total / (mc_total_ms / 1000),
            "per_isovalue": rows}
     eng.close()
@@ -796,8 +806,9 @@ def main():
                     help="a launch shape as JSON (block_threads, blocks_per_sm, emit_records, top_pass_queries) "
                          "instead of tuning, e.g. to profile the shape a tuned run chose")
     ap.add_argument("--plain-queries", type=int, default=256)
-    ap.add_argument("--sweep", action="store_true", help="also run every value type x kind x selectivity")
-    ap.add_argument("--isosurface", action="store_true", help="also run the 512^3 isosurface pipeline")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the large-random-tree matrix (every value type x "
+                                                              "kind x selectivity, and the interval scans)")
+    ap.add_argument("--no-isosurface", action="store_true", help="skip the 512^3 isosurface pipeline")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -1015,22 +1026,29 @@ def main():
             "{:.0f}x the plain launches in queries/s".format(batched_cfg["batched_ms"], batched_cfg["batched_pts_per_s"],
                                                             batched_cfg["batched_vs_plain_qps"]))
 
-    sweep_rows = None
-    if rank == 0 and args.sweep:
+    levels_main = tree.info()["levels"]
+    sweep_rows = ips_rows = None
+    if rank == 0 and not args.no_sweep:
+        # the large random trees need the device to themselves
         eng.close()
         tree.close()
+        eng = tree = None
         torch.cuda.empty_cache()
-        sweep_rows, ips_rows = sweep(pst, torch, n)
-        tree = pst.StaticPSTGPU(gen_points_device(n, seed=1 + rank, torch=torch), n, "f32", True)
-        eng = pst.BatchEngine(tree, max_queries=NQ)
+        try:
+            sweep_rows, ips_rows = sweep(pst, torch, n, peak)
+        except Exception as e:  # an extra table must never sink the headline
+            sweep_rows = {"error": str(e)}
 
     iso_res = None
-    if rank == 0 and args.isosurface:
-        iso_res = isosurface_bench(pst, torch)
-        log("isosurface: metacells {:.2f} ms, build {:.2f} ms, 16 isovalues batched {:.3f} ms, "
-            "marching cubes {:.3g} triangles/s".format(iso_res["form_metacells_ms"], iso_res["build_ms"],
-                                                     iso_res["batched_16_isovalues_ms"],
-                                                     iso_res["marching_cubes_triangles_per_s"]))
+    if rank == 0 and not args.no_isosurface:
+        try:
+            iso_res = isosurface_bench(pst, torch, peak=peak)
+            log("isosurface: metacells {:.2f} ms, build {:.2f} ms, 16 isovalues batched {:.3f} ms, "
+                "marching cubes {:.3g} triangles/s".format(iso_res["form_metacells_ms"], iso_res["build_ms"],
+                                                         iso_res["batched_16_isovalues_ms"],
+                                                         iso_res["marching_cubes_triangles_per_s"]))
+        except Exception as e:
+            iso_res = {"error": str(e)}
 
     serving = None
     if rank == 0 and not args.no_serving:
@@ -1084,11 +1102,12 @@ def main():
             line["ips"] = ips_rows
         if iso_res is not None:
             line["isosurface"] = iso_res
-        levels = tree.info()["levels"]
-        line["gpu_launches"] = (levels + 6) * args.steps  # unpack+check + levels + 3 scan + emit per step
+        line["gpu_launches"] = (levels_main + 6) * args.steps  # unpack+check + levels + 3 scan + emit per step
         print(json.dumps(line))
-    eng.close()
-    tree.close()
+    if eng is not None:
+        eng.close()
+    if tree is not None:
+        tree.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
