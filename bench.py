@@ -637,7 +637,9 @@ def serving_bench(pst, torch, rates=(1000, 10000, 100000), seconds=1.5, seed=11)
                              "mean_ms": st["mean_ms"], "completed": st["completed"], "failed": st["failed"],
                              "batches": st["batches"], "points": st["points"], "spilled_batches": st["spilled"],
                              "peak_arena_bytes": st["peak_out_bytes"],
-                             "throughput_qps": st["completed"] / st["busy_s"] if st["busy_s"] else None}
+                             "throughput_qps": st["completed"] / st["busy_s"] if st["busy_s"] else None,
+                             "worker_cpu_s": st["worker_cpu_s"],
+                             "worker_cpu_share": st["worker_cpu_s"] / st["busy_s"] if st["busy_s"] else None}
     srv.close()
     for t in trees:
         t.close()

@@ -284,6 +284,7 @@ typedef struct pst_server_stats {
 	uint64_t spilled;          /* batches admitted into free HBM beyond the arena */
 	double p50_ms, p90_ms, p99_ms, mean_ms, max_ms; /* over requests completed since the last reset */
 	double busy_s;             /* wall time from the first arrival to the last completion */
+	double worker_cpu_s;       /* CPU time of the server's worker thread since the last reset */
 } pst_server_stats;
 
 pst_status pst_server_create(pst_server **out, const pst_server_opts *opts);

@@ -2,6 +2,7 @@
 // exact output bytes of each batch's count pass, overlapping batches on separate
 // streams, p50/p99 latency from arrival to host result.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -173,6 +174,8 @@ struct Server {
 	bool stop = false;
 	std::thread worker;
 	std::string worker_error;
+	std::atomic<uint64_t> worker_cpu_ns{0};  // the worker thread's CPU time so far
+	uint64_t worker_cpu_base = 0;            // ... at the last statistics reset
 	// statistics (guarded by mu)
 	pst_server_stats st{};
 	std::vector<double> lat_ms;
@@ -473,6 +476,12 @@ struct Server {
 				for (auto &ts : trees)
 					for (auto &sl : ts->slots)
 						progress |= step(*ts, *sl);
+				{
+					timespec c{};
+					clock_gettime(CLOCK_THREAD_CPUTIME_ID, &c);
+					worker_cpu_ns.store((uint64_t) c.tv_sec * 1000000000ull + (uint64_t) c.tv_nsec,
+					                    std::memory_order_relaxed);
+				}
 				if (!progress) {
 					if (inflight) {
 						// GPU steps in flight: poll their events again right away.  A timed
@@ -711,6 +720,7 @@ void server_stats(Server *s, pst_server_stats *out)
 		sum += x;
 	st.mean_ms = v.empty() ? 0.0 : sum / (double) v.size();
 	st.busy_s = s->last_done > s->first_arrival ? (double) (s->last_done - s->first_arrival) / 1e9 : 0.0;
+	st.worker_cpu_s = (double) (s->worker_cpu_ns.load() - s->worker_cpu_base) / 1e9;
 	*out = st;
 }
 
@@ -723,6 +733,7 @@ void server_reset_stats(Server *s)
 	s->lat_ms.clear();
 	s->first_arrival = s->last_done = 0;
 	s->arena.peak = s->arena.used;
+	s->worker_cpu_base = s->worker_cpu_ns.load();
 }
 
 void server_destroy(Server *s) { delete s; }

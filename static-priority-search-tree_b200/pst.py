@@ -52,7 +52,8 @@ class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
                 ("cancelled", C.c_uint64), ("batches", C.c_uint64), ("points", C.c_uint64),
                 ("peak_out_bytes", C.c_uint64), ("spilled", C.c_uint64), ("p50_ms", C.c_double), ("p90_ms", C.c_double),
-                ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double), ("busy_s", C.c_double)]
+                ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double), ("busy_s", C.c_double),
+                ("worker_cpu_s", C.c_double)]
 
 
 class BatchStats(C.Structure):
