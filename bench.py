@@ -588,14 +588,16 @@ SERVING_VOLUMES = [(256, 256, 64), (256, 256, 256), (512, 512, 256), (512, 512, 
                    (1024, 1024, 1024), (2048, 2048, 512), (2048, 2048, 2048)]
 
 
-def serving_bench(pst, torch, rates=(1000, 10000, 100000), seconds=1.5, seed=11):
+def serving_bench(pst, torch, seconds=1.5, seed=11):
     """8 resident trees of 4^3 metacells (2^16 .. 2^27 points) from Gaussian-blob
     volumes; Poisson arrivals; 90% isovalue queries (iso, iso) with iso ~ U[0,1] and
-    10% 3-sided range queries [a, a + w], w ~ U[0, 0.1], min2 = a; results copied to
-    host memory.  A batch is admitted by its exact result bytes (from its count
-    pass) into a 4 GiB result arena, or else into free HBM while 16 GiB stay free.
-    Latency runs from the scheduled arrival to the result in host memory (open
-    loop)."""
+    10% 3-sided range queries [a, a + w], w ~ U[0, 0.1], min2 = a.  A batch is
+    admitted by its exact result bytes (from its count pass) into a 4 GiB result
+    arena, or else into free HBM while 16 GiB stay free.  Latency runs from the
+    scheduled arrival (open loop) to the result complete in device memory
+    (`device`, at 1k, 10k and 100k qps) and to the result in host memory (`host`,
+    at 1k and 10k qps: at 100k qps the offered results, ~240 GB/s of ids, are far
+    beyond the host link, so the queue only grows)."""
     trees = []
     for i, (px, py, pz) in enumerate(SERVING_VOLUMES):
         vol = blob_volume_device(px, py, pz, seed + i, torch)
@@ -605,42 +607,45 @@ def serving_bench(pst, torch, rates=(1000, 10000, 100000), seconds=1.5, seed=11)
         trees.append(pst.StaticPSTGPU(mc, n, "f32", True))
         del mc
     torch.cuda.empty_cache()
-    srv = pst.Server(max_batch=1024, slots_per_tree=2, out_budget_bytes=4 << 30, keep_results=2,
-                     hbm_headroom_bytes=16 << 30)
-    idx = [srv.add_tree(t) for t in trees]
-    rng = np.random.default_rng(seed)
     out = {"trees_points": [t.n for t in trees]}
-    for rate in rates:
-        n = int(rate * seconds)
-        gaps = rng.exponential(1.0 / rate, n)
-        tree_of = rng.integers(0, len(trees), n).astype(np.uint32)
-        three = rng.random(n) < 0.1
-        a = rng.uniform(0, 1, n).astype(np.float32)
-        w = rng.uniform(0, 0.1, n).astype(np.float32)
-        kinds = np.where(three, 0, 1).astype(np.int32)
-        q = pst.make_queries(kinds, np.where(three, a, 0), np.where(three, a + w, a), a, "f32")
-        srv.reset_stats()
-        t0 = time.monotonic_ns() + 2_000_000
-        arrive = t0 + np.cumsum(gaps * 1e9).astype(np.uint64)
-        k = 0
-        while k < n:
-            now = time.monotonic_ns()
-            j = int(np.searchsorted(arrive, now, side="right"))
-            if j > k:
-                srv.submit(tree_of[k:j], q[k:j], arrival_ns=arrive[k:j])
-                k = j
-            else:
-                time.sleep(20e-6)
-        srv.drain(120000)
-        st = srv.stats()
-        out[f"{rate}qps"] = {"p50_ms": st["p50_ms"], "p90_ms": st["p90_ms"], "p99_ms": st["p99_ms"],
-                             "mean_ms": st["mean_ms"], "completed": st["completed"], "failed": st["failed"],
-                             "batches": st["batches"], "points": st["points"], "spilled_batches": st["spilled"],
-                             "peak_arena_bytes": st["peak_out_bytes"],
-                             "throughput_qps": st["completed"] / st["busy_s"] if st["busy_s"] else None,
-                             "worker_cpu_s": st["worker_cpu_s"],
-                             "worker_cpu_share": st["worker_cpu_s"] / st["busy_s"] if st["busy_s"] else None}
-    srv.close()
+    for mode, keep, rates in (("device", 0, (1000, 10000, 100000)), ("host", 2, (1000, 10000))):
+        srv = pst.Server(max_batch=1024, slots_per_tree=2, out_budget_bytes=4 << 30, keep_results=keep,
+                         hbm_headroom_bytes=16 << 30)
+        idx = [srv.add_tree(t) for t in trees]
+        rng = np.random.default_rng(seed)
+        res = {}
+        for rate in rates:
+            n = int(rate * seconds)
+            gaps = rng.exponential(1.0 / rate, n)
+            tree_of = np.asarray(idx, np.uint32)[rng.integers(0, len(trees), n)]
+            three = rng.random(n) < 0.1
+            a = rng.uniform(0, 1, n).astype(np.float32)
+            w = rng.uniform(0, 0.1, n).astype(np.float32)
+            kinds = np.where(three, 0, 1).astype(np.int32)
+            q = pst.make_queries(kinds, np.where(three, a, 0), np.where(three, a + w, a), a, "f32")
+            srv.reset_stats()
+            t0 = time.monotonic_ns() + 2_000_000
+            arrive = t0 + np.cumsum(gaps * 1e9).astype(np.uint64)
+            k = 0
+            while k < n:
+                now = time.monotonic_ns()
+                j = int(np.searchsorted(arrive, now, side="right"))
+                if j > k:
+                    srv.submit(tree_of[k:j], q[k:j], arrival_ns=arrive[k:j])
+                    k = j
+                else:
+                    time.sleep(20e-6)
+            srv.drain(120000)
+            st = srv.stats()
+            res[f"{rate}qps"] = {"p50_ms": st["p50_ms"], "p90_ms": st["p90_ms"], "p99_ms": st["p99_ms"],
+                                 "mean_ms": st["mean_ms"], "completed": st["completed"], "failed": st["failed"],
+                                 "batches": st["batches"], "points": st["points"], "spilled_batches": st["spilled"],
+                                 "peak_arena_bytes": st["peak_out_bytes"],
+                                 "throughput_qps": st["completed"] / st["busy_s"] if st["busy_s"] else None,
+                                 "worker_cpu_s": st["worker_cpu_s"],
+                                 "worker_cpu_share": st["worker_cpu_s"] / st["busy_s"] if st["busy_s"] else None}
+        srv.close()
+        out[mode] = res
     for t in trees:
         t.close()
     return out
@@ -1056,8 +1061,9 @@ def main():
     if rank == 0 and not args.no_serving:
         try:
             serving = serving_bench(pst, torch)
-            log("serving: " + ", ".join(f"{k} p50 {v['p50_ms']:.2f} p99 {v['p99_ms']:.2f} ms"
-                                        for k, v in serving.items() if k.endswith("qps")))
+            for mode in ("device", "host"):
+                log(f"serving ({mode}): " + ", ".join(f"{k} p50 {v['p50_ms']:.2f} p99 {v['p99_ms']:.2f} ms"
+                                                      for k, v in serving[mode].items()))
         except Exception as e:
             serving = {"error": str(e)}
 

@@ -202,8 +202,7 @@ typedef struct pst_batch_opts {
 	uint32_t block_threads;    /* CTA size of the level and emit kernels: 128, 256 or 512 (0 = 256) */
 	uint32_t blocks_per_sm;    /* level-kernel CTAs per SM (0 = as many as fit) */
 	int32_t use_graph;         /* replay the pass from a captured CUDA graph */
-	uint32_t emit_records;     /* records in flight per warp when ids are emitted: 4, 8 or 16 held in
-	                              registers, or 64 staged in shared memory (0 = 8) */
+	uint32_t emit_records;     /* records in flight per warp when ids are emitted: 4, 8 or 16 (0 = 8) */
 	uint32_t top_pass_queries; /* largest waiting batch that starts with the one-CTA top pass, at
 	                              most 1024 (0 = 32) */
 } pst_batch_opts;

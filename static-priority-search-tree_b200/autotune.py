@@ -7,9 +7,8 @@ launch shape is a set of choices the engine takes at creation (pst_batch_opts):
 
   * block_threads: CTA size of the level and emit kernels (128, 256, 512);
   * blocks_per_sm: level-kernel CTAs per SM (all that fit, or half of them);
-  * emit_records: 64-slot records each emit warp keeps in flight (4, 8, 16 with the
-    ids in registers: more loads in flight against more registers and fewer
-    resident warps; 64 with the id rows staged in shared memory by cp.async);
+  * emit_records: 64-slot records each emit warp keeps in flight (4, 8, 16: more
+    loads in flight against more registers and fewer resident warps);
   * top_pass_queries: the largest waiting batch that starts with the one-CTA top
     pass, which walks the upper levels with the frontier kept by one CTA instead of
     a kernel launch per level (batches of up to 1024 queries: off, or the batch).
@@ -64,7 +63,7 @@ def cached(tree: StaticPSTGPU, nq: int, cache_path: Path | None = None) -> dict 
     return _load(path).get(cache_key(tree, nq))
 
 
-def candidates(nq: int, block_threads=(128, 256, 512), blocks_per_sm=(0, -2), emit_records=(4, 8, 16, 64)):
+def candidates(nq: int, block_threads=(128, 256, 512), blocks_per_sm=(0, -2), emit_records=(4, 8, 16)):
     """The launch shapes tried for a batch of nq queries (blocks_per_sm -2 = half of
     what fits; it is resolved against the device when the engine is made)."""
     tops = (1, nq) if 1 < nq <= MAX_TOP_PASS else (0,)

@@ -411,8 +411,13 @@ __device__ __forceinline__ void level_body(const TreeDev<T> &t, const QDev<T> &q
 		// expansion of the previous level's alive records into their child blocks, 32
 		// consecutive records per warp (their children stay together in the next
 		// level's region, which keeps that level's chunks local)
-		for (uint64_t wb = (gwarp - wp - ws) * 32; wb < n_prev; wb += wr * 32) {
-			const bool valid = wb + lane < n_prev;
+		// A narrow level (records fewer than a quarter of the record warps' lanes)
+		// gives each warp 8 consecutive records instead of 32: four times the warps
+		// work on it, each with a quarter of the dependent load rounds, and the
+		// children of 8 consecutive parents still stay together in the next level.
+		const uint64_t per = n_prev * 4 < wr * 32 ? 8 : 32;
+		for (uint64_t wb = (gwarp - wp - ws) * per; wb < n_prev; wb += wr * per) {
+			const bool valid = lane < per && wb + lane < n_prev;
 			const uint4 mine = valid ? w.rec[base_prev + wb + lane] : make_uint4(0, 0, 0, 0);
 			uint4 child[2];
 			uint32_t pts;
@@ -749,143 +754,6 @@ __global__ void __launch_bounds__(THREADS) k_emit(TreeDev<T> t, WorkDev w, void 
 	}
 }
 
-// The emit of ids with the records' id rows staged in shared memory by cp.async
-// instead of held in registers: each warp keeps ES_STAGES - 1 batches of 32
-// records (8 KiB of id rows each) in flight while it writes the results of the
-// batch before them, so a warp has 16 KiB of loads outstanding against the 2 KiB
-// of the register path (emit_records 8).  Only the 16-byte chunks (four slots) that
-// hold a reported slot are copied.  A batch's output ranges are claimed when it is
-// issued, so the claims' atomics also overlap the writes.  (Selected by
-// emit_records = ES_RECORDS.)
-constexpr int ES_THREADS = 128;
-constexpr int ES_STAGES = 3;
-constexpr uint32_t ES_RECORDS = 64;  // the emit_records value that selects this kernel
-
-struct EmitMeta {
-	uint4 rec[32];
-	unsigned long long ob[32];
-};
-constexpr size_t ES_IDS_BYTES = 32 * 64 * 4;  // one batch's id rows
-constexpr size_t ES_WARP_BYTES = ES_STAGES * (ES_IDS_BYTES + sizeof(EmitMeta));
-constexpr size_t ES_SMEM_BYTES = (ES_THREADS / 32) * ES_WARP_BYTES;
-static_assert(ES_WARP_BYTES % 16 == 0 && ES_IDS_BYTES % 16 == 0, "16-byte aligned stages");
-
-template <typename T>
-__global__ void __launch_bounds__(ES_THREADS) k_emit_staged(TreeDev<T> t, WorkDev w, uint32_t *__restrict__ out,
-                                                          uint64_t capacity)
-{
-	extern __shared__ __align__(16) unsigned char es_smem[];
-	__shared__ uint64_t s_total;
-	__shared__ EmitStage s_stage[ES_THREADS / 32];
-	if (threadIdx.x == 0) {
-		uint64_t b = 0;
-		for (uint32_t e = 0; e < t.levels; e++)
-			b += w.ctl->lvl_cnt[e];
-		s_total = b;
-	}
-	__syncthreads();
-	if (w.ctl->total > capacity || (w.ctl->flags & BATCH_FLAG_TASK_OVERFLOW)) {
-		if (blockIdx.x == 0 && threadIdx.x == 0 && w.ctl->total > capacity)
-			atomicOr(&w.ctl->flags, BATCH_FLAG_OUT_OVERFLOW);
-		return;
-	}
-	const uint64_t total = s_total < w.rec_cap ? s_total : w.rec_cap;
-	const uint32_t nro = min(w.ctl->rec_cnt, w.ro_cap);
-	const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-	const uint64_t gwarps = (uint64_t) gridDim.x * (ES_THREADS / 32);
-	const uint64_t gwarp = (uint64_t) blockIdx.x * (ES_THREADS / 32) + warp;
-	unsigned char *wbase = es_smem + warp * ES_WARP_BYTES;
-	uint32_t *ids_s = reinterpret_cast<uint32_t *>(wbase);                       // [stage][record][64]
-	EmitMeta *meta = reinterpret_cast<EmitMeta *>(wbase + ES_STAGES * ES_IDS_BYTES);  // [stage]
-	const uint64_t stride = gwarps * 32;
-
-	// Reads the batch of records at wb, claims their output ranges and starts the
-	// copies of their id rows into stage st (one commit group per batch, empty past
-	// the end, so that the group count stays uniform).
-	auto issue = [&](uint64_t wb, int st) {
-		if (wb < total) {
-			const bool v = wb + lane < total;
-			uint4 m = v ? w.rec[wb + lane] : make_uint4(0, 0, 0, 0);
-			meta[st].rec[lane] = m;
-			__syncwarp();
-			const uint32_t c = lane & 15;
-			uint32_t *dst = ids_s + (size_t) st * 32 * 64;
-#pragma unroll 4
-			for (int k = 0; k < 16; k++) {
-				// lanes 0-15 take record 2k, lanes 16-31 record 2k + 1, one chunk each
-				const int r = 2 * k + (int) (lane >> 4);
-				const uint4 rc = meta[st].rec[r];
-				if (((rc.z | rc.w) >> (2 * c)) & 3u)
-					cp_async16(dst + r * 64 + 4 * c, t.id + rc.x + 4 * c);
-			}
-			const uint64_t ob = claim_output(w, m.y, __popc(m.z) + __popc(m.w), v);
-			guard_claim(w, m, ob, capacity);
-			meta[st].rec[lane] = m;  // cleared if its claim would overrun (never: see guard_claim)
-			meta[st].ob[lane] = ob;
-		}
-		cp_async_commit();
-	};
-
-	uint64_t wb_issue = gwarp * 32, wb = gwarp * 32;
-#pragma unroll
-	for (int s = 0; s < ES_STAGES - 1; s++) {
-		issue(wb_issue, s);
-		wb_issue += stride;
-	}
-	int st_issue = ES_STAGES - 1, st = 0;
-	const uint32_t lt = lanemask_lt();
-	while (wb < total) {
-		issue(wb_issue, st_issue);
-		wb_issue += stride;
-		st_issue = st_issue + 1 == ES_STAGES ? 0 : st_issue + 1;
-		cp_async_wait_group<ES_STAGES - 1>();
-		__syncwarp();
-		const uint32_t *row = ids_s + (size_t) st * 32 * 64 + 2 * lane;
-#pragma unroll 8
-		for (int r = 0; r < 32; r++) {
-			const uint4 rc = meta[st].rec[r];
-			const uint32_t b2 = ((rc.z >> lane) & 1u) | (((rc.w >> lane) & 1u) << 1);
-			if (b2) {
-				const uint2 v = *reinterpret_cast<const uint2 *>(row + r * 64);
-				const uint64_t o = meta[st].ob[r] + __popc(rc.z & lt) + __popc(rc.w & lt);
-				// evict-first: the output streams through L2 once
-				if (b2 & 1u)
-					__stcs(out + o, v.x);
-				if (b2 & 2u)
-					__stcs(out + o + (b2 & 1u), v.y);
-			}
-		}
-		__syncwarp();  // the stage is refilled by a later issue
-		st = st + 1 == ES_STAGES ? 0 : st + 1;
-		wb += stride;
-	}
-	cp_async_wait_all();
-	for (uint64_t wb2 = gwarp * 32; wb2 < nro; wb2 += gwarps * 32) {
-		const bool valid = wb2 + lane < nro;
-		uint4 mine = valid ? w.ro[wb2 + lane] : make_uint4(0, 0, 0, 0);
-		const uint64_t ob = claim_output(w, mine.y, __popc(mine.z) + __popc(mine.w), valid);
-		guard_claim(w, mine, ob, capacity);
-		emit_blocks<T, true, false, 8>(t, mine, ob, valid, s_stage[warp], out);
-	}
-}
-
-template <typename T>
-void launch_emit_staged(const TreeDev<T> &tv, const WorkDev &w, void *out, uint64_t capacity, cudaStream_t s)
-{
-	static const int occ = [] {
-		cudaFuncSetAttribute(k_emit_staged<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) ES_SMEM_BYTES);
-		int o = 0;
-		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_emit_staged<T>, ES_THREADS, ES_SMEM_BYTES) !=
-		    cudaSuccess) {
-			cudaGetLastError();
-			o = 1;
-		}
-		return o > 0 ? o : 1;
-	}();
-	k_emit_staged<T><<<(unsigned) (device_info().sms * occ), ES_THREADS, ES_SMEM_BYTES, s>>>(
-	    tv, w, static_cast<uint32_t *>(out), capacity);
-}
-
 // Grid of k_emit: as many CTAs as fit on the device at once (its own occupancy,
 // which can differ from the level kernel's), so the grid-stride loop has no tail wave.
 template <typename T, bool HAS_ID, bool POINTS, int THREADS, int U>
@@ -972,12 +840,6 @@ template <typename T, bool HAS_ID, bool POINTS>
 void launch_emit(const TreeDev<T> &tv, const WorkDev &w, void *out, uint64_t capacity, uint32_t threads, uint32_t u,
                  cudaStream_t s)
 {
-	if constexpr (HAS_ID && !POINTS) {
-		if (u == ES_RECORDS) {
-			launch_emit_staged<T>(tv, w, out, capacity, s);
-			return;
-		}
-	}
 	switch (threads) {
 	case 128: launch_emit_t<T, HAS_ID, POINTS, 128>(tv, w, out, capacity, u, s); break;
 	case 512: launch_emit_t<T, HAS_ID, POINTS, 512>(tv, w, out, capacity, u, s); break;
@@ -1037,8 +899,8 @@ void Batch::init(TreeStorage *t, const pst_batch_opts &o)
 	if (threads != 128 && threads != 256 && threads != 512)
 		fail(PST_ERR_INVALID, "block_threads must be 0, 128, 256 or 512");
 	emit_u = o.emit_records ? o.emit_records : 8;
-	if (emit_u != 4 && emit_u != 8 && emit_u != 16 && emit_u != ES_RECORDS)
-		fail(PST_ERR_INVALID, "emit_records must be 0, 4, 8, 16 or " + std::to_string(ES_RECORDS));
+	if (emit_u != 4 && emit_u != 8 && emit_u != 16)
+		fail(PST_ERR_INVALID, "emit_records must be 0, 4, 8 or 16");
 	top_q = o.top_pass_queries ? o.top_pass_queries : SMALL_BATCH_Q;
 	if (top_q > MAX_TOP_PASS_Q)
 		fail(PST_ERR_INVALID, "top_pass_queries must be at most " + std::to_string(MAX_TOP_PASS_Q));

@@ -32,9 +32,9 @@ def test_every_launch_shape_matches_the_oracle(pst, oracle, ret):
             want.append(oracle.canon(oracle.Orc.search_ids(ref, kind, a, b, m2)))
         else:
             want.append(oracle.canon(oracle.Orc.search_points(ref, kind, a, b, m2)))
-    for bt, er, tq, bps in itertools.product((128, 256, 512), (4, 8, 16, 64), (0, 1024), (0, 1)):
+    for bt, er, tq, bps in itertools.product((128, 256, 512), (4, 8, 16), (0, 1024), (0, 1)):
         eng = pst.BatchEngine(tree, max_queries=len(qs), block_threads=bt, emit_records=er, top_pass_queries=tq,
-                              blocks_per_sm=bps, task_capacity=64)  # small frontier: growth on the way
+                              blocks_per_sm=bps, task_capacity=4096)  # small frontier: growth on the way
         shape = eng.launch_shape()
         assert shape["block_threads"] == bt and shape["emit_records"] == er
         assert shape["top_pass_queries"] == (tq or 32)
