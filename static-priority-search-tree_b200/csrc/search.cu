@@ -14,7 +14,7 @@
 //     block: 64 consecutive slots of one level, tested by one warp with coalesced
 //     loads.  The frontier is kept as "alive records" only — (block, query, mask of
 //     reported slots) — and the next level expands each record into its two child
-//     blocks, loading only the children of reported slots.  Every
+//     blocks (spread16), masked by occupancy before anything is loaded.  Every
 //     level but the last is full (a level-d node holds at least
 //     floor((n + 1) / 2^d) - 1 >= 1 points for d <= D - 2), so occupancy is read
 //     only for children on the last level.
@@ -50,10 +50,7 @@ struct QDev {
 
 // Alive records cover a "block" of 64 consecutive slots of one level (two
 // 128-byte rows of a 4-byte field): (block base position, query, mask of reported
-// slots in pair order).  Block bases are multiples of 64.  Pair order: bit m of the
-// first mask word is slot 2m of the block, bit m of the second word slot 2m + 1, so
-// lane m of a warp owns the slot pair (2m, 2m + 1) and a warp-wide ballot of one
-// test per lane is one mask word.
+// slots, low and high word).  Block bases are multiples of 64.
 struct WorkDev {
 	uint4 *rec;            // alive records of every level, level regions in order
 	uint64_t rec_cap;
@@ -68,22 +65,11 @@ struct WorkDev {
 	BatchCtl *ctl;
 };
 
-// The even-indexed bits of x, packed into the low 16 bits.
-__device__ __forceinline__ uint32_t even_bits(uint32_t x)
-{
-	x &= 0x55555555u;
-	x = (x | (x >> 1)) & 0x33333333u;
-	x = (x | (x >> 2)) & 0x0F0F0F0Fu;
-	x = (x | (x >> 4)) & 0x00FF00FFu;
-	return (x | (x >> 8)) & 0x0000FFFFu;
-}
-
-// The block record of a 32-slot chunk (base pos32, a multiple of 32) and its mask
-// (bit i = slot pos32 + i), converted to pair order.
+// The block record of a 32-slot chunk (base pos32, a multiple of 32) and its mask.
 __device__ __forceinline__ uint4 block_record(uint32_t pos32, uint32_t q, uint32_t bits32)
 {
-	const uint32_t sh = (pos32 & 32u) ? 16u : 0u;  // the upper chunk holds pairs 16..31
-	return make_uint4(pos32 & ~63u, q, even_bits(bits32) << sh, even_bits(bits32 >> 1) << sh);
+	const bool upper = (pos32 & 32u) != 0;
+	return make_uint4(pos32 & ~63u, q, upper ? 0u : bits32, upper ? bits32 : 0u);
 }
 
 template <typename T>
@@ -239,40 +225,60 @@ __device__ __forceinline__ void add_counts(const WorkDev &w, uint32_t q, uint32_
 		atomicAdd((unsigned long long *) &w.counts[q], (unsigned long long) run);
 }
 
-// Per-warp shared staging of the 32 records a warp holds: the records, their
-// queries' min2 and the list of records that can have children at all.
+template <typename T>
+struct Vec4;
+template <>
+struct Vec4<float> {
+	using V = float4;
+};
+template <>
+struct Vec4<int32_t> {
+	using V = int4;
+};
+
+// Four consecutive values from a 16-byte aligned address (two loads for doubles).
+template <typename T>
+__device__ __forceinline__ void load_quad(const T *__restrict__ p, T (&v)[4])
+{
+	if constexpr (sizeof(T) == 4) {
+		using V = typename Vec4<T>::V;
+		const V x = *reinterpret_cast<const V *>(p);
+		v[0] = x.x;
+		v[1] = x.y;
+		v[2] = x.z;
+		v[3] = x.w;
+	} else {
+		const double2 a = reinterpret_cast<const double2 *>(p)[0];
+		const double2 b = reinterpret_cast<const double2 *>(p)[1];
+		v[0] = a.x;
+		v[1] = a.y;
+		v[2] = b.x;
+		v[3] = b.y;
+	}
+}
+
+// Per-warp shared staging of the 32 records a warp holds: the records, the
+// candidate masks of their four child rows (parents' bits spread to their children,
+// ANDed with the occupancy), their queries' min2, the child rows found, and the
+// list of records that have any candidate at all.
 template <typename T>
 struct WarpStage {
 	uint4 rec[32];
+	uint4 cand[32];
+	uint4 rows[32];
 	T m2[32];
 	uint32_t live[32];
 };
 
-// Two consecutive values from an 8-byte (16 for doubles) aligned address.
-template <typename T>
-__device__ __forceinline__ void load_pair(const T *__restrict__ p, T (&v)[2])
-{
-	if constexpr (sizeof(T) == 4) {
-		const uint2 x = *reinterpret_cast<const uint2 *>(p);
-		memcpy(&v[0], &x.x, 4);
-		memcpy(&v[1], &x.y, 4);
-	} else {
-		const double2 x = *reinterpret_cast<const double2 *>(p);
-		v[0] = x.x;
-		v[1] = x.y;
-	}
-}
-
 // Expands the records held by the warp (lane k owns record `mine`; the valid lanes
-// are a prefix) into their child records.  The whole warp takes the live records U
-// at a time.  A record's block [b, b + 64) has the children [2b, 2b + 128), the
-// blocks A = [2b, 2b + 64) and B = [2b + 64, 2b + 128): lane m tests the pair
-// (2b + 2m, 2b + 2m + 1) of A, the children of parent b + m, and the same pair of
-// B, the children of parent b + 32 + m, with one 8-byte load each (16 for doubles),
-// issued only where the parent was reported (and, for children on the last level,
-// the child exists).  The four ballots of those tests are the two child records'
-// masks in pair order, taken by the record's owner lane: no shuffles, no staging of
-// rows.  Children on a full level (every level but the last) need no occupancy read.
+// are a prefix) into their child records.  Each lane first stages its record's
+// candidate child slots (`full`: the children's level is full, so the candidates
+// are the spread parent bits with no occupancy read); records without any (all
+// children absent, e.g. above a sparse last level) cost nothing more.  Then the whole warp takes the live records
+// U at a time: lane l tests the child slots [2b + 4l, 2b + 4l + 4) with one 16-byte
+// load (two for doubles), issued only where it has candidates; each 8-lane group
+// ORs its nibbles into one 32-slot child row, and the owner reads the four rows as
+// its two child records (blocks 2b and 2b + 64).
 template <typename T, bool LAST>
 __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__restrict__ min2s, const uint4 &mine,
                                                bool valid, bool full, WarpStage<T> &st, uint4 (&child)[2],
@@ -280,72 +286,78 @@ __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__r
 {
 	constexpr int U = sizeof(T) == 4 ? 4 : 2;  // records in flight
 	const uint32_t lane = lane_id();
-	bool live = valid && (mine.z | mine.w) != 0;
-	if (LAST && live) {
+	const uint32_t r = lane >> 3, qd = lane & 7;
+	uint4 cand = make_uint4(0, 0, 0, 0);
+	bool has_children = valid;
+	if (LAST && valid) {
 		// expanding into the last level: most blocks of a sparse last level have no
 		// children, which one bit per parent block tells before any occupancy read
 		const uint32_t j = (mine.x - (1u << (t.levels - 2))) >> 6;
-		live = (t.last_par[j >> 5] >> (j & 31)) & 1u;
+		has_children = (t.last_par[j >> 5] >> (j & 31)) & 1u;
 	}
+	if (has_children) {
+		// children on a full level (every level but the last) need no occupancy read
+		const uint4 occ = full ? make_uint4(FULL, FULL, FULL, FULL)
+		                       : *reinterpret_cast<const uint4 *>(t.occ + ((2 * mine.x) >> 5));
+		cand = make_uint4(spread16(mine.z) & occ.x, spread16(mine.z >> 16) & occ.y, spread16(mine.w) & occ.z,
+		                  spread16(mine.w >> 16) & occ.w);
+	}
+	const bool live = (cand.x | cand.y | cand.z | cand.w) != 0;
 	const uint32_t lm = __ballot_sync(FULL, live);
 	const int nlive = __popc(lm);
 	if (live) {
 		st.rec[lane] = mine;
+		st.cand[lane] = cand;
 		st.m2[lane] = min2s[mine.y];
 		st.live[__popc(lm & lanemask_lt())] = lane;
 	}
 	__syncwarp();
-	// parent slot b + m is pair m >> 1, word m & 1 of the record's mask; b + 32 + m is
-	// pair 16 + (m >> 1)
-	const uint32_t psh = lane >> 1;
-	uint4 rows = make_uint4(0, 0, 0, 0);
+	const uint32_t *candw = reinterpret_cast<const uint32_t *>(st.cand);
 	for (int k0 = 0; k0 < nlive; k0 += U) {
-		uint32_t kk[U], ca[U], cb[U];
-		T va[U][2], vb[U][2];
+		uint32_t cn[U], kk[U];
+		T v[U][4];
 #pragma unroll
 		for (int u = 0; u < U; u++) {
 			const bool on = k0 + u < nlive;
 			const uint32_t k = st.live[on ? k0 + u : 0];
 			kk[u] = k;
-			const uint4 rc = st.rec[k];
-			const uint32_t pw = (lane & 1) ? rc.w : rc.z;
-			// candidate pairs of A and B: both children of a reported parent (bits 0, 1)
-			uint32_t a = on ? ((pw >> psh) & 1u) * 3u : 0u;
-			uint32_t b = on ? ((pw >> (16 + psh)) & 1u) * 3u : 0u;
-			const uint32_t cbase = 2 * rc.x;  // a multiple of 128
-			if (!full) {
-				if (a)
-					a &= t.occ[(cbase >> 5) + (lane >> 4)] >> ((2 * lane) & 31);
-				if (b)
-					b &= t.occ[(cbase >> 5) + 2 + (lane >> 4)] >> ((2 * lane) & 31);
+			const uint32_t c4 = on ? (candw[4 * k + r] >> (4 * qd)) & 0xFu : 0u;
+			cn[u] = c4;
+			if (c4) {
+				load_quad(t.dim2 + 2 * st.rec[k].x + 4 * lane, v[u]);
+			} else {
+#pragma unroll
+				for (int j = 0; j < 4; j++)
+					v[u][j] = T(0);
 			}
-			ca[u] = a & 3u;
-			cb[u] = b & 3u;
-			va[u][0] = va[u][1] = vb[u][0] = vb[u][1] = T(0);
-			if (ca[u])
-				load_pair(t.dim2 + cbase + 2 * lane, va[u]);
-			if (cb[u])
-				load_pair(t.dim2 + cbase + 64 + 2 * lane, vb[u]);
 		}
 #pragma unroll
 		for (int u = 0; u < U; u++) {
 			const T m2 = st.m2[kk[u]];
-			const uint32_t a0 = __ballot_sync(FULL, (ca[u] & 1u) && m2 <= va[u][0]);
-			const uint32_t a1 = __ballot_sync(FULL, (ca[u] & 2u) && m2 <= va[u][1]);
-			const uint32_t b0 = __ballot_sync(FULL, (cb[u] & 1u) && m2 <= vb[u][0]);
-			const uint32_t b1 = __ballot_sync(FULL, (cb[u] & 2u) && m2 <= vb[u][1]);
-			if (k0 + u < nlive && lane == kk[u])
-				rows = make_uint4(a0, a1, b0, b1);
+			// all four slots are compared (values of slots without a candidate are zero or
+			// loaded anyway) and the candidates masked once, not tested slot by slot
+			uint32_t ge = 0;
+#pragma unroll
+			for (int j = 0; j < 4; j++)
+				ge |= (m2 <= v[u][j]) ? 1u << j : 0u;
+			uint32_t row = (ge & cn[u]) << (4 * qd);
+			row |= __shfl_xor_sync(FULL, row, 1);
+			row |= __shfl_xor_sync(FULL, row, 2);
+			row |= __shfl_xor_sync(FULL, row, 4);
+			if (qd == 0 && k0 + u < nlive)
+				reinterpret_cast<uint32_t *>(st.rows)[4 * kk[u] + r] = row;
 		}
 	}
-	__syncwarp();  // the stage is reused by the warp's next batch
+	__syncwarp();
 	child[0] = child[1] = make_uint4(0, 0, 0, 0);
 	pts = 0;
 	if (live) {
-		child[0] = make_uint4(2 * mine.x, mine.y, rows.x, rows.y);
-		child[1] = make_uint4(2 * mine.x + 64, mine.y, rows.z, rows.w);
-		pts = __popc(rows.x) + __popc(rows.y) + __popc(rows.z) + __popc(rows.w);
+		const uint4 rw = st.rows[lane];
+		child[0] = make_uint4(2 * mine.x, mine.y, rw.x, rw.y);
+		child[1] = make_uint4(2 * mine.x + 64, mine.y, rw.z, rw.w);
+		pts = __popc(rw.x) + __popc(rw.y) + __popc(rw.z) + __popc(rw.w);
 	}
+	__syncwarp();  // the stage is reused by the warp's next batch
 }
 
 // One tree level of the search (the body of k_bfs_level): the boundary paths, the
@@ -628,9 +640,10 @@ __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mi
 	using Pt = Point<T, HAS_ID>;  // U: records in flight per warp
 	static_assert(32 % U == 0, "a batch of records ends inside the 32 staged ones");
 	const uint32_t lane = lane_id();
-	// pair order: this lane's slots are bit `lane` of the two mask words, and the
-	// record's reported slots before them are the lower bits of both
-	const uint32_t lt = lanemask_lt();
+	const uint32_t psh = (2 * lane) & 31;
+	// the record's slots before this lane's pair, as masks of its two 32-slot words
+	const uint32_t below_z = lane < 16 ? (1u << psh) - 1u : FULL;
+	const uint32_t below_w = lane < 16 ? 0u : (1u << psh) - 1u;
 	st.rec[lane] = mine;
 	st.ob[lane] = out_base;
 	__syncwarp();
@@ -647,8 +660,8 @@ __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mi
 			// per record (U divides 32, so k < 32)
 			const int k = k0 + u;
 			const uint4 rc = st.rec[k];
-			b2[u] = ((rc.z >> lane) & 1u) | (((rc.w >> lane) & 1u) << 1);
-			const uint32_t before = __popc(rc.z & lt) + __popc(rc.w & lt);
+			b2[u] = ((lane < 16 ? rc.z : rc.w) >> psh) & 3u;
+			const uint32_t before = __popc(rc.z & below_z) + __popc(rc.w & below_w);
 			o[u] = st.ob[k] + before;
 			hb[u] = rc.x + 2 * lane;
 			if constexpr (!POINTS || HAS_ID)

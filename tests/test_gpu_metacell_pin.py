@@ -72,7 +72,9 @@ def test_reference_metacells_equal_oracle_and_library(pst, oracle, dt, dims, mc)
     mine, n2 = pst.formMetacellTags(vol_d, dims, mc, dt, True)
     assert n2 == n
     got = mine.cpu().numpy().view(rec)
-    assert got.tobytes() == ref.tobytes()
+    # field by field: the reference leaves the records' padding bytes as they were
+    for f in ("dim1", "dim2", "id"):
+        assert got[f].tobytes() == ref[f].tobytes(), f
 
 
 def test_reference_harness_refuses_sizes_it_mishandles():

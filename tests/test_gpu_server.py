@@ -121,8 +121,8 @@ def test_open_loop_latency(pst):
 
 def test_admission_into_free_hbm(pst, oracle):
     """With a headroom set, batches whose results do not fit a 1 MiB arena (one
-    request alone needs 2.4 MB) are admitted into free HBM, one at a time, instead
-    of waiting for the arena or failing; every result equals the oracle's."""
+    request alone needs 2.4 MB) are admitted into free HBM, one batch at a time,
+    instead of failing; every result equals the oracle's."""
     pts = rand_points(200000, "f32", ids="arange", seed=19)
     ref = oracle.Orc.build(pts, "f32")
     t = pst.StaticPSTGPU.from_numpy(pts, "f32")
@@ -138,6 +138,6 @@ def test_admission_into_free_hbm(pst, oracle):
         assert np.array_equal(oracle.canon(got), oracle.canon(want)), (kind, a, b, m2)
     st = srv.stats()
     assert st["failed"] == 0 and st["completed"] == len(qs)
-    assert st["spilled"] >= 3  # at least the three whole-tree requests went past the arena
+    assert st["spilled"] >= 1  # the whole-tree requests (batched together or not) went past the arena
     srv.close()
     t.close()
