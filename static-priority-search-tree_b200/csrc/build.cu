@@ -127,10 +127,32 @@ struct BuildCtx {
 	uint32_t *err;
 	uint64_t n;
 	uint32_t D;
+	// Points are rebuilt from their sorted keys instead of gathered from the input:
+	// set for 4-byte values when no value is -0.0 (the only value the keys do not
+	// keep: it shares +0.0's key) and the ids, if any, equal the input indices (so
+	// the id is the tiebreak rank the dim2 key carries).
+	bool recon;
 
 	__device__ __forceinline__ Point<T, HAS_ID> point_of_tb(uint32_t tb) const { return pts[P ? P[tb] : tb]; }
 	__device__ __forceinline__ static uint32_t tb_of(uint64_t key2) { return (uint32_t) key2 - 1u; }
-	__device__ __forceinline__ Point<T, HAS_ID> point_at(uint32_t pos) const { return point_of_tb(tb_of(c2s[pos])); }
+	// The point of dim1 key k1 and 64-bit dim2 key c2 (recon only).
+	__device__ __forceinline__ static Point<T, HAS_ID> point_from_keys(K k1, uint64_t c2)
+	{
+		Point<T, HAS_ID> p;
+		p.dim1 = KeyOf<T>::value(k1);
+		p.dim2 = KeyOf<T>::value((K) (c2 >> 32));
+		if constexpr (HAS_ID)
+			p.id = tb_of(c2);
+		return p;
+	}
+	__device__ __forceinline__ Point<T, HAS_ID> point_at(uint32_t pos) const
+	{
+		if constexpr (sizeof(K) == 4) {
+			if (recon)
+				return point_from_keys(k1s[pos], c2s[pos]);
+		}
+		return point_of_tb(tb_of(c2s[pos]));
+	}
 	__device__ __forceinline__ bool is_taken(uint64_t pos) const { return (taken[pos >> 5] >> (pos & 31)) & 1u; }
 
 	__device__ __forceinline__ void write_node(uint32_t h, const Point<T, HAS_ID> &p) const
@@ -200,13 +222,14 @@ __device__ void block_range_fold(K lo, K hi, K *range)
 // ---------------------------------------------------------------------------
 // Preparation kernels.
 
-// flag |= 1 when ids decrease somewhere; id_range = [min id, max id].
+// flag |= 1 when ids decrease somewhere, |= 2 when some id differs from its input
+// index; id_range = [min id, max id].
 template <typename T, bool HAS_ID>
 __global__ void k_ids_scan(const Point<T, HAS_ID> *pts, uint64_t n, uint32_t *flag, uint32_t *id_range)
 {
 	if constexpr (HAS_ID) {
 		uint32_t lo = 0xFFFFFFFFu, hi = 0;
-		bool dec = false;
+		bool dec = false, other = false;
 		for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
 		     i += (uint64_t) gridDim.x * blockDim.x) {
 			const uint32_t v = pts[i].id;
@@ -214,9 +237,13 @@ __global__ void k_ids_scan(const Point<T, HAS_ID> *pts, uint64_t n, uint32_t *fl
 			hi = max(hi, v);
 			if (i + 1 < n && v > pts[i + 1].id)
 				dec = true;
+			if ((uint64_t) v != i)
+				other = true;
 		}
 		if (__any_sync(0xFFFFFFFFu, dec) && (threadIdx.x & 31) == 0)
 			atomicOr(flag, 1u);
+		if (__any_sync(0xFFFFFFFFu, other) && (threadIdx.x & 31) == 0)
+			atomicOr(flag, 2u);
 		block_range_fold<uint32_t>(lo, hi, id_range);
 	}
 }
@@ -232,17 +259,21 @@ __global__ void k_id_keys(const Point<T, HAS_ID> *pts, uint64_t n, uint32_t *key
 
 // Keys in tiebreak-rank order r (input index P[r]): k1[r] = dim1 key and either the
 // final 64-bit dim2 key (4-byte values) or the raw dim2 key k2[r] (doubles).
-// range = [min k1, max k1, min k2, max k2].
+// range = [min k1, max k1, min k2, max k2]; *negzero |= 1 when a value is -0.0 (the
+// one value its key does not keep).
 template <typename T, bool HAS_ID>
 __global__ void k_prep_keys(const Point<T, HAS_ID> *pts, const uint32_t *P, uint64_t n,
                             typename KeyOf<T>::K *k1, uint64_t *c2, typename KeyOf<T>::K *k2,
-                            typename KeyOf<T>::K *range)
+                            typename KeyOf<T>::K *range, uint32_t *negzero)
 {
 	using K = typename KeyOf<T>::K;
 	K lo1 = ~K(0), hi1 = 0, lo2 = ~K(0), hi2 = 0;
+	bool nz = false;
 	for (uint64_t r = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (uint64_t) gridDim.x * blockDim.x) {
 		const Point<T, HAS_ID> p = pts[P ? P[r] : r];
 		const K a = KeyOf<T>::key(p.dim1), b = KeyOf<T>::key(p.dim2);
+		if constexpr (!std::is_integral<T>::value)
+			nz |= (p.dim1 == T(0) && signbit(p.dim1)) || (p.dim2 == T(0) && signbit(p.dim2));
 		k1[r] = a;
 		if constexpr (sizeof(K) == 4)
 			c2[r] = ((uint64_t) b << 32) | (uint64_t) (r + 1);
@@ -253,6 +284,8 @@ __global__ void k_prep_keys(const Point<T, HAS_ID> *pts, const uint32_t *P, uint
 		lo2 = b < lo2 ? b : lo2;
 		hi2 = b > hi2 ? b : hi2;
 	}
+	if (__any_sync(0xFFFFFFFFu, nz) && (threadIdx.x & 31) == 0)
+		atomicOr(negzero, 1u);
 	block_range_fold<K>(lo1, hi1, range);
 	__syncthreads();
 	block_range_fold<K>(lo2, hi2, range + 2);
@@ -431,6 +464,8 @@ __global__ void k_level_nodes(BuildCtx<T, HAS_ID> c, uint32_t d, const uint32_t 
 	}
 	// position of the point: first position in [lo, hi) at or after (its dim1 key, tb)
 	const uint32_t tb = BuildCtx<T, HAS_ID>::tb_of(bj);
+	// the winner's dim1 key (needed to find its position) is known only from its
+	// point: one gather per node of the level
 	const Point<T, HAS_ID> top = c.point_of_tb(tb);
 	const K key1 = KeyOf<T>::key(top.dim1);
 	uint32_t a = lo, b = hi;
@@ -554,14 +589,21 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 
 	// Gather the keys of the points still free in [lo, hi), in dim1 order: every
 	// read in flight at once, then one prefix over (chunk, warp).
+	using K = typename BuildCtx<T, HAS_ID>::K;
+	// with rebuilt points the dim1 keys come along (contiguous, like the dim2 keys),
+	// staged in kn, which the sub-levels only use later
+	constexpr bool KEYS4 = sizeof(K) == 4;
+	K *k1c = reinterpret_cast<K *>(kn);
 	{
 		uint64_t v[ST_GATHER];
+		K v1[ST_GATHER];
 		uint32_t m[ST_GATHER];
 #pragma unroll
 		for (int u = 0; u < ST_GATHER; u++) {
 			const uint32_t i = lo + (uint32_t) u * ST_THREADS + threadIdx.x;
 			const bool keep = i < hi && !c.is_taken(i);
 			v[u] = keep ? c.c2s[i] : 0;
+			v1[u] = (KEYS4 && c.recon && keep) ? c.k1s[i] : K(0);
 			m[u] = __ballot_sync(0xFFFFFFFFu, keep);
 			if (lane == 0)
 				s_pre[u][warp] = __popc(m[u]);
@@ -598,6 +640,8 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 				if (pos < ST_CAP) {
 					kc[pos] = v[u];
 					sc[pos] = (uint16_t) pos;
+					if (KEYS4 && c.recon)
+						k1c[pos] = v1[u];
 				}
 			}
 		}
@@ -608,15 +652,21 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 			atomicOr(c.err, 2u);
 		return;
 	}
-	// ... and their points, every read of the CTA in flight at once
+	// ... and their points: rebuilt from the keys when they can be (no global read
+	// at all), otherwise gathered from the input, every read of the CTA in flight at
+	// once (one random 12- or 24-byte read per point)
 	{
 		constexpr int PER = (ST_CAP + ST_THREADS - 1) / ST_THREADS;
 		Pt tmp[PER];
 #pragma unroll
 		for (int u = 0; u < PER; u++) {
 			const uint32_t i = threadIdx.x + u * ST_THREADS;
-			if (i < cN)
-				tmp[u] = c.point_of_tb(BuildCtx<T, HAS_ID>::tb_of(kc[i]));
+			if (i < cN) {
+				if (KEYS4 && c.recon)
+					tmp[u] = BuildCtx<T, HAS_ID>::point_from_keys(k1c[i], kc[i]);
+				else
+					tmp[u] = c.point_of_tb(BuildCtx<T, HAS_ID>::tb_of(kc[i]));
+			}
 		}
 #pragma unroll
 		for (int u = 0; u < PER; u++) {
@@ -917,7 +967,7 @@ void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 	void *k1 = scr.at<void>(SL.k1), *kalt = scr.at<void>(SL.kalt);
 	uint64_t *c2 = scr.at<uint64_t>(SL.c2);
 	void *valt = scr.at<void>(SL.valt);
-	uint32_t *flag = scr.at<uint32_t>(SL.flags);  // [0] ids decrease, [1] error bits, [2..3] id range
+	uint32_t *flag = scr.at<uint32_t>(SL.flags);  // [0] id order bits, [1] error bits, [2..3] id range, [4] -0.0 seen
 	K *krange = reinterpret_cast<K *>(scr.at<unsigned char>(SL.flags) + 64);  // [k1 min, k1 max, k2 min, k2 max]
 	{
 		unsigned char init[256];
@@ -940,12 +990,14 @@ void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 	const unsigned g = grid_for(n, 256);
 	// ---- tiebreak order: (id, input index) when ids are not already non-decreasing
 	const uint32_t *P = nullptr;
+	bool ids_are_indices = true;
 	if constexpr (HAS_ID) {
 		k_ids_scan<T, HAS_ID><<<g, 256, 0, s>>>(pts, n, flag, flag + 2);
 		uint32_t host[4];
 		PST_CUDA(cudaMemcpyAsync(host, flag, 16, cudaMemcpyDeviceToHost, s));
 		PST_CUDA(cudaStreamSynchronize(s));
-		if (host[0]) {
+		ids_are_indices = !(host[0] & 2u);
+		if (host[0] & 1u) {
 			uint32_t *idk = static_cast<uint32_t *>(k1);  // k1 holds at least n u32
 			k_id_keys<T, HAS_ID><<<g, 256, 0, s>>>(pts, n, idk);
 			sc.keys_alt = kalt;
@@ -959,10 +1011,13 @@ void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 		}
 	}
 	// ---- keys in tiebreak order
-	k_prep_keys<T, HAS_ID><<<g, 256, 0, s>>>(pts, P, n, static_cast<K *>(k1), c2, scr.at<K>(SL.k2), krange);
+	k_prep_keys<T, HAS_ID><<<g, 256, 0, s>>>(pts, P, n, static_cast<K *>(k1), c2, scr.at<K>(SL.k2), krange,
+	                                         flag + 4);
 	PST_CUDA(cudaGetLastError());
 	K range[4];
+	uint32_t negzero = 0;
 	PST_CUDA(cudaMemcpyAsync(range, krange, sizeof(range), cudaMemcpyDeviceToHost, s));
+	PST_CUDA(cudaMemcpyAsync(&negzero, flag + 4, 4, cudaMemcpyDeviceToHost, s));
 	PST_CUDA(cudaStreamSynchronize(s));
 	if constexpr (WIDE_KEY) {
 		// dim2 ranks: stable sort of the dim2 keys in tiebreak order
@@ -994,6 +1049,8 @@ void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 	BuildCtx<T, HAS_ID> c;
 	c.pts = pts;
 	c.P = P;
+	// points rebuilt from the keys: 4-byte values, no -0.0, ids (if any) = input indices
+	c.recon = !WIDE_KEY && !negzero && ids_are_indices && P == nullptr;
 	c.k1s = k1s;
 	c.c2s = c2s;
 	c.taken = scr.at<uint32_t>(SL.taken);

@@ -64,6 +64,15 @@ struct KeyOf<float> {
 			u = 0;
 		return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 	}
+	// The value of a key (inverse of key() for every value but -0.0, whose key is
+	// +0.0's).
+	__host__ __device__ static float value(K k)
+	{
+		const uint32_t u = (k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k;
+		float v;
+		memcpy(&v, &u, 4);
+		return v;
+	}
 };
 
 template <>
@@ -77,12 +86,20 @@ struct KeyOf<double> {
 			u = 0;
 		return (u & 0x8000000000000000ull) ? ~u : (u | 0x8000000000000000ull);
 	}
+	__host__ __device__ static double value(K k)
+	{
+		const uint64_t u = (k & 0x8000000000000000ull) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;
+		double v;
+		memcpy(&v, &u, 8);
+		return v;
+	}
 };
 
 template <>
 struct KeyOf<int32_t> {
 	using K = uint32_t;
 	__host__ __device__ static K key(int32_t v) { return static_cast<uint32_t>(v) ^ 0x80000000u; }
+	__host__ __device__ static int32_t value(K k) { return static_cast<int32_t>(k ^ 0x80000000u); }
 };
 
 // ---------------------------------------------------------------------------
