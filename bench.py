@@ -445,6 +445,8 @@ def sweep(pst, torch, n, peak, seed=1):
         vs_ = 8 if dt == "f64" else 4
         r["survey_bytes"] = n * 2 * vs_ + r["hits"] * ((4 if has_id else 0) + (4 if has_id else 2 * vs_))
         r["frac"] = r["survey_bytes"] / (r["ms"] / 1000) / 1e9 / peak
+        # the records are read whole (the id sits between the values): bytes of the layout
+        r["frac_layout"] = r["gbs"] / peak
         ips_rows.append(r)
         log(f"ips {dt}{'' if has_id else '-noid'}: {r['hits']} hits, {r['ms']:.3f} ms = {r['gbs']:.0f} GB/s")
         del pts
