@@ -223,7 +223,7 @@ def calibrate(count_fn, kinds, sel, anchor, n, iters=24, domain=float(1 << 24), 
     return bounds(best)
 
 
-def disjoint_plan(nq, seed, domain=float(1 << 24)):
+def disjoint_plan(nq, seed, domain=float(1 << 24), origin=0.0):
     """nq 3-sided queries over consecutive, disjoint dim1 ranges that cover the whole
     domain, with min2 = the range's lower bound, so every point is reported by
     exactly one query (dim2 >= dim1 >= the bound): no point is read for two queries.
@@ -232,7 +232,7 @@ def disjoint_plan(nq, seed, domain=float(1 << 24)):
     min2) in float32."""
     rng = np.random.default_rng(seed)
     w = np.exp(rng.uniform(np.log(SEL_LO), np.log(SEL_HI), nq))
-    edges = (np.concatenate([[0.0], np.cumsum(w / w.sum())]) * domain).astype(np.float32)
+    edges = (origin + np.concatenate([[0.0], np.cumsum(w / w.sum())]) * domain).astype(np.float32)
     edges[0] = np.float32(-np.inf)
     a = edges[:-1]
     # each range ends just below where the next one starts (bounds are inclusive)
@@ -533,7 +533,20 @@ def isosurface_bench(pst, torch, dims=(512, 512, 512), seed=1, peak=None):
     vol = blob_volume_device(*dims, seed, torch).reshape(-1).contiguous()
     recs, n = timed(lambda: pst.formMetacellTags(vol, dims, (4, 4, 4), "f32", True))[0], None
     (recs, n), mc_ms = timed(lambda: pst.formMetacellTags(vol, dims, (4, 4, 4), "f32", True))
-    tree, build_ms = timed(lambda: pst.StaticPSTGPU(recs, n, "f32", True), reps=1)
+    # build time: mean of three builds after a first one, each timed alone (the previous
+    # tree is released outside the timed region)
+    pst.StaticPSTGPU(recs, n, "f32", True).close()
+    bms = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        ev[0].record()
+        tree = pst.StaticPSTGPU(recs, n, "f32", True)
+        ev[1].record()
+        ev[1].synchronize()
+        bms.append(ev[0].elapsed_time(ev[1]))
+        if len(bms) < 3:
+            tree.close()
+    build_ms = statistics.mean(bms)
     isos = [0.05 + 0.06 * i for i in range(16)]
     eng = pst.BatchEngine(tree, max_queries=16)
     q = pst.make_queries(np.full(16, 1, np.int32), np.zeros(16), np.array(isos), np.array(isos), "f32")
@@ -828,12 +841,17 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
+    # one GPU per rank (LOCAL_RANK); a box with fewer GPUs than ranks runs several
+    # ranks per GPU, which only a functional check of the N > 1 path should do
+    torch.cuda.set_device(local % max(torch.cuda.device_count(), 1))
     dist = None
+    cdev = "cuda"  # device of the collectives' tensors
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = os.environ.get("PST_BENCH_DIST_BACKEND", "nccl")  # gloo: the functional check
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        cdev = "cuda" if backend == "nccl" else "cpu"
     n = 1 << args.points_log2
     stream = torch.cuda.current_stream()
 
@@ -874,11 +892,11 @@ def main():
         _spec = _ilu.spec_from_file_location("pst_sharded", PKG_DIR / "sharded.py")
         sharded = _ilu.module_from_spec(_spec)
         _spec.loader.exec_module(sharded)
-        qb = torch.from_numpy(q_host.view(np.uint8).copy()).to("cuda")
+        qb = torch.from_numpy(q_host.view(np.uint8).copy()).to(cdev)
         blocks = [torch.empty_like(qb) for _ in range(world)]
         dist.all_gather(blocks, qb)
-        rb = [torch.zeros(4, dtype=torch.float64, device="cuda") for _ in range(world)]
-        dist.all_gather(rb, torch.tensor(bounds, dtype=torch.float64, device="cuda"))
+        rb = [torch.zeros(4, dtype=torch.float64, device=cdev) for _ in range(world)]
+        dist.all_gather(rb, torch.tensor(bounds, dtype=torch.float64, device=cdev))
         ranges = torch.stack(rb).cpu().numpy()
         q_all = torch.cat(blocks).cpu().numpy().view(pst.pst.QUERY_NP)
         ak, a1, a2, a3 = query_fields(q_all)
@@ -940,10 +958,10 @@ def main():
     log(f"timed {args.steps} steps: {my_ms:.3f} ms/step, {total} points/step")
     pts_all, ms_all = float(total), my_ms
     if dist:
-        t = torch.tensor([my_ms], device="cuda")
+        t = torch.tensor([my_ms], device=cdev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_all = float(t.item())
-        p = torch.tensor([float(total)], device="cuda", dtype=torch.float64)
+        p = torch.tensor([float(total)], device=cdev, dtype=torch.float64)
         dist.all_reduce(p, op=dist.ReduceOp.SUM)
         pts_all = float(p.item())
     value = pts_all / (ms_all / 1000.0)
@@ -965,8 +983,13 @@ def main():
         ev[1].synchronize()
         if i >= args.warmup:
             e2e_ms.append(ev[0].elapsed_time(ev[1]))
-    e2e_val = total / (statistics.mean(e2e_ms) / 1000.0) * world
-    log(f"e2e {statistics.mean(e2e_ms):.3f} ms/step")
+    e2e_mean = statistics.mean(e2e_ms)
+    if dist:
+        t = torch.tensor([e2e_mean], device=cdev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_mean = float(t.item())
+    e2e_val = pts_all / (e2e_mean / 1000.0)
+    log(f"e2e {e2e_mean:.3f} ms/step")
 
     # ---- plain per-query drop-in path on a sample of the same queries: the blocking
     # call that hands back a device array of exactly `count` ids (as the reference's
@@ -989,7 +1012,7 @@ def main():
     # ---- the same tree, queries over disjoint dim1 ranges: every point reported
     # exactly once per pass, so no row is read for two queries (no L2 reuse between
     # queries); the pass's HBM efficiency without overlap
-    dk, da, db, dc = disjoint_plan(NQ, 13)
+    dk, da, db, dc = disjoint_plan(NQ, 13, origin=float(rank) * SLAB)  # this shard's slab
     dq_host = pst.make_queries(dk, da, db, dc, "f32")
     dq_dev = torch.from_numpy(dq_host.view(np.uint8).copy()).to("cuda")
     st_d, tot_d = eng.run(dq_dev, out, offs, queries_on_device=True, sync=True)
