@@ -9,7 +9,17 @@ once by bisection on exact counts.
 
 Metric: points reported per second (value: inputs resident in HBM, results to a
 device buffer; e2e: the same call from host memory with the query upload and the
-result download inside the timed region).
+result download inside the timed region).  The engine's launch shape is picked by
+the project's autotuner on the step's queries before timing.
+
+Beside the headline, the line carries: the same tree under 4096 queries over
+disjoint ranges (every point reported once), the 2^26 exponential-gap
+configuration against 4096 plain launches, construction with its roofline, the
+2^28 large-random-tree matrix and interval scans, the 512^3 isosurface pipeline,
+serving over 8 resident trees, and the reference's CPU search timed on a sample.
+
+With N > 1 ranks (torchrun) each rank holds one dim1 shard of one point set
+(weak scaling) and answers the queries routed to it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
