@@ -3,10 +3,16 @@
  * the parity tests, the smoke check and the CPU-baseline leg of the benchmark
  * use it as the checker.  No product code path links or calls it.
  *
- * Parity status: pinned.  Every function here is checked against the reference
- * implementation itself (StaticPSTCPUIter compiled unmodified from its own
- * sources into oracle/_ref/) by tests/test_oracle_pin.py, and against golden
- * fixtures produced by that compiled reference (tests/golden/make_golden.py).
+ * Parity status: pinned.  The tree, the searches and the interval scan are
+ * checked against the reference implementation itself (StaticPSTCPUIter compiled
+ * unmodified from its own sources into oracle/_ref/libpstref.so) by
+ * tests/test_oracle_pin.py, and against golden fixtures produced by that compiled
+ * reference (tests/golden/make_golden.py).  Metacell formation is checked against
+ * the reference's own metacell kernel (compiled from its sources into
+ * oracle/_ref/libmcref.so by ref_metacells.cu) in tests/test_gpu_metacell_pin.py,
+ * on the sizes that kernel handles (it needs a GPU to run).  The many-query brute
+ * force (orc_brute_multi) is checked against the one-query brute force in
+ * tests/test_oracle_brute_multi.py.
  *
  * Restated from the reference (paths relative to the reference project):
  *   - point total order          helpers/point-struct.h:62-92, :154-188
