@@ -287,6 +287,9 @@ __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__r
 	constexpr int U = sizeof(T) == 4 ? 4 : 2;  // records in flight
 	const uint32_t lane = lane_id();
 	const uint32_t r = lane >> 3, qd = lane & 7;
+	// the record's min2 stays in its owner lane's register (its load overlaps the
+	// staging below) and is broadcast by a shuffle where it is compared
+	const T m2_own = valid ? min2s[mine.y] : T(0);
 	uint4 cand = make_uint4(0, 0, 0, 0);
 	bool has_children = valid;
 	if (LAST && valid) {
@@ -308,7 +311,6 @@ __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__r
 	if (live) {
 		st.rec[lane] = mine;
 		st.cand[lane] = cand;
-		st.m2[lane] = min2s[mine.y];
 		st.live[__popc(lm & lanemask_lt())] = lane;
 	}
 	__syncwarp();
@@ -333,7 +335,7 @@ __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__r
 		}
 #pragma unroll
 		for (int u = 0; u < U; u++) {
-			const T m2 = st.m2[kk[u]];
+			const T m2 = __shfl_sync(FULL, m2_own, kk[u]);
 			// all four slots are compared (values of slots without a candidate are zero or
 			// loaded anyway) and the candidates masked once, not tested slot by slot
 			uint32_t ge = 0;
@@ -428,9 +430,16 @@ __device__ __forceinline__ void level_body(const TreeDev<T> &t, const QDev<T> &q
 		// work on it, each with a quarter of the dependent load rounds, and the
 		// children of 8 consecutive parents still stay together in the next level.
 		const uint64_t per = n_prev * 4 < wr * 32 ? 8 : 32;
-		for (uint64_t wb = (gwarp - wp - ws) * per; wb < n_prev; wb += wr * per) {
-			const bool valid = lane < per && wb + lane < n_prev;
-			const uint4 mine = valid ? w.rec[base_prev + wb + lane] : make_uint4(0, 0, 0, 0);
+		uint64_t wb = (gwarp - wp - ws) * per;
+		bool nvalid = lane < per && wb + lane < n_prev;
+		uint4 nxt = nvalid ? w.rec[base_prev + wb + lane] : make_uint4(0, 0, 0, 0);
+		for (; wb < n_prev; wb += wr * per) {
+			const bool valid = nvalid;
+			const uint4 mine = nxt;
+			// the next round's record is read now, its load overlapping this round
+			const uint64_t nb = wb + wr * per;
+			nvalid = lane < per && nb + lane < n_prev;
+			nxt = nvalid ? w.rec[base_prev + nb + lane] : make_uint4(0, 0, 0, 0);
 			uint4 child[2];
 			uint32_t pts;
 			expand_records<T, LAST>(t, qd.min2, mine, valid, !LAST && d + 1 < t.levels, stage,
