@@ -433,6 +433,23 @@ __device__ __forceinline__ void level_body(const TreeDev<T> &t, const QDev<T> &q
 		uint64_t wb = (gwarp - wp - ws) * per;
 		bool nvalid = lane < per && wb + lane < n_prev;
 		uint4 nxt = nvalid ? w.rec[base_prev + wb + lane] : make_uint4(0, 0, 0, 0);
+		// A round's children are reserved with one atomic per warp, but written in the
+		// next round, after that round's loads: the reservation's latency overlaps them.
+		// Pending: this lane's parent block (children at 2p and 2p + 64), query, the
+		// four child mask words, its first slot offset in the warp's run, and the
+		// warp's reservation (lane 31; ~0 = none or refused).
+		uint32_t pp = 0, pq = 0, pofs = 0, pres = ~0u;
+		uint4 pm = make_uint4(0, 0, 0, 0);
+		auto flush = [&]() {
+			const uint32_t r0 = __shfl_sync(FULL, pres, 31);
+			if (r0 == ~0u)
+				return;
+			uint64_t sl = base_cur + r0 + pofs;
+			if (pm.x | pm.y)
+				w.rec[sl++] = make_uint4(2 * pp, pq, pm.x, pm.y);
+			if (pm.z | pm.w)
+				w.rec[sl] = make_uint4(2 * pp + 64, pq, pm.z, pm.w);
+		};
 		for (; wb < n_prev; wb += wr * per) {
 			const bool valid = nvalid;
 			const uint4 mine = nxt;
@@ -449,8 +466,26 @@ __device__ __forceinline__ void level_body(const TreeDev<T> &t, const QDev<T> &q
 			if (__ballot_sync(FULL, pts != 0) == 0)
 				continue;
 			add_counts(w, mine.y, pts, valid);
-			append_blocks<2>(w, d, base_cur, child);
+			flush();
+			const uint32_t nrec = ((child[0].z | child[0].w) ? 1u : 0u) + ((child[1].z | child[1].w) ? 1u : 0u);
+			const uint32_t inc = warp_incl_scan(nrec);
+			pres = ~0u;
+			if (lane == 31) {
+				// inc = the warp's total here (pts != 0 somewhere, so it is positive)
+				const uint32_t off = atomicAdd(&w.ctl->lvl_cnt[d], inc);
+				if (base_cur + off + inc > w.rec_cap) {
+					atomicMax((unsigned long long *) &w.ctl->need_tasks, (unsigned long long) (base_cur + off + inc));
+					atomicOr(&w.ctl->flags, BATCH_FLAG_TASK_OVERFLOW);
+				} else {
+					pres = off;
+				}
+			}
+			pp = mine.x;
+			pq = mine.y;
+			pofs = inc - nrec;
+			pm = make_uint4(child[0].z, child[0].w, child[1].z, child[1].w);
 		}
+		flush();
 	}
 }
 
