@@ -365,17 +365,19 @@ __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__r
 // One tree level of the search (the body of k_bfs_level): the boundary paths, the
 // seeds and the expansion of the previous level's records, spread over `gwarps`
 // warps (of the grid, or of the one CTA of k_bfs_cta).
+// cnt: the level's boundary-path tasks and seeds (ctl->path_cnt[d], seed_cnt[d]
+// capped at path_cap) in shared memory, read by the caller with the level's other
+// counters.
 template <typename T, bool LAST>
 __device__ __forceinline__ void level_body(const TreeDev<T> &t, const QDev<T> &qd, const WorkDev &w, uint32_t d,
                                            uint64_t gwarp, uint64_t gwarps, uint64_t base_prev, uint64_t base_cur,
-                                           uint64_t n_prev, WarpStage<T> &stage)
+                                           uint64_t n_prev, const uint32_t *cnt, WarpStage<T> &stage)
 {
 	const uint32_t lane = lane_id();
+	const uint32_t np = cnt[0], ns = cnt[1];
 	// The level's three kinds of work go to disjoint sets of warps so that their
 	// dependent-load chains overlap instead of adding up: a few warps take the
 	// boundary paths, a few the seeds, the rest the records.
-	const uint32_t np = min(w.ctl->path_cnt[d], w.path_cap);
-	const uint32_t ns = min(w.ctl->seed_cnt[d], w.path_cap);
 	const uint64_t cap = gwarps / 8 + 1;
 	const uint64_t wp = min((uint64_t) (np + 31) / 32, cap);
 	const uint64_t ws = min((uint64_t) (ns + 31) / 32, cap);
@@ -501,21 +503,29 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_bfs_level(TreeDev<T
 	// scheduled while that level drains, and wait here until it has completed and
 	// its writes are visible (a no-op for an ordinary launch).
 	asm volatile("griddepcontrol.wait;" ::: "memory");
+	__shared__ uint64_t s_base[2];
+	__shared__ uint32_t s_cnt[3];  // paths, seeds, stop
+	__shared__ WarpStage<T> s_stage[THREADS / 32];
+	if (threadIdx.x == 0) {
+		// the level's counters, all in one round trip: the previous region's start and
+		// length, this level's paths and seeds, and the flags
+		const uint64_t b = d ? w.ctl->lvl_base[d - 1] : 0;
+		const uint32_t c = d ? w.ctl->lvl_cnt[d - 1] : 0u;
+		const uint32_t np = w.ctl->path_cnt[d], ns = w.ctl->seed_cnt[d], fl = w.ctl->flags;
+		s_base[0] = b;
+		s_base[1] = b + c;
+		s_cnt[0] = min(np, w.path_cap);
+		s_cnt[1] = min(ns, w.path_cap);
+		s_cnt[2] = fl & BATCH_FLAG_TASK_OVERFLOW;
+		if (blockIdx.x == 0)
+			w.ctl->lvl_base[d] = b + c;
+	}
+	__syncthreads();
 	// Once the frontier has overflowed, the reservation that crossed the capacity
 	// left some slots below it unwritten, so nothing of the previous level may be
 	// read: the pass stops here and the host repeats it with a larger buffer.
-	if (w.ctl->flags & BATCH_FLAG_TASK_OVERFLOW)
+	if (s_cnt[2])
 		return;
-	__shared__ uint64_t s_base[2];
-	__shared__ WarpStage<T> s_stage[THREADS / 32];
-	if (threadIdx.x == 0) {
-		uint64_t b = 0;  // start of the previous level's records
-		for (uint32_t e = 0; e + 1 < d; e++)
-			b += w.ctl->lvl_cnt[e];
-		s_base[0] = b;
-		s_base[1] = b + (d ? w.ctl->lvl_cnt[d - 1] : 0u);
-	}
-	__syncthreads();
 	const uint64_t base_prev = s_base[0], base_cur = s_base[1];
 	// after a frontier overflow the counters run past what was stored: never read beyond it
 	const uint64_t end_prev = min(base_cur, w.rec_cap);
@@ -523,7 +533,8 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_bfs_level(TreeDev<T
 	const uint64_t gthreads = (uint64_t) gridDim.x * blockDim.x;
 	const uint64_t gtid = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
 	const uint64_t gwarps = gthreads / 32, gwarp = gtid / 32;
-	level_body<T, LAST>(t, qd, w, d, gwarp, gwarps, base_prev, base_cur, n_prev, s_stage[threadIdx.x >> 5]);
+	level_body<T, LAST>(t, qd, w, d, gwarp, gwarps, base_prev, base_cur, n_prev, s_cnt,
+	                    s_stage[threadIdx.x >> 5]);
 }
 
 // Small batches (a single query, or a few): one CTA takes the tree from the top,
@@ -532,75 +543,194 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_bfs_level(TreeDev<T
 // ctl->cta_levels = the levels done and the host launches the per-level kernels
 // for the rest only.  When it reaches the bottom it also scans the queries'
 // counts into offsets[0..max_q] and total, so no scan pass is needed.
+//
+// The pass works in shared memory: the control block, the boundary paths and
+// seeds (pcap of each of the four lists) and the alive records of every level it
+// takes (rcap) live in the dynamic shared array, so a level waits on its tree
+// loads alone, not on round trips to L2 for its counters, records and
+// reservations.  Where it stops, it writes the records, the control block and the
+// next level's paths and seeds to their global buffers, in the layout the
+// per-level kernels and the emit read.  It stops early when the next level might
+// not fit in rcap.
 constexpr uint32_t CTA_REC_CAP = 256;
 
-template <typename T>
-__global__ void __launch_bounds__(BFS_THREADS) k_bfs_cta(TreeDev<T> t, QDev<T> qd, WorkDev w, uint32_t max_q)
+// Dynamic shared memory of k_bfs_cta: the control block, then the four path and
+// seed lists, then the records.
+__host__ __device__ constexpr size_t cta_smem_bytes(uint32_t pcap, uint32_t rcap)
 {
+	return sizeof(BatchCtl) + (size_t) (4 * pcap + rcap) * sizeof(uint4);
+}
+static_assert(sizeof(BatchCtl) % 16 == 0, "the lists after the control block stay 16-byte aligned");
+
+template <typename T>
+__global__ void __launch_bounds__(BFS_THREADS, 1) k_bfs_cta(TreeDev<T> t, QDev<T> qd, WorkDev wg, uint32_t max_q,
+                                                         uint32_t pcap, uint32_t rcap)
+{
+	extern __shared__ __align__(16) unsigned char s_dyn[];
 	__shared__ WarpStage<T> s_stage[BFS_THREADS / 32];
 	__shared__ uint64_t s_base[2];
 	__shared__ uint64_t s_wsum[BFS_THREADS / 32];
-	__shared__ uint32_t s_go;
+	__shared__ uint32_t s_go, s_cnt[2];
+	BatchCtl *sc = reinterpret_cast<BatchCtl *>(s_dyn);
+	uint4 *sl = reinterpret_cast<uint4 *>(s_dyn + sizeof(BatchCtl));
+	// the shared-memory view of the work buffers (ids of reported boundary nodes,
+	// counts and offsets stay global)
+	WorkDev w = wg;
+	w.ctl = sc;
+	w.path0 = sl;
+	w.path1 = sl + pcap;
+	w.seed0 = sl + 2 * pcap;
+	w.seed1 = sl + 3 * pcap;
+	w.path_cap = pcap;
+	w.rec = sl + 4 * pcap;
+	w.rec_cap = rcap;
+	{
+		const uint32_t *src = reinterpret_cast<const uint32_t *>(wg.ctl);
+		uint32_t *dst = reinterpret_cast<uint32_t *>(sc);
+		for (uint32_t i = threadIdx.x; i < sizeof(BatchCtl) / 4; i += BFS_THREADS)
+			dst[i] = src[i];
+		// the level-0 paths (one per query, from k_unpack_queries)
+		const uint32_t n0 = min(wg.ctl->path_cnt[0], pcap);
+		for (uint32_t i = threadIdx.x; i < n0; i += BFS_THREADS)
+			w.path0[i] = wg.path0[i];
+	}
+	__syncthreads();
 	const uint64_t gwarps = BFS_THREADS / 32, gwarp = threadIdx.x >> 5;
 	uint64_t acc_prev = 0, acc = 0;  // (thread 0) start of the previous level's records, and of this level's
 	uint32_t d = 0;
 	for (; d < t.levels; d++) {
 		if (threadIdx.x == 0) {
-			const uint32_t prev = d ? w.ctl->lvl_cnt[d - 1] : 0u;
+			const uint32_t prev = d ? sc->lvl_cnt[d - 1] : 0u;
+			const uint32_t np = min(sc->path_cnt[d], pcap), ns = min(sc->seed_cnt[d], pcap);
 			if (d) {
 				acc_prev = acc;
 				acc += prev;
 			}
 			s_base[0] = acc_prev;
 			s_base[1] = acc;
-			s_go = !(w.ctl->flags & BATCH_FLAG_TASK_OVERFLOW) && prev <= CTA_REC_CAP;
+			s_cnt[0] = np;
+			s_cnt[1] = ns;
+			// the level appends at most two children per record and one record per seed
+			s_go = !(sc->flags & BATCH_FLAG_TASK_OVERFLOW) && prev <= CTA_REC_CAP &&
+			       acc + 2 * (uint64_t) prev + ns <= rcap;
+			if (s_go)
+				sc->lvl_base[d] = acc;
 		}
 		__syncthreads();
 		if (!s_go)
 			break;
 		const uint64_t base_prev = s_base[0], base_cur = s_base[1];
-		const uint64_t end_prev = min(base_cur, w.rec_cap);
-		const uint64_t n_prev = end_prev > base_prev ? end_prev - base_prev : 0;
+		const uint64_t n_prev = base_cur - base_prev;
 		if (d + 1 == t.levels && t.last_par)
-			level_body<T, true>(t, qd, w, d, gwarp, gwarps, base_prev, base_cur, n_prev, s_stage[gwarp]);
+			level_body<T, true>(t, qd, w, d, gwarp, gwarps, base_prev, base_cur, n_prev, s_cnt, s_stage[gwarp]);
 		else
-			level_body<T, false>(t, qd, w, d, gwarp, gwarps, base_prev, base_cur, n_prev, s_stage[gwarp]);
+			level_body<T, false>(t, qd, w, d, gwarp, gwarps, base_prev, base_cur, n_prev, s_cnt, s_stage[gwarp]);
 		__syncthreads();  // the level's records, paths, seeds and counts are visible to the CTA
 		if (threadIdx.x == 0)
-			w.ctl->cta_levels = d + 1;
+			sc->cta_levels = d + 1;
 	}
-	if (threadIdx.x == 0)
-		s_go = d == t.levels && !(w.ctl->flags & BATCH_FLAG_TASK_OVERFLOW);
-	__syncthreads();
-	if (!s_go)
-		return;
-	// exclusive scan of counts[0..max_q) in chunks of one count per thread
-	const uint32_t nq = w.ctl->nq, lane = lane_id();
-	uint64_t *offsets = const_cast<uint64_t *>(w.offsets);
-	uint64_t carry = 0;
-	for (uint32_t b = 0; b < max_q; b += BFS_THREADS) {
-		const uint32_t q = b + threadIdx.x;
-		const uint64_t c = q < nq ? w.counts[q] : 0;
-		const uint64_t inc = warp_incl_scan(c);
-		if (lane == 31)
-			s_wsum[gwarp] = inc;
-		__syncthreads();
-		if (gwarp == 0) {
-			uint64_t v = lane < BFS_THREADS / 32 ? s_wsum[lane] : 0;
-			v = warp_incl_scan(v);
-			if (lane < BFS_THREADS / 32)
-				s_wsum[lane] = v;
-		}
-		__syncthreads();
-		if (q < max_q)
-			offsets[q] = carry + (gwarp ? s_wsum[gwarp - 1] : 0) + inc - c;
-		carry += s_wsum[BFS_THREADS / 32 - 1];
-		__syncthreads();  // s_wsum is rewritten by the next chunk
-	}
+	// Hand over: the records of the levels taken (acc of them, levels 0..d-1), and,
+	// where the pass stopped above the bottom, the paths and seeds of level d.
 	if (threadIdx.x == 0) {
-		offsets[max_q] = carry;
-		w.ctl->total = carry;
+		const uint64_t n = d ? acc + sc->lvl_cnt[d - 1] : 0;  // acc = start of level d - 1 when the loop ended
+		s_base[0] = n;
+		if (n > wg.rec_cap) {
+			sc->need_tasks = max((unsigned long long) sc->need_tasks, (unsigned long long) n);
+			sc->flags |= BATCH_FLAG_TASK_OVERFLOW;
+		}
+		s_go = d == t.levels && !(sc->flags & BATCH_FLAG_TASK_OVERFLOW);
 	}
+	__syncthreads();
+	{
+		const uint64_t n = s_base[0];
+		if (n <= wg.rec_cap)
+			for (uint64_t i = threadIdx.x; i < n; i += BFS_THREADS)
+				wg.rec[i] = w.rec[i];
+		if (d < t.levels) {
+			const uint32_t np = min(sc->path_cnt[d], pcap), ns = min(sc->seed_cnt[d], pcap);
+			const uint4 *ps = (d & 1) ? w.path1 : w.path0, *ss = (d & 1) ? w.seed1 : w.seed0;
+			uint4 *pd = (d & 1) ? wg.path1 : wg.path0, *sd = (d & 1) ? wg.seed1 : wg.seed0;
+			for (uint32_t i = threadIdx.x; i < np; i += BFS_THREADS)
+				pd[i] = ps[i];
+			for (uint32_t i = threadIdx.x; i < ns; i += BFS_THREADS)
+				sd[i] = ss[i];
+		}
+	}
+	if (s_go) {
+		// exclusive scan of counts[0..max_q) in chunks of one count per thread
+		const uint32_t nq = sc->nq, lane = lane_id();
+		uint64_t *offsets = const_cast<uint64_t *>(w.offsets);
+		uint64_t carry = 0;
+		for (uint32_t b = 0; b < max_q; b += BFS_THREADS) {
+			const uint32_t q = b + threadIdx.x;
+			const uint64_t c = q < nq ? w.counts[q] : 0;
+			const uint64_t inc = warp_incl_scan(c);
+			if (lane == 31)
+				s_wsum[gwarp] = inc;
+			__syncthreads();
+			if (gwarp == 0) {
+				uint64_t v = lane < BFS_THREADS / 32 ? s_wsum[lane] : 0;
+				v = warp_incl_scan(v);
+				if (lane < BFS_THREADS / 32)
+					s_wsum[lane] = v;
+			}
+			__syncthreads();
+			if (q < max_q)
+				offsets[q] = carry + (gwarp ? s_wsum[gwarp - 1] : 0) + inc - c;
+			carry += s_wsum[BFS_THREADS / 32 - 1];
+			__syncthreads();  // s_wsum is rewritten by the next chunk
+		}
+		if (threadIdx.x == 0) {
+			offsets[max_q] = carry;
+			sc->total = carry;
+		}
+	}
+	__syncthreads();
+	// the control block last: every counter the host and the next kernels read
+	{
+		const uint32_t *src = reinterpret_cast<const uint32_t *>(sc);
+		uint32_t *dst = reinterpret_cast<uint32_t *>(wg.ctl);
+		for (uint32_t i = threadIdx.x; i < sizeof(BatchCtl) / 4; i += BFS_THREADS)
+			dst[i] = src[i];
+	}
+}
+
+// Shared memory the one-CTA top pass may take beyond its static arrays on the
+// current device, after allowing it for the kernel there (once per device; done
+// before any launch is captured into a graph).
+template <typename T>
+size_t cta_pass_budget()
+{
+	static std::mutex mu;
+	static size_t budget[64];
+	static bool done[64] = {};
+	const DeviceInfo &di = device_info();
+	std::lock_guard<std::mutex> lk(mu);
+	if (!done[di.device]) {
+		cudaFuncAttributes a{};
+		PST_CUDA(cudaFuncGetAttributes(&a, k_bfs_cta<T>));
+		const size_t b = di.smem_optin > a.sharedSizeBytes + 1024 ? di.smem_optin - a.sharedSizeBytes - 1024 : 0;
+		PST_CUDA(cudaFuncSetAttribute(k_bfs_cta<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) b));
+		budget[di.device] = b;
+		done[di.device] = true;
+	}
+	return budget[di.device];
+}
+
+// Launches the one-CTA top pass with its shared-memory lists: pcap entries for each
+// path and seed list (at least two per query of the batch) and as many records as
+// the rest of the CTA's shared memory holds.
+template <typename T>
+void launch_cta_pass(const TreeDev<T> &tv, const QDev<T> &qd, const WorkDev &w, uint32_t max_q, uint32_t pcap,
+                     cudaStream_t s)
+{
+	const size_t budget = cta_pass_budget<T>();
+	const size_t fixed = cta_smem_bytes(pcap, 0);
+	// room for at least one level's records beyond the lists
+	if (budget < fixed + (size_t) (2 * CTA_REC_CAP + pcap) * sizeof(uint4))
+		fail(PST_ERR_INTERNAL, "shared memory too small for the top pass of " + std::to_string(max_q) + " queries");
+	const uint32_t rcap = (uint32_t) ((budget - fixed) / sizeof(uint4));
+	k_bfs_cta<T><<<1, BFS_THREADS, cta_smem_bytes(pcap, rcap), s>>>(tv, qd, w, max_q, pcap, rcap);
 }
 
 template <typename T>
@@ -964,9 +1094,9 @@ void Batch::init(TreeStorage *t, const pst_batch_opts &o)
 	int occ = 0;
 	const void *kfn = nullptr;
 	switch (t->dtype) {
-	case PST_F32: kfn = bfs_kernel_ptr<float>(threads); break;
-	case PST_F64: kfn = bfs_kernel_ptr<double>(threads); break;
-	case PST_I32: kfn = bfs_kernel_ptr<int32_t>(threads); break;
+	case PST_F32: kfn = bfs_kernel_ptr<float>(threads); cta_pass_budget<float>(); break;
+	case PST_F64: kfn = bfs_kernel_ptr<double>(threads); cta_pass_budget<double>(); break;
+	case PST_I32: kfn = bfs_kernel_ptr<int32_t>(threads); cta_pass_budget<int32_t>(); break;
 	}
 	PST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kfn, threads, 0));
 	blocks_per_sm = o.blocks_per_sm ? std::min<uint32_t>(o.blocks_per_sm, (uint32_t) std::max(occ, 1))
@@ -1056,7 +1186,7 @@ void Batch::enqueue_count_top(cudaStream_t s)
 	k_check_kinds<<<1, qt, 0, s>>>(q_raw, ctl);
 	k_unpack_queries<T><<<1, qt, 0, s>>>(q_raw, ctl, kind, static_cast<T *>(min1), static_cast<T *>(max1),
 	                                     static_cast<T *>(min2), path0);
-	k_bfs_cta<T><<<1, BFS_THREADS, 0, s>>>(tv, qd, w, max_q);
+	launch_cta_pass<T>(tv, qd, w, max_q, 2 * std::min(top_q, max_q), s);
 	PST_CUDA(cudaGetLastError());
 }
 
@@ -1294,7 +1424,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 
 // Sub-buffers of the scratch array, 256-byte aligned, in bytes.
 constexpr size_t NA_CTL = 0;
-constexpr size_t NA_QRAW = 512;
+constexpr size_t NA_QRAW = 1024;
 constexpr size_t NA_KIND = NA_QRAW + 256;
 constexpr size_t NA_MIN1 = NA_KIND + 256;
 constexpr size_t NA_MAX1 = NA_MIN1 + 256;
@@ -1427,7 +1557,7 @@ uint64_t noalloc_run(TreeStorage &t, const pst_query &q, pst_ret ret, void *out,
 	k_check_kinds<<<1, 32, 0, s>>>(qraw, ctl);
 	k_unpack_queries<T><<<1, 32, 0, s>>>(qraw, ctl, kind, min1, max1, min2, path0);
 	// the one-CTA top pass, then the per-level kernels for whatever it left
-	k_bfs_cta<T><<<1, BFS_THREADS, 0, s>>>(tv, qd, w, 1u);
+	launch_cta_pass<T>(tv, qd, w, 1u, 2u, s);
 	PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
 	PST_CUDA(cudaStreamSynchronize(s));
 	if (!(h.flags & (BATCH_FLAG_BAD_QUERY | BATCH_FLAG_INTERNAL | BATCH_FLAG_TASK_OVERFLOW)) &&

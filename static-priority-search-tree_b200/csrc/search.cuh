@@ -31,6 +31,10 @@ struct BatchCtl {
 	uint32_t cta_levels;    // levels already done by the one-CTA top pass (small batches)
 	uint64_t need_tasks;
 	uint64_t total;
+	// start of each level region (the sum of the counts before it), written by the
+	// kernel that fills the region, so the next kernel reads its bounds in one load
+	// each instead of summing every count before them
+	uint64_t lvl_base[40];
 };
 
 struct Batch {
