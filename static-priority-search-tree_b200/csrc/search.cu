@@ -48,6 +48,15 @@ struct QDev {
 	const T *min2;
 };
 
+// The same arrays, written once per pass from the caller's pst_query records.
+template <typename T>
+struct QOut {
+	uint32_t *kind;
+	T *min1;
+	T *max1;
+	T *min2;
+};
+
 // Alive records cover a "block" of 64 consecutive slots of one level (two
 // 128-byte rows of a 4-byte field): (block base position, query, mask of reported
 // slots, low and high word).  Block bases are multiples of 64.
@@ -537,6 +546,51 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_bfs_level(TreeDev<T
 	                    s_stage[threadIdx.x >> 5]);
 }
 
+// Query i of the batch: its kind and bounds into the engine's per-query arrays, and
+// its level-0 boundary path task (returned); a kind out of range raises
+// BATCH_FLAG_BAD_QUERY in *flags (the pass still runs, and the host reports it).
+template <typename T>
+__device__ __forceinline__ uint4 unpack_query(const pst_query *__restrict__ raw, uint32_t i, const QOut<T> &qo,
+                                              uint32_t *flags)
+{
+	const pst_query q = raw[i];
+	T a, b, c;
+	if constexpr (sizeof(T) == 8) {
+		a = q.min1.f64; b = q.max1.f64; c = q.min2.f64;
+	} else if constexpr (std::is_same<T, float>::value) {
+		a = q.min1.f32; b = q.max1.f32; c = q.min2.f32;
+	} else {
+		a = q.min1.i32; b = q.max1.i32; c = q.min2.i32;
+	}
+	const int32_t k = q.kind;
+	if (k < PST_Q_THREE || k > PST_Q_RIGHT)
+		atomicOr(flags, BATCH_FLAG_BAD_QUERY);
+	qo.kind[i] = (uint32_t) k;
+	qo.min1[i] = a;
+	qo.max1[i] = b;
+	qo.min2[i] = c;
+	const uint32_t mode = k == PST_Q_THREE ? MODE_THREE : k == PST_Q_LEFT ? MODE_LEFT : MODE_RIGHT;
+	return make_uint4(1u, i, mode, 0u);
+}
+
+// Start of a full pass (after the control block's upload): the batch's queries
+// unpacked and checked, their level-0 paths, and the per-query counts and output
+// cursors zeroed (all max_q of them: the scan reads every count).
+template <typename T>
+__global__ void k_prepare_queries(const pst_query *raw, BatchCtl *ctl, QOut<T> qo, uint4 *path0, uint64_t *counts,
+                                  uint64_t *cursor, uint32_t max_q)
+{
+	const uint32_t nq = ctl->nq;
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < max_q; i += gridDim.x * blockDim.x) {
+		if (i < nq)
+			path0[i] = unpack_query<T>(raw, i, qo, &ctl->flags);
+		counts[i] = 0;
+		cursor[i] = 0;
+	}
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+		ctl->path_cnt[0] = nq;
+}
+
 // Small batches (a single query, or a few): one CTA takes the tree from the top,
 // level by level with a CTA barrier in place of a kernel boundary, while the
 // records to expand stay few enough for it (at most CTA_REC_CAP); it leaves
@@ -564,7 +618,8 @@ static_assert(sizeof(BatchCtl) % 16 == 0, "the lists after the control block sta
 
 template <typename T>
 __global__ void __launch_bounds__(BFS_THREADS, 1) k_bfs_cta(TreeDev<T> t, QDev<T> qd, WorkDev wg, uint32_t max_q,
-                                                         uint32_t pcap, uint32_t rcap)
+                                                            uint32_t pcap, uint32_t rcap, const pst_query *raw,
+                                                            QOut<T> qo)
 {
 	extern __shared__ __align__(16) unsigned char s_dyn[];
 	__shared__ WarpStage<T> s_stage[BFS_THREADS / 32];
@@ -589,10 +644,21 @@ __global__ void __launch_bounds__(BFS_THREADS, 1) k_bfs_cta(TreeDev<T> t, QDev<T
 		uint32_t *dst = reinterpret_cast<uint32_t *>(sc);
 		for (uint32_t i = threadIdx.x; i < sizeof(BatchCtl) / 4; i += BFS_THREADS)
 			dst[i] = src[i];
-		// the level-0 paths (one per query, from k_unpack_queries)
-		const uint32_t n0 = min(wg.ctl->path_cnt[0], pcap);
-		for (uint32_t i = threadIdx.x; i < n0; i += BFS_THREADS)
-			w.path0[i] = wg.path0[i];
+	}
+	__syncthreads();
+	{
+		// the start of the pass (k_prepare_queries of a full pass): the queries
+		// unpacked and checked, their level-0 paths (at most pcap / 2 queries: the
+		// host runs this pass for small batches only), the counts and cursors zeroed
+		const uint32_t nq = min(sc->nq, pcap);
+		for (uint32_t i = threadIdx.x; i < max_q; i += BFS_THREADS) {
+			if (i < nq)
+				w.path0[i] = unpack_query<T>(raw, i, qo, &sc->flags);
+			wg.counts[i] = 0;
+			wg.cursor[i] = 0;
+		}
+		if (threadIdx.x == 0)
+			sc->path_cnt[0] = nq;
 	}
 	__syncthreads();
 	const uint64_t gwarps = BFS_THREADS / 32, gwarp = threadIdx.x >> 5;
@@ -632,8 +698,15 @@ __global__ void __launch_bounds__(BFS_THREADS, 1) k_bfs_cta(TreeDev<T> t, QDev<T
 	// Hand over: the records of the levels taken (acc of them, levels 0..d-1), and,
 	// where the pass stopped above the bottom, the paths and seeds of level d.
 	if (threadIdx.x == 0) {
-		const uint64_t n = d ? acc + sc->lvl_cnt[d - 1] : 0;  // acc = start of level d - 1 when the loop ended
-		s_base[0] = n;
+		// records written: at the bottom, acc is the start of the last level's region
+		// and that level's count follows it; where the pass stopped at level d, the
+		// top of the loop had already advanced acc past level d - 1, so acc is the
+		// number written (at most rcap in both cases: each level's bound was checked
+		// before it ran)
+		const uint64_t n = d == t.levels && d ? acc + sc->lvl_cnt[d - 1] : acc;
+		// (a refused reservation, which the bound rules out, would have raised the
+		// overflow flag and left the counts past what was stored: never copy beyond)
+		s_base[0] = min(n, (uint64_t) rcap);
 		if (n > wg.rec_cap) {
 			sc->need_tasks = max((unsigned long long) sc->need_tasks, (unsigned long long) n);
 			sc->flags |= BATCH_FLAG_TASK_OVERFLOW;
@@ -722,7 +795,7 @@ size_t cta_pass_budget()
 // the rest of the CTA's shared memory holds.
 template <typename T>
 void launch_cta_pass(const TreeDev<T> &tv, const QDev<T> &qd, const WorkDev &w, uint32_t max_q, uint32_t pcap,
-                     cudaStream_t s)
+                     const pst_query *raw, const QOut<T> &qo, cudaStream_t s)
 {
 	const size_t budget = cta_pass_budget<T>();
 	const size_t fixed = cta_smem_bytes(pcap, 0);
@@ -730,44 +803,7 @@ void launch_cta_pass(const TreeDev<T> &tv, const QDev<T> &qd, const WorkDev &w, 
 	if (budget < fixed + (size_t) (2 * CTA_REC_CAP + pcap) * sizeof(uint4))
 		fail(PST_ERR_INTERNAL, "shared memory too small for the top pass of " + std::to_string(max_q) + " queries");
 	const uint32_t rcap = (uint32_t) ((budget - fixed) / sizeof(uint4));
-	k_bfs_cta<T><<<1, BFS_THREADS, cta_smem_bytes(pcap, rcap), s>>>(tv, qd, w, max_q, pcap, rcap);
-}
-
-template <typename T>
-__global__ void k_unpack_queries(const pst_query *raw, BatchCtl *ctl, uint32_t *kind, T *min1, T *max1, T *min2,
-                                 uint4 *path0)
-{
-	const uint32_t nq = ctl->nq;
-	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
-		const pst_query q = raw[i];
-		T a, b, c;
-		if constexpr (sizeof(T) == 8) {
-			a = q.min1.f64; b = q.max1.f64; c = q.min2.f64;
-		} else if constexpr (std::is_same<T, float>::value) {
-			a = q.min1.f32; b = q.max1.f32; c = q.min2.f32;
-		} else {
-			a = q.min1.i32; b = q.max1.i32; c = q.min2.i32;
-		}
-		const uint32_t k = (uint32_t) q.kind;
-		kind[i] = k;
-		min1[i] = a;
-		max1[i] = b;
-		min2[i] = c;
-		const uint32_t mode = k == PST_Q_THREE ? MODE_THREE : k == PST_Q_LEFT ? MODE_LEFT : MODE_RIGHT;
-		path0[i] = make_uint4(1u, i, mode, 0u);
-	}
-	if (blockIdx.x == 0 && threadIdx.x == 0)
-		ctl->path_cnt[0] = nq;
-}
-
-__global__ void k_check_kinds(const pst_query *raw, BatchCtl *ctl)
-{
-	const uint32_t nq = ctl->nq;
-	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
-		const int32_t k = raw[i].kind;
-		if (k < PST_Q_THREE || k > PST_Q_RIGHT)
-			atomicOr(&ctl->flags, BATCH_FLAG_BAD_QUERY);
-	}
+	k_bfs_cta<T><<<1, BFS_THREADS, cta_smem_bytes(pcap, rcap), s>>>(tv, qd, w, max_q, pcap, rcap, raw, qo);
 }
 
 // Output slot of this lane's record inside its query's result: one atomic per run
@@ -892,6 +928,8 @@ __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mi
 template <typename T, bool HAS_ID, bool POINTS, int THREADS, int U>
 __global__ void __launch_bounds__(THREADS) k_emit(TreeDev<T> t, WorkDev w, void *out, uint64_t capacity)
 {
+	// a programmatic dependent of the scan (a no-op after any other predecessor)
+	asm volatile("griddepcontrol.wait;" ::: "memory");
 	__shared__ uint64_t s_total;
 	__shared__ EmitStage s_stage[THREADS / 32];
 	if (threadIdx.x == 0) {
@@ -941,6 +979,75 @@ __global__ void __launch_bounds__(THREADS) k_emit(TreeDev<T> t, WorkDev w, void 
 	}
 }
 
+// Result offsets of a batch in one launch: offsets[q] = the counts of the queries
+// before q, offsets[max_q] = ctl->total = all of them.  One CTA walks the counts a
+// tile at a time (batches of up to OFFSETS_ONE_CTA queries; larger ones take the
+// three-kernel scan).  Launched as a programmatic dependent of the last level.
+constexpr uint32_t OFFSETS_ONE_CTA = 4 * SCAN_TILE;
+
+__global__ void __launch_bounds__(SCAN_THREADS) k_offsets(const uint64_t *counts, uint64_t *offsets, uint32_t n,
+                                                          BatchCtl *ctl)
+{
+	asm volatile("griddepcontrol.wait;" ::: "memory");
+	__shared__ uint64_t ws[33];
+	uint64_t carry = 0;
+	for (uint32_t c0 = 0; c0 < n; c0 += SCAN_TILE) {
+		const uint32_t base = c0 + threadIdx.x * SCAN_ITEMS;
+		uint64_t v[SCAN_ITEMS];
+		uint64_t sum = 0;
+#pragma unroll
+		for (int i = 0; i < SCAN_ITEMS; i++) {
+			v[i] = base + i < n ? counts[base + i] : 0;
+			sum += v[i];
+		}
+		uint64_t tot;
+		uint64_t ex = block_excl_scan(sum, &tot, ws) + carry;
+#pragma unroll
+		for (int i = 0; i < SCAN_ITEMS; i++) {
+			if (base + i < n)
+				offsets[base + i] = ex;
+			ex += v[i];
+		}
+		carry += tot;
+	}
+	if (threadIdx.x == 0) {
+		offsets[n] = carry;
+		ctl->total = carry;
+	}
+}
+
+// Launch configuration of a programmatic dependent of the kernel before it on `s`:
+// its CTAs may be scheduled while that kernel drains, and wait (griddepcontrol.wait)
+// until it has completed and its writes are visible.
+struct DependentLaunch {
+	cudaLaunchConfig_t cfg{};
+	cudaLaunchAttribute attr[1];
+	DependentLaunch(unsigned grid, unsigned threads, cudaStream_t s)
+	{
+		cfg.gridDim = dim3(grid);
+		cfg.blockDim = dim3(threads);
+		cfg.dynamicSmemBytes = 0;
+		cfg.stream = s;
+		attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+		attr[0].val.programmaticStreamSerializationAllowed = 1;
+		cfg.attrs = attr;
+		cfg.numAttrs = 1;
+	}
+};
+
+// The batch's result offsets and total (exclusive scan of its counts).
+inline void scan_offsets(uint64_t *counts, uint64_t *offsets, uint32_t max_q, uint64_t *scan_tmp, BatchCtl *ctl,
+                         cudaStream_t s)
+{
+	if (max_q <= OFFSETS_ONE_CTA) {
+		DependentLaunch l(1, SCAN_THREADS, s);
+		PST_CUDA(cudaLaunchKernelEx(&l.cfg, k_offsets, (const uint64_t *) counts, offsets, max_q, ctl));
+		return;
+	}
+	exclusive_scan<uint64_t>(counts, offsets, max_q, scan_tmp, &ctl->total, s);
+	PST_CUDA(cudaMemcpyAsync(offsets + max_q, &ctl->total, 8, cudaMemcpyDeviceToDevice, s));
+}
+
 // Grid of k_emit: as many CTAs as fit on the device at once (its own occupancy,
 // which can differ from the level kernel's), so the grid-stride loop has no tail wave.
 template <typename T, bool HAS_ID, bool POINTS, int THREADS, int U>
@@ -962,18 +1069,10 @@ template <typename T>
 void launch_level(const TreeDev<T> &tv, const QDev<T> &qd, const WorkDev &w, uint32_t d, unsigned grid,
                   unsigned threads, cudaStream_t s)
 {
-	// programmatic dependent launch: the level's CTAs start as the previous kernel
+	// a programmatic dependent launch: the level's CTAs start as the previous kernel
 	// drains (the kernel waits for it before reading anything)
-	cudaLaunchConfig_t cfg{};
-	cfg.gridDim = dim3(grid);
-	cfg.blockDim = dim3(threads);
-	cfg.dynamicSmemBytes = 0;
-	cfg.stream = s;
-	cudaLaunchAttribute attr[1];
-	attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-	attr[0].val.programmaticStreamSerializationAllowed = 1;
-	cfg.attrs = attr;
-	cfg.numAttrs = 1;
+	DependentLaunch l(grid, threads, s);
+	cudaLaunchConfig_t &cfg = l.cfg;
 	const bool last = d + 1 == tv.levels && tv.last_par;
 	switch (threads) {
 	case 128:
@@ -1004,8 +1103,8 @@ const void *bfs_kernel_ptr(unsigned threads)
 template <typename T, bool HAS_ID, bool POINTS, int THREADS, int U>
 void launch_emit_tu(const TreeDev<T> &tv, const WorkDev &w, void *out, uint64_t capacity, cudaStream_t s)
 {
-	k_emit<T, HAS_ID, POINTS, THREADS, U><<<emit_grid<T, HAS_ID, POINTS, THREADS, U>(), THREADS, 0, s>>>(tv, w, out,
-	                                                                                                   capacity);
+	DependentLaunch l(emit_grid<T, HAS_ID, POINTS, THREADS, U>(), THREADS, s);
+	PST_CUDA(cudaLaunchKernelEx(&l.cfg, k_emit<T, HAS_ID, POINTS, THREADS, U>, tv, w, out, capacity));
 }
 
 template <typename T, bool HAS_ID, bool POINTS, int THREADS>
@@ -1159,16 +1258,12 @@ void Batch::enqueue_count(cudaStream_t s)
 	QDev<T> qd{kind, static_cast<const T *>(min1), static_cast<const T *>(max1), static_cast<const T *>(min2)};
 	PST_WORKDEV;
 	PST_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
-	PST_CUDA(cudaMemsetAsync(counts, 0, (size_t) max_q * 8, s));
-	PST_CUDA(cudaMemsetAsync(cursor, 0, (size_t) max_q * 8, s));
 	const unsigned ug = (unsigned) std::min<uint64_t>((max_q + 255) / 256, (uint64_t) device_info().sms * 4);
-	k_check_kinds<<<ug, 256, 0, s>>>(q_raw, ctl);
-	k_unpack_queries<T><<<ug, 256, 0, s>>>(q_raw, ctl, kind, static_cast<T *>(min1), static_cast<T *>(max1),
-	                                       static_cast<T *>(min2), path0);
+	const QOut<T> qo{kind, static_cast<T *>(min1), static_cast<T *>(max1), static_cast<T *>(min2)};
+	k_prepare_queries<T><<<ug, 256, 0, s>>>(q_raw, ctl, qo, path0, counts, cursor, max_q);
 	for (uint32_t d = 0; d < tv.levels; d++)
 		launch_level<T>(tv, qd, w, d, grid, threads, s);
-	exclusive_scan<uint64_t>(counts, offsets, max_q, scan_tmp, &ctl->total, s);
-	PST_CUDA(cudaMemcpyAsync(offsets + max_q, &ctl->total, 8, cudaMemcpyDeviceToDevice, s));
+	scan_offsets(counts, offsets, max_q, scan_tmp, ctl, s);
 	PST_CUDA(cudaGetLastError());
 }
 
@@ -1178,15 +1273,10 @@ void Batch::enqueue_count_top(cudaStream_t s)
 	TreeDev<T> tv = tree->view<T>();
 	QDev<T> qd{kind, static_cast<const T *>(min1), static_cast<const T *>(max1), static_cast<const T *>(min2)};
 	PST_WORKDEV;
-	// one CTA over the batch's queries (the loops are grid-strided)
-	const unsigned qt = SMALL_BATCH_Q;
+	// the control block, then one kernel: the queries unpacked and the whole top pass
 	PST_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
-	PST_CUDA(cudaMemsetAsync(counts, 0, (size_t) max_q * 8, s));
-	PST_CUDA(cudaMemsetAsync(cursor, 0, (size_t) max_q * 8, s));
-	k_check_kinds<<<1, qt, 0, s>>>(q_raw, ctl);
-	k_unpack_queries<T><<<1, qt, 0, s>>>(q_raw, ctl, kind, static_cast<T *>(min1), static_cast<T *>(max1),
-	                                     static_cast<T *>(min2), path0);
-	launch_cta_pass<T>(tv, qd, w, max_q, 2 * std::min(top_q, max_q), s);
+	const QOut<T> qo{kind, static_cast<T *>(min1), static_cast<T *>(max1), static_cast<T *>(min2)};
+	launch_cta_pass<T>(tv, qd, w, max_q, 2 * std::min(top_q, max_q), q_raw, qo, s);
 	PST_CUDA(cudaGetLastError());
 }
 
@@ -1198,8 +1288,7 @@ void Batch::enqueue_count_rest(uint32_t from, cudaStream_t s)
 	PST_WORKDEV;
 	for (uint32_t d = from; d < tv.levels; d++)
 		launch_level<T>(tv, qd, w, d, grid, threads, s);
-	exclusive_scan<uint64_t>(counts, offsets, max_q, scan_tmp, &ctl->total, s);
-	PST_CUDA(cudaMemcpyAsync(offsets + max_q, &ctl->total, 8, cudaMemcpyDeviceToDevice, s));
+	scan_offsets(counts, offsets, max_q, scan_tmp, ctl, s);
 	PST_CUDA(cudaGetLastError());
 }
 
@@ -1539,14 +1628,12 @@ uint64_t noalloc_run(TreeStorage &t, const pst_query &q, pst_ret ret, void *out,
 	uint64_t *scan = reinterpret_cast<uint64_t *>(base + NA_SCAN);
 	uint4 *rec = reinterpret_cast<uint4 *>(base + NA_RECS);
 
-	// The array keeps the previous call's contents: reset everything that must
-	// start at zero (control block with nq = 1, count, output cursor).
+	// The array keeps the previous call's contents: the control block starts over
+	// (with nq = 1) here, and the top pass zeroes the query's count and output cursor.
 	BatchCtl h{};
 	h.nq = 1;
 	PST_CUDA(cudaMemcpyAsync(ctl, &h, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
 	PST_CUDA(cudaMemcpyAsync(qraw, &q, sizeof(pst_query), cudaMemcpyHostToDevice, s));
-	PST_CUDA(cudaMemsetAsync(counts, 0, 8, s));
-	PST_CUDA(cudaMemsetAsync(cursor, 0, 8, s));
 
 	int occ = 0;
 	PST_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, bfs_kernel_ptr<T>(BFS_THREADS), BFS_THREADS, 0));
@@ -1554,17 +1641,16 @@ uint64_t noalloc_run(TreeStorage &t, const pst_query &q, pst_ret ret, void *out,
 	TreeDev<T> tv = t.view<T>();
 	QDev<T> qd{kind, min1, max1, min2};
 	WorkDev w{rec, NA_REC_CAP, path0, path1, seed0, seed1, 2u, ro, NA_RO_CAP, counts, cursor, offsets, ctl};
-	k_check_kinds<<<1, 32, 0, s>>>(qraw, ctl);
-	k_unpack_queries<T><<<1, 32, 0, s>>>(qraw, ctl, kind, min1, max1, min2, path0);
-	// the one-CTA top pass, then the per-level kernels for whatever it left
-	launch_cta_pass<T>(tv, qd, w, 1u, 2u, s);
+	// the one-CTA top pass (which unpacks the query and zeroes its count and output
+	// cursor), then the per-level kernels for whatever it left
+	launch_cta_pass<T>(tv, qd, w, 1u, 2u, qraw, QOut<T>{kind, min1, max1, min2}, s);
 	PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
 	PST_CUDA(cudaStreamSynchronize(s));
 	if (!(h.flags & (BATCH_FLAG_BAD_QUERY | BATCH_FLAG_INTERNAL | BATCH_FLAG_TASK_OVERFLOW)) &&
 	    h.cta_levels < tv.levels) {
 		for (uint32_t d = h.cta_levels; d < tv.levels; d++)
 			launch_level<T>(tv, qd, w, d, grid, BFS_THREADS, s);
-		exclusive_scan<uint64_t>(counts, offsets, 1, scan, &ctl->total, s);
+		scan_offsets(counts, offsets, 1, scan, ctl, s);
 		PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
 		PST_CUDA(cudaStreamSynchronize(s));
 	}
