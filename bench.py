@@ -1156,7 +1156,9 @@ def main():
             line["ips"] = ips_rows
         if iso_res is not None:
             line["isosurface"] = iso_res
-        line["gpu_launches"] = (levels_main + 6) * args.steps  # unpack+check + levels + 3 scan + emit per step
+        # per step: query preparation, one kernel per level, offsets, emit (a batch of
+        # 4096 queries takes the one-launch offsets scan)
+        line["gpu_launches"] = (levels_main + 3) * args.steps
         print(json.dumps(line))
     if eng is not None:
         eng.close()
