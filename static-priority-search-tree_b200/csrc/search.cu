@@ -573,7 +573,19 @@ __device__ __forceinline__ uint4 unpack_query(const pst_query *__restrict__ raw,
 	return make_uint4(1u, i, mode, 0u);
 }
 
-// Start of a full pass (after the control block's upload): the batch's queries
+// The pass's control block from the engine's pinned host copy, read through its
+// mapped device address: a kernel, because inside the captured pass a
+// host-to-device copy node ahead of the first kernel left the device idle for
+// ≈ 25 µs per pass.
+__global__ void k_load_ctl(const BatchCtl *src, BatchCtl *dst)
+{
+	const uint32_t *s = reinterpret_cast<const uint32_t *>(src);
+	uint32_t *d = reinterpret_cast<uint32_t *>(dst);
+	for (uint32_t i = threadIdx.x; i < sizeof(BatchCtl) / 4; i += blockDim.x)
+		d[i] = s[i];
+}
+
+// Start of a full pass (after the control block's load): the batch's queries
 // unpacked and checked, their level-0 paths, and the per-query counts and output
 // cursors zeroed (all max_q of them: the scan reads every count).
 template <typename T>
@@ -619,7 +631,7 @@ static_assert(sizeof(BatchCtl) % 16 == 0, "the lists after the control block sta
 template <typename T>
 __global__ void __launch_bounds__(BFS_THREADS, 1) k_bfs_cta(TreeDev<T> t, QDev<T> qd, WorkDev wg, uint32_t max_q,
                                                             uint32_t pcap, uint32_t rcap, const pst_query *raw,
-                                                            QOut<T> qo)
+                                                            QOut<T> qo, const BatchCtl *ctl_src)
 {
 	extern __shared__ __align__(16) unsigned char s_dyn[];
 	__shared__ WarpStage<T> s_stage[BFS_THREADS / 32];
@@ -640,7 +652,9 @@ __global__ void __launch_bounds__(BFS_THREADS, 1) k_bfs_cta(TreeDev<T> t, QDev<T
 	w.rec = sl + 4 * pcap;
 	w.rec_cap = rcap;
 	{
-		const uint32_t *src = reinterpret_cast<const uint32_t *>(wg.ctl);
+		// the pass's starting control block: the engine's pinned host copy (or the
+		// no-alloc search's device copy), wg.ctl receives the final one
+		const uint32_t *src = reinterpret_cast<const uint32_t *>(ctl_src);
 		uint32_t *dst = reinterpret_cast<uint32_t *>(sc);
 		for (uint32_t i = threadIdx.x; i < sizeof(BatchCtl) / 4; i += BFS_THREADS)
 			dst[i] = src[i];
@@ -795,7 +809,7 @@ size_t cta_pass_budget()
 // the rest of the CTA's shared memory holds.
 template <typename T>
 void launch_cta_pass(const TreeDev<T> &tv, const QDev<T> &qd, const WorkDev &w, uint32_t max_q, uint32_t pcap,
-                     const pst_query *raw, const QOut<T> &qo, cudaStream_t s)
+                     const pst_query *raw, const QOut<T> &qo, const BatchCtl *ctl_src, cudaStream_t s)
 {
 	const size_t budget = cta_pass_budget<T>();
 	const size_t fixed = cta_smem_bytes(pcap, 0);
@@ -803,7 +817,8 @@ void launch_cta_pass(const TreeDev<T> &tv, const QDev<T> &qd, const WorkDev &w, 
 	if (budget < fixed + (size_t) (2 * CTA_REC_CAP + pcap) * sizeof(uint4))
 		fail(PST_ERR_INTERNAL, "shared memory too small for the top pass of " + std::to_string(max_q) + " queries");
 	const uint32_t rcap = (uint32_t) ((budget - fixed) / sizeof(uint4));
-	k_bfs_cta<T><<<1, BFS_THREADS, cta_smem_bytes(pcap, rcap), s>>>(tv, qd, w, max_q, pcap, rcap, raw, qo);
+	k_bfs_cta<T><<<1, BFS_THREADS, cta_smem_bytes(pcap, rcap), s>>>(tv, qd, w, max_q, pcap, rcap, raw, qo,
+	                                                                  ctl_src);
 }
 
 // Output slot of this lane's record inside its query's result: one atomic per run
@@ -1162,6 +1177,7 @@ void Batch::release()
 		cudaFreeHost(q_stage);
 	q_raw = nullptr;
 	ctl_host = nullptr;
+	ctl_host_d = nullptr;
 	q_stage = nullptr;
 	rec = nullptr;
 }
@@ -1222,6 +1238,7 @@ void Batch::init(TreeStorage *t, const pst_batch_opts &o)
 	PST_CUDA(cudaMallocHost((void **) &ctl_host, sizeof(BatchCtl)));
 	PST_CUDA(cudaMallocHost((void **) &q_stage, (size_t) max_q * sizeof(pst_query)));
 	memset(ctl_host, 0, sizeof(BatchCtl));
+	PST_CUDA(cudaHostGetDevicePointer((void **) &ctl_host_d, ctl_host, 0));
 	const uint64_t want = o.task_capacity ? o.task_capacity : std::max<uint64_t>(1ull << 16, (uint64_t) max_q * 64);
 	grow_tasks(want, 0);
 	PST_CUDA(cudaStreamSynchronize(0));
@@ -1257,7 +1274,7 @@ void Batch::enqueue_count(cudaStream_t s)
 	TreeDev<T> tv = tree->view<T>();
 	QDev<T> qd{kind, static_cast<const T *>(min1), static_cast<const T *>(max1), static_cast<const T *>(min2)};
 	PST_WORKDEV;
-	PST_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
+	k_load_ctl<<<1, 256, 0, s>>>(ctl_host_d, ctl);
 	const unsigned ug = (unsigned) std::min<uint64_t>((max_q + 255) / 256, (uint64_t) device_info().sms * 4);
 	const QOut<T> qo{kind, static_cast<T *>(min1), static_cast<T *>(max1), static_cast<T *>(min2)};
 	k_prepare_queries<T><<<ug, 256, 0, s>>>(q_raw, ctl, qo, path0, counts, cursor, max_q);
@@ -1273,10 +1290,10 @@ void Batch::enqueue_count_top(cudaStream_t s)
 	TreeDev<T> tv = tree->view<T>();
 	QDev<T> qd{kind, static_cast<const T *>(min1), static_cast<const T *>(max1), static_cast<const T *>(min2)};
 	PST_WORKDEV;
-	// the control block, then one kernel: the queries unpacked and the whole top pass
-	PST_CUDA(cudaMemcpyAsync(ctl, ctl_host, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
+	// one kernel: the control block read from its pinned host copy, the queries
+	// unpacked and the whole top pass
 	const QOut<T> qo{kind, static_cast<T *>(min1), static_cast<T *>(max1), static_cast<T *>(min2)};
-	launch_cta_pass<T>(tv, qd, w, max_q, 2 * std::min(top_q, max_q), q_raw, qo, s);
+	launch_cta_pass<T>(tv, qd, w, max_q, 2 * std::min(top_q, max_q), q_raw, qo, ctl_host_d, s);
 	PST_CUDA(cudaGetLastError());
 }
 
@@ -1643,7 +1660,7 @@ uint64_t noalloc_run(TreeStorage &t, const pst_query &q, pst_ret ret, void *out,
 	WorkDev w{rec, NA_REC_CAP, path0, path1, seed0, seed1, 2u, ro, NA_RO_CAP, counts, cursor, offsets, ctl};
 	// the one-CTA top pass (which unpacks the query and zeroes its count and output
 	// cursor), then the per-level kernels for whatever it left
-	launch_cta_pass<T>(tv, qd, w, 1u, 2u, qraw, QOut<T>{kind, min1, max1, min2}, s);
+	launch_cta_pass<T>(tv, qd, w, 1u, 2u, qraw, QOut<T>{kind, min1, max1, min2}, ctl, s);
 	PST_CUDA(cudaMemcpyAsync(&h, ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
 	PST_CUDA(cudaStreamSynchronize(s));
 	if (!(h.flags & (BATCH_FLAG_BAD_QUERY | BATCH_FLAG_INTERNAL | BATCH_FLAG_TASK_OVERFLOW)) &&

@@ -62,6 +62,7 @@ struct Batch {
 	uint64_t *counts = nullptr, *cursor = nullptr, *offsets = nullptr, *scan_tmp = nullptr;
 	BatchCtl *ctl = nullptr;
 	BatchCtl *ctl_host = nullptr;  // pinned, zeroed except nq
+	const BatchCtl *ctl_host_d = nullptr;  // its device address (mapped pinned memory)
 	BatchCtl last{};
 	// captured passes, each for the stream it was captured for: the whole count pass,
 	// and the top pass of small batches
