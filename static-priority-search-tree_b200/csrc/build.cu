@@ -26,6 +26,8 @@
 //   3. once every node of a level holds at most ST_CAP points, one CTA per node
 //      builds the whole remaining subtree in shared memory.
 #include <algorithm>
+#include <limits>
+#include <type_traits>
 #include <vector>
 
 #include "scan_sort.cuh"
@@ -1115,9 +1117,19 @@ void attach_tree_memory(TreeStorage &t, void *mem)
 	t.occ = reinterpret_cast<uint32_t *>(b + L.off_occ);
 }
 
+// The separately allocated search indexes of finish_tree_aux.
+static uint64_t aux_bytes(pst_dtype dt, uint64_t n)
+{
+	const uint32_t D = tree_levels(n);
+	if (D < 8)
+		return 0;
+	const uint64_t last_par = ((1ull << (D - 2)) / 64 + 31) / 32 * 4;
+	return last_par + (1ull << (D - 1)) / 64 * value_size(dt);
+}
+
 uint64_t build_bytes_needed(pst_dtype dt, pst_idtype it, uint64_t n)
 {
-	return tree_bytes(dt, it, n) + build_scratch_bytes(dt, it, n);
+	return tree_bytes(dt, it, n) + build_scratch_bytes(dt, it, n) + aux_bytes(dt, n);
 }
 
 void build_tree(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
@@ -1181,6 +1193,84 @@ __global__ void k_last_par(const uint32_t *__restrict__ occ, uint32_t L, uint32_
 	}
 }
 
+// Minimum of two dim2 values that keeps a NaN (so that no query's min2 compares
+// at most the minimum of a block with a NaN below it).
+template <typename T>
+__device__ __forceinline__ T min_keep_nan(T a, T b)
+{
+	if constexpr (std::is_floating_point<T>::value) {
+		if (a != a)
+			return a;
+		if (b != b)
+			return b;
+	}
+	return b < a ? b : a;
+}
+
+// sub_min of the 64-slot blocks of level e (one warp per block): its 128 children
+// on level e + 1 (positions 2^(e+1) + 128 j ..), only the occupied ones when that
+// is the last level, and the sub_min of the two child blocks below them.
+template <typename T>
+__global__ void k_sub_min(const T *__restrict__ dim2, const uint32_t *__restrict__ occ, T *sub_min, uint32_t D,
+                          uint32_t e)
+{
+	const uint64_t nb = (1ull << e) / 64;
+	const uint32_t lane = threadIdx.x & 31;
+	for (uint64_t j = ((uint64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < nb;
+	     j += ((uint64_t) gridDim.x * blockDim.x) >> 5) {
+		const uint64_t c0 = (1ull << (e + 1)) + 128 * j;  // first child position
+		const uint64_t p = c0 + 4 * lane;
+		T v[4];
+		if constexpr (sizeof(T) == 4) {
+			const uint4 x = *reinterpret_cast<const uint4 *>(dim2 + p);
+			memcpy(&v[0], &x.x, 4);
+			memcpy(&v[1], &x.y, 4);
+			memcpy(&v[2], &x.z, 4);
+			memcpy(&v[3], &x.w, 4);
+		} else {
+			const double2 a = reinterpret_cast<const double2 *>(dim2 + p)[0];
+			const double2 b = reinterpret_cast<const double2 *>(dim2 + p)[1];
+			v[0] = a.x;
+			v[1] = a.y;
+			v[2] = b.x;
+			v[3] = b.y;
+		}
+		// children on the last level exist where their occupancy bit is set
+		const uint32_t om = e + 2 == D ? (occ[p >> 5] >> (p & 31)) & 0xFu : 0xFu;
+		bool have = false;
+		T m = T(0);
+#pragma unroll
+		for (int k = 0; k < 4; k++)
+			if ((om >> k) & 1u) {
+				m = have ? min_keep_nan(m, v[k]) : v[k];
+				have = true;
+			}
+		if (lane == 0 && e + 2 < D) {
+			// the child blocks' own descendants (levels e + 2 .. D - 1)
+			const T a = sub_min[c0 >> 6], b = sub_min[(c0 >> 6) + 1];
+			m = have ? min_keep_nan(min_keep_nan(m, a), b) : min_keep_nan(a, b);
+			have = true;
+		}
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1) {
+			const T om2 = __shfl_xor_sync(0xFFFFFFFFu, m, o);
+			const bool oh = __shfl_xor_sync(0xFFFFFFFFu, have, o);
+			if (oh)
+				m = have ? min_keep_nan(m, om2) : om2;
+			have = have || oh;
+		}
+		if (lane == 0) {
+			// a block without descendants holds nothing to test: the largest value
+			T none;
+			if constexpr (std::is_floating_point<T>::value)
+				none = std::numeric_limits<T>::infinity();
+			else
+				none = std::numeric_limits<T>::max();
+			sub_min[((1ull << e) >> 6) + j] = have ? m : none;
+		}
+	}
+}
+
 }  // namespace
 
 void finish_tree_aux(TreeStorage &t, cudaStream_t s)
@@ -1199,6 +1289,34 @@ void finish_tree_aux(TreeStorage &t, cudaStream_t s)
 	const unsigned g = (unsigned) std::max<uint64_t>(1, std::min<uint64_t>((nb + 255) / 256, 65535));
 	k_last_par<<<g, 256, 0, s>>>(t.occ, L, t.last_par);
 	PST_CUDA(cudaGetLastError());
+	// sub_min: one value per 64-slot block of positions [64, 2^(D-1)), levels
+	// 6..D-2, built from the bottom up
+	const size_t vs = value_size(t.dtype);
+	e = cudaMalloc(&t.sub_min, ((1ull << (t.levels - 1)) / 64) * vs);
+	if (e == cudaErrorMemoryAllocation) {
+		cudaGetLastError();
+		fail(PST_ERR_NOMEM, "search index allocation failed");
+	}
+	check_cuda(e, "cudaMalloc(search index)");
+	for (uint32_t lv = t.levels - 2; lv >= 6; lv--) {
+		const uint64_t warps = (1ull << lv) / 64;
+		const unsigned gb = (unsigned) std::max<uint64_t>(1, std::min<uint64_t>((warps * 32 + 255) / 256, 1u << 20));
+		switch (t.dtype) {
+		case PST_F32:
+			k_sub_min<float><<<gb, 256, 0, s>>>(static_cast<const float *>(t.dim2), t.occ,
+			                                    static_cast<float *>(t.sub_min), t.levels, lv);
+			break;
+		case PST_F64:
+			k_sub_min<double><<<gb, 256, 0, s>>>(static_cast<const double *>(t.dim2), t.occ,
+			                                     static_cast<double *>(t.sub_min), t.levels, lv);
+			break;
+		case PST_I32:
+			k_sub_min<int32_t><<<gb, 256, 0, s>>>(static_cast<const int32_t *>(t.dim2), t.occ,
+			                                      static_cast<int32_t *>(t.sub_min), t.levels, lv);
+			break;
+		}
+		PST_CUDA(cudaGetLastError());
+	}
 }
 
 void free_tree(TreeStorage &t)
@@ -1209,6 +1327,9 @@ void free_tree(TreeStorage &t)
 	if (t.last_par)
 		cudaFree(t.last_par);
 	t.last_par = nullptr;
+	if (t.sub_min)
+		cudaFree(t.sub_min);
+	t.sub_min = nullptr;
 }
 
 void export_tree(const TreeStorage &t, void *dim1, void *dim2, void *med, uint32_t *ids, uint8_t *bitcodes)

@@ -122,6 +122,11 @@ struct TreeDev {
 	// (null when D-2 < 6).  A sparse last level lets the last expansion skip the
 	// records whose blocks have no children before reading their occupancy.
 	const uint32_t *last_par;
+	// Per 64-slot block of levels 6..D-2 (index = its first position / 64): the
+	// smallest dim2 among all the block's descendants (NaN if any is NaN; null when
+	// D < 8).  A query whose min2 is at most this value reports every descendant of
+	// the block's reported slots, so their dim2 need no test.
+	const T *sub_min;
 };
 
 // Number of levels of a tree of n points: floor(log2 n) + 1 (0 for n == 0).

@@ -59,7 +59,11 @@ struct QOut {
 
 // Alive records cover a "block" of 64 consecutive slots of one level (two
 // 128-byte rows of a 4-byte field): (block base position, query, mask of reported
-// slots, low and high word).  Block bases are multiples of 64.
+// slots, low and high word).  Block bases are multiples of 64; bit 0 of the first
+// word (RECORD_WHOLE) marks a block below which every descendant of the reported
+// slots is reported (its dim2 need no test).
+constexpr uint32_t RECORD_WHOLE = 1u;
+
 struct WorkDev {
 	uint4 *rec;            // alive records of every level, level regions in order
 	uint64_t rec_cap;
@@ -296,25 +300,32 @@ __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__r
 	constexpr int U = sizeof(T) == 4 ? 4 : 2;  // records in flight
 	const uint32_t lane = lane_id();
 	const uint32_t r = lane >> 3, qd = lane & 7;
+	const uint32_t base = mine.x & ~63u;  // bit 0 of a record's block: RECORD_WHOLE
 	// the record's min2 stays in its owner lane's register (its load overlaps the
 	// staging below) and is broadcast by a shuffle where it is compared
 	const T m2_own = valid ? min2s[mine.y] : T(0);
+	// A block whose every descendant has dim2 >= min2 (TreeDev::sub_min): all
+	// descendants of its reported slots are reported, with no test; its child
+	// records carry RECORD_WHOLE, so theirs need no look-up either.
+	bool whole = (mine.x & RECORD_WHOLE) != 0;
+	if (valid && !whole && t.sub_min && base >= 64)
+		whole = m2_own <= t.sub_min[base >> 6];
 	uint4 cand = make_uint4(0, 0, 0, 0);
 	bool has_children = valid;
 	if (LAST && valid) {
 		// expanding into the last level: most blocks of a sparse last level have no
 		// children, which one bit per parent block tells before any occupancy read
-		const uint32_t j = (mine.x - (1u << (t.levels - 2))) >> 6;
+		const uint32_t j = (base - (1u << (t.levels - 2))) >> 6;
 		has_children = (t.last_par[j >> 5] >> (j & 31)) & 1u;
 	}
 	if (has_children) {
 		// children on a full level (every level but the last) need no occupancy read
 		const uint4 occ = full ? make_uint4(FULL, FULL, FULL, FULL)
-		                       : *reinterpret_cast<const uint4 *>(t.occ + ((2 * mine.x) >> 5));
+		                       : *reinterpret_cast<const uint4 *>(t.occ + ((2 * base) >> 5));
 		cand = make_uint4(spread16(mine.z) & occ.x, spread16(mine.z >> 16) & occ.y, spread16(mine.w) & occ.z,
 		                  spread16(mine.w >> 16) & occ.w);
 	}
-	const bool live = (cand.x | cand.y | cand.z | cand.w) != 0;
+	const bool live = !whole && (cand.x | cand.y | cand.z | cand.w) != 0;
 	const uint32_t lm = __ballot_sync(FULL, live);
 	const int nlive = __popc(lm);
 	if (live) {
@@ -335,7 +346,7 @@ __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__r
 			const uint32_t c4 = on ? (candw[4 * k + r] >> (4 * qd)) & 0xFu : 0u;
 			cn[u] = c4;
 			if (c4) {
-				load_quad(t.dim2 + 2 * st.rec[k].x + 4 * lane, v[u]);
+				load_quad(t.dim2 + 2 * (st.rec[k].x & ~63u) + 4 * lane, v[u]);
 			} else {
 #pragma unroll
 				for (int j = 0; j < 4; j++)
@@ -360,14 +371,12 @@ __device__ __forceinline__ void expand_records(const TreeDev<T> &t, const T *__r
 		}
 	}
 	__syncwarp();
-	child[0] = child[1] = make_uint4(0, 0, 0, 0);
-	pts = 0;
-	if (live) {
-		const uint4 rw = st.rows[lane];
-		child[0] = make_uint4(2 * mine.x, mine.y, rw.x, rw.y);
-		child[1] = make_uint4(2 * mine.x + 64, mine.y, rw.z, rw.w);
-		pts = __popc(rw.x) + __popc(rw.y) + __popc(rw.z) + __popc(rw.w);
-	}
+	// the tested rows, or for a whole block its candidates (all reported)
+	const uint4 rw = live ? st.rows[lane] : whole ? cand : make_uint4(0, 0, 0, 0);
+	const uint32_t cx = 2 * base + (whole ? RECORD_WHOLE : 0u);
+	child[0] = make_uint4(cx, mine.y, rw.x, rw.y);
+	child[1] = make_uint4(cx + 64, mine.y, rw.z, rw.w);
+	pts = __popc(rw.x) + __popc(rw.y) + __popc(rw.z) + __popc(rw.w);
 	__syncwarp();  // the stage is reused by the warp's next batch
 }
 
@@ -446,7 +455,7 @@ __device__ __forceinline__ void level_body(const TreeDev<T> &t, const QDev<T> &q
 		uint4 nxt = nvalid ? w.rec[base_prev + wb + lane] : make_uint4(0, 0, 0, 0);
 		// A round's children are reserved with one atomic per warp, but written in the
 		// next round, after that round's loads: the reservation's latency overlaps them.
-		// Pending: this lane's parent block (children at 2p and 2p + 64), query, the
+		// Pending: this lane's first child block (the second at pp + 64), query, the
 		// four child mask words, its first slot offset in the warp's run, and the
 		// warp's reservation (lane 31; ~0 = none or refused).
 		uint32_t pp = 0, pq = 0, pofs = 0, pres = ~0u;
@@ -457,9 +466,9 @@ __device__ __forceinline__ void level_body(const TreeDev<T> &t, const QDev<T> &q
 				return;
 			uint64_t sl = base_cur + r0 + pofs;
 			if (pm.x | pm.y)
-				w.rec[sl++] = make_uint4(2 * pp, pq, pm.x, pm.y);
+				w.rec[sl++] = make_uint4(pp, pq, pm.x, pm.y);
 			if (pm.z | pm.w)
-				w.rec[sl] = make_uint4(2 * pp + 64, pq, pm.z, pm.w);
+				w.rec[sl] = make_uint4(pp + 64, pq, pm.z, pm.w);
 		};
 		for (; wb < n_prev; wb += wr * per) {
 			const bool valid = nvalid;
@@ -491,7 +500,7 @@ __device__ __forceinline__ void level_body(const TreeDev<T> &t, const QDev<T> &q
 					pres = off;
 				}
 			}
-			pp = mine.x;
+			pp = child[0].x;
 			pq = mine.y;
 			pofs = inc - nrec;
 			pm = make_uint4(child[0].z, child[0].w, child[1].z, child[1].w);
@@ -888,7 +897,7 @@ __device__ __forceinline__ void emit_blocks(const TreeDev<T> &t, const uint4 &mi
 			b2[u] = ((lane < 16 ? rc.z : rc.w) >> psh) & 3u;
 			const uint32_t before = __popc(rc.z & below_z) + __popc(rc.w & below_w);
 			o[u] = st.ob[k] + before;
-			hb[u] = rc.x + 2 * lane;
+			hb[u] = (rc.x & ~63u) + 2 * lane;  // (without RECORD_WHOLE)
 			if constexpr (!POINTS || HAS_ID)
 				idv[u] = b2[u] ? *reinterpret_cast<const uint2 *>(t.id + hb[u]) : make_uint2(0, 0);
 			if constexpr (POINTS) {

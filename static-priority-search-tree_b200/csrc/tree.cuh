@@ -23,6 +23,7 @@ struct TreeStorage {
 	uint32_t *id = nullptr;
 	uint32_t *occ = nullptr;
 	uint32_t *last_par = nullptr;  // separate allocation, see TreeDev::last_par
+	void *sub_min = nullptr;       // separate allocation, see TreeDev::sub_min
 	int device = 0;
 	std::mutex mu;        // serialises the single-query engine
 	Batch *single = nullptr;
@@ -31,7 +32,7 @@ struct TreeStorage {
 	TreeDev<T> view() const
 	{
 		return TreeDev<T>{static_cast<const T *>(dim1), static_cast<const T *>(dim2), static_cast<const T *>(med),
-		                  id, occ, n, levels, last_par};
+		                  id, occ, n, levels, last_par, static_cast<const T *>(sub_min)};
 	}
 };
 
@@ -44,7 +45,8 @@ uint64_t build_bytes_needed(pst_dtype dt, pst_idtype it, uint64_t n);
 // Points the field pointers of t (dtype, idtype, n set) into one allocation of
 // tree_bytes(...) bytes laid out as the builder lays it out.
 void attach_tree_memory(TreeStorage &t, void *mem);
-// Derives the auxiliary search index (TreeDev::last_par) from the occupancy.
+// Derives the auxiliary search indexes (TreeDev::last_par, TreeDev::sub_min) from
+// the occupancy and the dim2 values.
 void finish_tree_aux(TreeStorage &t, cudaStream_t s);
 // Tree image: a 64-byte header followed by the device allocation byte for byte.
 uint64_t serialized_size(const TreeStorage &t);
