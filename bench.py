@@ -451,10 +451,10 @@ def sweep(pst, torch, n, peak, seed=1):
         torch.cuda.synchronize()
         build_ms = 1000 * (time.perf_counter() - t0)
         r = ips_scan(pst, torch, pts, n, dt, has_id)
-        # the survey's algorithmic bytes: dim1 and dim2 of every point, id and record of every hit
+        # the scan's algorithmic bytes: dim1 and dim2 of every point, id and record of every hit
         vs_ = 8 if dt == "f64" else 4
-        r["survey_bytes"] = n * 2 * vs_ + r["hits"] * ((4 if has_id else 0) + (4 if has_id else 2 * vs_))
-        r["frac"] = r["survey_bytes"] / (r["ms"] / 1000) / 1e9 / peak
+        r["algorithmic_bytes"] = n * 2 * vs_ + r["hits"] * ((4 if has_id else 0) + (4 if has_id else 2 * vs_))
+        r["frac"] = r["algorithmic_bytes"] / (r["ms"] / 1000) / 1e9 / peak
         # the records are read whole (the id sits between the values): bytes of the layout
         r["frac_layout"] = r["gbs"] / peak
         ips_rows.append(r)
