@@ -193,3 +193,40 @@ def test_large_random_trees_2p26(pst, oracle, dt, has_id):
     eng.close()
     tree.close()
     torch.cuda.empty_cache()
+
+
+def test_top_pass_large_limit_2p25(pst, oracle):
+    """Small batches on a deep tree with the largest top-pass batch limit (1024, so
+    the one-CTA pass keeps 4 x 2048 path and seed slots and ~5300 records in shared
+    memory): batches of 40 … 240 tiny queries run the top pass over most of the 26
+    levels and hand their records, paths and seeds over to the level kernels where
+    a level first holds more than 256 records.  Every query is checked against brute
+    force.  (The record array's own bound, checked before each level, is a safety
+    net: records grow about geometrically with depth, so a level exceeds 256 records
+    before the levels above it fill the array.)"""
+    import torch
+    n = 1 << 25
+    rec = bench.gen_points_device(n, seed=4, torch=torch)
+    tree = pst.StaticPSTGPU(rec, n, "f32", True)
+    assert tree.info()["levels"] == 26
+    pts_host = _device_records_to_host(rec, "f32", True, oracle)
+    del rec
+    eng = pst.BatchEngine(tree, max_queries=1024, task_capacity=1 << 22, top_pass_queries=1024)
+    rng = np.random.default_rng(11)
+    D, w = float(1 << 24), float(1 << 16)
+    for nq in (40, 80, 120, 160, 240):
+        kinds = np.where(np.arange(nq) % 2 == 0, 0, 1).astype(np.int32)
+        a = rng.uniform(w, D - w, nq)
+        width = rng.uniform(4.0, 40.0, nq)
+        min1 = np.where(kinds == 0, a, 0.0)
+        max1 = np.where(kinds == 0, a + width, a)
+        min2 = np.where(kinds == 0, a, a + w - width)  # left: only points within ~width of max1 reach min2
+        q_host = pst.make_queries(kinds, min1.astype(np.float32), max1.astype(np.float32),
+                                  min2.astype(np.float32), "f32")
+        out, offs, counts = _batched_results(pst, torch, eng, q_host, "ids", 4)
+        assert counts.sum() > 0
+        _check_sample(oracle, pts_host, "f32", q_host, np.arange(nq), out, offs, 4, "ids")
+        del out
+    eng.close()
+    tree.close()
+    torch.cuda.empty_cache()
