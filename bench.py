@@ -1157,9 +1157,9 @@ def main():
             line["ips"] = ips_rows
         if iso_res is not None:
             line["isosurface"] = iso_res
-        # per step: query preparation, one kernel per level, offsets, emit (a batch of
-        # 4096 queries takes the one-launch offsets scan)
-        line["gpu_launches"] = (levels_main + 3) * args.steps
+        # per step: the control block's load, query preparation, one kernel per level,
+        # offsets, emit (a batch of 4096 queries takes the one-launch offsets scan)
+        line["gpu_launches"] = (levels_main + 4) * args.steps
         print(json.dumps(line))
     if eng is not None:
         eng.close()
