@@ -106,3 +106,21 @@ def test_whole_blocks_after_image(pst, oracle):
         got = back.search(kind, a, b, m2, ret="ids")
         assert np.array_equal(oracle.canon(got), _oracle_set(oracle, ref, kind, a, b, m2, False)), (kind, a, b, m2)
     back.close()
+
+
+@pytest.mark.parametrize("dt", ["f32", "f64", "i32"])
+@pytest.mark.parametrize("n", [127, 128, 200, 255, 256, 511, 1000])
+def test_whole_blocks_smallest_trees(pst, oracle, dt, n):
+    """Trees of 7 to 10 levels: the subtree minima exist from 8 levels on (one
+    64-slot block level at first), below that the shortcut is off.  Every query
+    of the whole-block mix, plus the extremes, against the oracle."""
+    pts = rand_points(n, dt, ids="random", seed=n + 17, width=3.0)
+    ref = oracle.Orc.build(pts, dt)
+    tr = pst.StaticPSTGPU.from_numpy(pts, dt)
+    qs = _low_min2_queries(pts, 12, seed=n)
+    lo, hi = (-(2 ** 31), 2 ** 31 - 1) if dt == "i32" else (-np.inf, np.inf)
+    qs += [("three", lo, hi, lo), ("left", 0, hi, lo), ("right", lo, 0, lo)]
+    for kind, a, b, m2 in qs:
+        got = tr.search(kind, a, b, m2, ret="ids")
+        assert np.array_equal(oracle.canon(got), _oracle_set(oracle, ref, kind, a, b, m2, False)), (kind, a, b, m2)
+    tr.close()
