@@ -17,10 +17,13 @@
 //     blocks (spread16), masked by occupancy before anything is loaded.  Every
 //     level but the last is full (a level-d node holds at least
 //     floor((n + 1) / 2^d) - 1 >= 1 points for d <= D - 2), so occupancy is read
-//     only for children on the last level.
-// A count of every query falls out of the pass; an exclusive scan gives each
-// query's exact output offset, and a flat emit kernel writes ids (or points) from
-// the alive records.
+//     only for children on the last level.  A block whose whole subtree lies at
+//     or above the query's min2 (TreeDev::sub_min) hands its descendants on
+//     without any dim2 test (RECORD_WHOLE).
+// Small batches start with one CTA that walks the upper levels with its frontier
+// in shared memory (k_bfs_cta).  A count of every query falls out of the pass; an
+// exclusive scan gives each query's exact output offset, and a flat emit kernel
+// writes ids (or points) from the alive records.
 #include <algorithm>
 #include <mutex>
 #include <string>
