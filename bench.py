@@ -874,21 +874,23 @@ def main():
     torch.cuda.synchronize()
     construct_cold_ms = 1000 * (time.perf_counter() - c0)
     tree.close()
-    # the median of five warm builds: a build's wall time includes the allocation
+    # the median of nine warm builds: a build's wall time includes the allocation
     # of the tree and of its working set (7.1 GiB and more at 2^28), whose cost
-    # varies from call to call while the kernels do not (NVTX range "construct"
-    # around the last build only)
+    # varies from call to call (single builds of several times the median were seen
+    # on shared machines) while the kernels do not (NVTX range "construct" around
+    # the last build only)
     construct_runs = []
-    for b in range(5):
+    n_builds = 9
+    for b in range(n_builds):
         c0 = time.perf_counter()
-        if b == 4:
+        if b == n_builds - 1:
             torch.cuda.nvtx.range_push("construct")
         tree = pst.StaticPSTGPU(pts_d, n, "f32", True)
-        if b == 4:
+        if b == n_builds - 1:
             torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         construct_runs.append(1000 * (time.perf_counter() - c0))
-        if b < 4:
+        if b < n_builds - 1:
             tree.close()
     construct_ms = statistics.median(construct_runs)
     log(f"constructed 2^{args.points_log2} points in {construct_ms:.1f} ms (median of "

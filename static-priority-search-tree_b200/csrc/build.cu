@@ -527,7 +527,8 @@ __global__ void k_level_nodes(BuildCtx<T, HAS_ID> c, uint32_t d, const uint32_t 
 // reads in flight together), so node writes never wait on global memory.
 
 // Shared-memory carve-up of k_subtree, in bytes: points first (8-byte aligned for
-// doubles), then the u64 keys, the u16 point slots and the u16 arg-max per sub-node.
+// doubles), then the u64 keys, the u16 point slots, the u16 sub-node of every key
+// and the u16 arg-max per sub-node.
 template <typename T, bool HAS_ID>
 struct SubtreeSmem {
 	static constexpr size_t PTS = 0;
@@ -535,7 +536,9 @@ struct SubtreeSmem {
 	static constexpr size_t KEYB = KEYA + (size_t) ST_CAP * 8;
 	static constexpr size_t SLOTA = KEYB + (size_t) ST_CAP * 8;
 	static constexpr size_t SLOTB = SLOTA + (size_t) ST_CAP * 2;
-	static constexpr size_t TOPI = SLOTB + (size_t) ST_CAP * 2;
+	static constexpr size_t SEGA = SLOTB + (size_t) ST_CAP * 2;
+	static constexpr size_t SEGB = SEGA + (size_t) ST_CAP * 2;
+	static constexpr size_t TOPI = SEGB + (size_t) ST_CAP * 2;
 	static constexpr size_t CNT = TOPI + (size_t) ST_CAP * 2;
 	static constexpr size_t START = CNT + (size_t) ST_CAP * 2;
 	static constexpr size_t WS = START + (size_t) ST_CAP * 2;
@@ -554,6 +557,21 @@ constexpr int ST_GATHER = (ST_CAP + ST_THREADS - 1) / ST_THREADS + 1;
 // the rest and the right child the others, so
 //   start(2t) = start(t) - t,  start(2t+1) = start(t) - t + floor(c/2).
 
+// The node count of node_count in 32 bits (trees hold fewer than 2^31 points).
+__device__ __forceinline__ uint32_t node_count32(uint32_t n, uint32_t d, uint32_t j)
+{
+	uint32_t c = n;
+	for (int b = (int) d - 1; b >= 0 && c != 0; b--)
+		c = ((j >> b) & 1u) ? c - 1u - (c >> 1) : c >> 1;
+	return c;
+}
+
+// Sub-node counts and warps come in powers of two: every quotient in the builder is
+// a shift (a run-time divisor costs a division sequence per use, and the builder is
+// bound by its instruction issue).
+constexpr int ST_LOG_WARPS = 3;
+static_assert(ST_THREADS == 32 << ST_LOG_WARPS, "k_subtree: 8 warps");
+
 template <typename T, bool HAS_ID>
 __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, uint32_t L0,
                                                        const uint32_t *__restrict__ B)
@@ -566,6 +584,8 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 	uint64_t *kn = reinterpret_cast<uint64_t *>(st_smem + SM::KEYB);
 	uint16_t *sc = reinterpret_cast<uint16_t *>(st_smem + SM::SLOTA);
 	uint16_t *sn = reinterpret_cast<uint16_t *>(st_smem + SM::SLOTB);
+	uint16_t *gc = reinterpret_cast<uint16_t *>(st_smem + SM::SEGA);     // sub-node of each key
+	uint16_t *gn = reinterpret_cast<uint16_t *>(st_smem + SM::SEGB);
 	uint16_t *topi = reinterpret_cast<uint16_t *>(st_smem + SM::TOPI);    // [ST_CAP]
 	uint16_t *scnt = reinterpret_cast<uint16_t *>(st_smem + SM::CNT);     // [ST_CAP]
 	uint16_t *sstart = reinterpret_cast<uint16_t *>(st_smem + SM::START); // [ST_CAP]
@@ -576,17 +596,16 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 	__shared__ uint32_t s_n;
 
 	const uint32_t j = blockIdx.x;
-	const uint64_t cN64 = node_count(c.n, L0, j);
-	if (cN64 == 0 || *c.err)
+	const uint32_t cN = node_count32((uint32_t) c.n, L0, j);
+	if (cN == 0 || *c.err)
 		return;
 	const uint32_t lo = L0 ? B[j] : 0u;
 	const uint32_t hi = L0 ? B[j + 1] : (uint32_t) c.n;
-	if (lo >= hi || hi > c.n || cN64 > ST_CAP || hi - lo > (uint32_t) (ST_GATHER * ST_THREADS)) {
+	if (lo >= hi || hi > c.n || cN > ST_CAP || hi - lo > (uint32_t) (ST_GATHER * ST_THREADS)) {
 		if (threadIdx.x == 0)
 			atomicOr(c.err, 16u);
 		return;
 	}
-	const uint32_t cN = (uint32_t) cN64;
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = ST_THREADS / 32;
 
 	// Gather the keys of the points still free in [lo, hi), in dim1 order: every
@@ -599,13 +618,20 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 	{
 		uint64_t v[ST_GATHER];
 		K v1[ST_GATHER];
-		uint32_t m[ST_GATHER];
+		uint32_t m[ST_GATHER], tw[ST_GATHER];
+		// the keys are read with the taken bits, not after them: one round trip
 #pragma unroll
 		for (int u = 0; u < ST_GATHER; u++) {
 			const uint32_t i = lo + (uint32_t) u * ST_THREADS + threadIdx.x;
-			const bool keep = i < hi && !c.is_taken(i);
-			v[u] = keep ? c.c2s[i] : 0;
-			v1[u] = (KEYS4 && c.recon && keep) ? c.k1s[i] : K(0);
+			const bool in = i < hi;
+			tw[u] = in ? c.taken[i >> 5] : 0u;
+			v[u] = in ? c.c2s[i] : 0;
+			v1[u] = (KEYS4 && c.recon && in) ? c.k1s[i] : K(0);
+		}
+#pragma unroll
+		for (int u = 0; u < ST_GATHER; u++) {
+			const uint32_t i = lo + (uint32_t) u * ST_THREADS + threadIdx.x;
+			const bool keep = i < hi && !((tw[u] >> (i & 31)) & 1u);
 			m[u] = __ballot_sync(0xFFFFFFFFu, keep);
 			if (lane == 0)
 				s_pre[u][warp] = __popc(m[u]);
@@ -642,6 +668,7 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 				if (pos < ST_CAP) {
 					kc[pos] = v[u];
 					sc[pos] = (uint16_t) pos;
+					gc[pos] = 0;
 					if (KEYS4 && c.recon)
 						k1c[pos] = v1[u];
 				}
@@ -689,14 +716,15 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 	__syncthreads();
 	for (uint32_t s = 0;; s++) {
 		const uint32_t nsub = 1u << s;
-		const bool wide = present / nsub >= 64;
+		const bool wide = (present >> s) >= 64;
 		// arg-max of every sub-node (keys are distinct)
 		if (wide && nsub < (uint32_t) nwarps) {
 			// fewer sub-nodes than warps: each sub-node's keys are split over
-			// nwarps / nsub warps, whose maxima meet in shared memory
-			const uint32_t W = (uint32_t) nwarps / nsub, t = warp / W, p = warp % W;
+			// W = nwarps / nsub warps, whose maxima meet in shared memory
+			const uint32_t lw = ST_LOG_WARPS - s;  // log2 W
+			const uint32_t W = 1u << lw, t = (uint32_t) warp >> lw, p = (uint32_t) warp & (W - 1u);
 			const uint32_t ct = scnt[t], st = sstart[t];
-			const uint32_t a = st + (uint32_t) ((uint64_t) ct * p / W), e = st + (uint32_t) ((uint64_t) ct * (p + 1) / W);
+			const uint32_t a = st + ((ct * p) >> lw), e = st + ((ct * (p + 1)) >> lw);
 			uint64_t bk = 0;
 			uint32_t bi = 0;
 			for (uint32_t i = a + lane; i < e; i += 32)
@@ -764,8 +792,10 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 			}
 		}
 		__syncthreads();
-		// write the nodes of this sub-level
+		// write the nodes of this sub-level (warps past the last sub-node skip whole)
 		for (uint32_t tb = 0; tb < nsub; tb += ST_THREADS) {
+			if (tb + (uint32_t) warp * 32 >= nsub)
+				break;
 			const uint32_t t = tb + threadIdx.x;
 			bool occupied = false;
 			uint32_t h = 0;
@@ -803,59 +833,47 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 		if (s == last_s)
 			break;
 		// drop each sub-node's point; every sub-node above the last level holds one.
-		// Up to 64 sub-nodes the keys move independently (each finds its sub-node by
-		// a binary search of the starts); below that each thread moves a sub-node's
-		// few keys.
-		if (nsub <= 64) {
-			for (uint32_t i = threadIdx.x; i < present; i += ST_THREADS) {
-				// the sub-node holding i: the last one starting at or before i (an empty
-				// sub-node starts where the next one does, so this one is not empty)
-				uint32_t tl = 0, th = nsub;
-				while (th - tl > 1) {
-					const uint32_t mid = (tl + th) / 2;
-					if (sstart[mid] <= i)
-						tl = mid;
-					else
-						th = mid;
-				}
-				const uint32_t ti = topi[tl];
-				if (i != ti) {
-					const uint32_t ni = i - tl - (i > ti ? 1u : 0u);
-					kn[ni] = kc[i];
-					sn[ni] = sc[i];
-				}
-			}
-		} else {
-			for (uint32_t t = threadIdx.x; t < nsub; t += ST_THREADS) {
-				const uint32_t ct = scnt[t], st = sstart[t];
-				const uint32_t ti = topi[t];
-				for (uint32_t i = st; i < st + ct; i++)
-					if (i != ti) {
-						const uint32_t ni = i - t - (i > ti ? 1u : 0u);
-						kn[ni] = kc[i];
-						sn[ni] = sc[i];
-					}
+		// Every key knows its sub-node t, so it moves on its own: past the t points
+		// dropped before its sub-node, and its own sub-node's if that came first.  Of
+		// the keys a sub-node keeps, the first floor(ct / 2) go to its left child.
+		for (uint32_t i = threadIdx.x; i < present; i += ST_THREADS) {
+			const uint32_t t = gc[i];
+			const uint32_t ti = topi[t];
+			if (i != ti) {
+				const uint32_t ni = i - t - (i > ti ? 1u : 0u);
+				const uint32_t rank = ni - (sstart[t] - t);  // among the sub-node's keys kept
+				kn[ni] = kc[i];
+				sn[ni] = sc[i];
+				gn[ni] = (uint16_t) (2u * t + (rank >= (uint32_t) (scnt[t] >> 1) ? 1u : 0u));
 			}
 		}
 		// spans of the next sub-level, in place: parents to registers, then children
+		// (warps past the last sub-node have none)
 		constexpr int PMAX = (ST_CAP / 2 + ST_THREADS - 1) / ST_THREADS;
-		uint32_t pc[PMAX], ps[PMAX];
+		uint32_t pc[PMAX] = {}, ps[PMAX] = {};
+		const bool spans = (uint32_t) warp * 32 < nsub;
+		if (spans) {
 #pragma unroll
-		for (int u = 0; u < PMAX; u++) {
-			const uint32_t t = threadIdx.x + u * ST_THREADS;
-			pc[u] = t < nsub ? scnt[t] : 0u;
-			ps[u] = t < nsub ? sstart[t] : 0u;
+			for (int u = 0; u < PMAX; u++) {
+				const uint32_t t = threadIdx.x + u * ST_THREADS;
+				if (t < nsub) {
+					pc[u] = scnt[t];
+					ps[u] = sstart[t];
+				}
+			}
 		}
 		__syncthreads();
+		if (spans) {
 #pragma unroll
-		for (int u = 0; u < PMAX; u++) {
-			const uint32_t t = threadIdx.x + u * ST_THREADS;
-			if (t < nsub) {
-				const uint32_t left = pc[u] / 2;
-				scnt[2 * t] = (uint16_t) (pc[u] ? left : 0u);
-				scnt[2 * t + 1] = (uint16_t) (pc[u] ? pc[u] - 1 - left : 0u);
-				sstart[2 * t] = (uint16_t) (ps[u] - t);
-				sstart[2 * t + 1] = (uint16_t) (ps[u] - t + left);
+			for (int u = 0; u < PMAX; u++) {
+				const uint32_t t = threadIdx.x + u * ST_THREADS;
+				if (t < nsub) {
+					const uint32_t left = pc[u] / 2;
+					scnt[2 * t] = (uint16_t) (pc[u] ? left : 0u);
+					scnt[2 * t + 1] = (uint16_t) (pc[u] ? pc[u] - 1 - left : 0u);
+					sstart[2 * t] = (uint16_t) (ps[u] - t);
+					sstart[2 * t + 1] = (uint16_t) (ps[u] - t + left);
+				}
 			}
 		}
 		present -= nsub;
@@ -865,8 +883,12 @@ __global__ void __launch_bounds__(ST_THREADS) k_subtree(BuildCtx<T, HAS_ID> c, u
 		uint16_t *ts = sc;
 		sc = sn;
 		sn = ts;
+		ts = gc;
+		gc = gn;
+		gn = ts;
 		__syncthreads();
 	}
+
 }
 
 template <typename T>
@@ -953,6 +975,23 @@ inline unsigned grid_for(uint64_t n, int threads)
 
 // Scratch bytes of build_impl beyond the tree itself.
 uint64_t build_scratch_bytes(pst_dtype dt, pst_idtype it, uint64_t n) { return scratch_layout(dt, it, n).total; }
+
+// The tree's memory (one allocation; its occupancy bitmap cleared on `s`).  Called
+// with the builder's sorts already queued on `s`: mapping several GB takes the host
+// milliseconds, which then overlap the sorts instead of preceding them.
+void alloc_tree(TreeStorage &t, cudaStream_t s)
+{
+	const TreeLayout L = tree_layout(t.dtype, t.idtype, t.n);
+	cudaError_t e = cudaMalloc(&t.mem, L.total);
+	if (e == cudaErrorMemoryAllocation) {
+		cudaGetLastError();
+		t.mem = nullptr;
+		fail(PST_ERR_NOMEM, "tree allocation of " + std::to_string(L.total) + " B failed");
+	}
+	check_cuda(e, "cudaMalloc(tree)");
+	attach_tree_memory(t, t.mem);
+	PST_CUDA(cudaMemsetAsync(t.occ, 0, L.total - L.off_occ, s));
+}
 
 template <typename T, bool HAS_ID>
 void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
@@ -1041,6 +1080,7 @@ void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 		sc.vals_tmp = nullptr;
 		radix_sort<K, uint64_t>(static_cast<K *>(k1), c2, n, rs_passes<K>(range[0], range[1]), sc, &k1s, &c2s, s);
 	}
+	alloc_tree(t, s);
 
 	// ---- levels
 	const uint32_t L0 = std::min(subtree_level(n), D - 1);
@@ -1142,16 +1182,8 @@ void build_tree(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 		return;
 	if (!pts_d)
 		fail(PST_ERR_INVALID, "null point array");
-	const TreeLayout L = tree_layout(t.dtype, t.idtype, n);
-	cudaError_t e = cudaMalloc(&t.mem, L.total);
-	if (e == cudaErrorMemoryAllocation) {
-		cudaGetLastError();
-		fail(PST_ERR_NOMEM, "tree allocation of " + std::to_string(L.total) + " B failed");
-	}
-	check_cuda(e, "cudaMalloc(tree)");
-	attach_tree_memory(t, t.mem);
-	PST_CUDA(cudaMemsetAsync(t.occ, 0, L.total - L.off_occ, s));
 	try {
+		// the tree's own memory is allocated by build_impl once its sorts are queued
 		switch (t.dtype) {
 		case PST_F32:
 			t.idtype == PST_ID_U32 ? build_impl<float, true>(t, pts_d, n, s) : build_impl<float, false>(t, pts_d, n, s);
