@@ -224,32 +224,6 @@ __device__ void block_range_fold(K lo, K hi, K *range)
 // ---------------------------------------------------------------------------
 // Preparation kernels.
 
-// flag |= 1 when ids decrease somewhere, |= 2 when some id differs from its input
-// index; id_range = [min id, max id].
-template <typename T, bool HAS_ID>
-__global__ void k_ids_scan(const Point<T, HAS_ID> *pts, uint64_t n, uint32_t *flag, uint32_t *id_range)
-{
-	if constexpr (HAS_ID) {
-		uint32_t lo = 0xFFFFFFFFu, hi = 0;
-		bool dec = false, other = false;
-		for (uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
-		     i += (uint64_t) gridDim.x * blockDim.x) {
-			const uint32_t v = pts[i].id;
-			lo = min(lo, v);
-			hi = max(hi, v);
-			if (i + 1 < n && v > pts[i + 1].id)
-				dec = true;
-			if ((uint64_t) v != i)
-				other = true;
-		}
-		if (__any_sync(0xFFFFFFFFu, dec) && (threadIdx.x & 31) == 0)
-			atomicOr(flag, 1u);
-		if (__any_sync(0xFFFFFFFFu, other) && (threadIdx.x & 31) == 0)
-			atomicOr(flag, 2u);
-		block_range_fold<uint32_t>(lo, hi, id_range);
-	}
-}
-
 template <typename T, bool HAS_ID>
 __global__ void k_id_keys(const Point<T, HAS_ID> *pts, uint64_t n, uint32_t *keys)
 {
@@ -259,20 +233,50 @@ __global__ void k_id_keys(const Point<T, HAS_ID> *pts, uint64_t n, uint32_t *key
 	}
 }
 
+// Copies of the digit histogram a block of k_prep_keys keeps in shared memory (a
+// quarter of its warps on each), so that keys sharing a digit meet on fewer counters.
+constexpr int PK_HIST_COPIES = 4;
+
 // Keys in tiebreak-rank order r (input index P[r]): k1[r] = dim1 key and either the
 // final 64-bit dim2 key (4-byte values) or the raw dim2 key k2[r] (doubles).
 // range = [min k1, max k1, min k2, max k2]; *negzero |= 1 when a value is -0.0 (the
 // one value its key does not keep).
-template <typename T, bool HAS_ID>
+// SCAN_IDS (P null, points with ids): the same pass checks the ids, idflag |= 1 when
+// they decrease somewhere and |= 2 when some id differs from its input index,
+// id_range = [min id, max id].  hist (non-null): the pass also counts the 8-bit
+// digits of the dim1 keys, hist[d * 256 + v] += keys whose digit d is v, for every
+// digit of the key (the radix sort's histogram, which the order of the keys does
+// not change); dynamic shared memory PK_HIST_COPIES * sizeof(K) * 256 words.
+template <typename T, bool HAS_ID, bool SCAN_IDS>
 __global__ void k_prep_keys(const Point<T, HAS_ID> *pts, const uint32_t *P, uint64_t n,
                             typename KeyOf<T>::K *k1, uint64_t *c2, typename KeyOf<T>::K *k2,
-                            typename KeyOf<T>::K *range, uint32_t *negzero)
+                            typename KeyOf<T>::K *range, uint32_t *negzero, uint32_t *idflag,
+                            uint32_t *id_range, uint32_t *hist)
 {
 	using K = typename KeyOf<T>::K;
+	constexpr int ND = (int) sizeof(K);  // 8-bit digits of a key
+	extern __shared__ uint32_t pk_hist[];
+	uint32_t *myh = pk_hist + ((threadIdx.x >> 5) % PK_HIST_COPIES) * (ND * 256);
+	if (hist) {
+		for (int i = threadIdx.x; i < PK_HIST_COPIES * ND * 256; i += blockDim.x)
+			pk_hist[i] = 0;
+		__syncthreads();
+	}
 	K lo1 = ~K(0), hi1 = 0, lo2 = ~K(0), hi2 = 0;
 	bool nz = false;
+	uint32_t ilo = 0xFFFFFFFFu, ihi = 0;
+	bool dec = false, other = false;
 	for (uint64_t r = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (uint64_t) gridDim.x * blockDim.x) {
 		const Point<T, HAS_ID> p = pts[P ? P[r] : r];
+		if constexpr (SCAN_IDS && HAS_ID) {
+			const uint32_t v = p.id;
+			ilo = min(ilo, v);
+			ihi = max(ihi, v);
+			if (r + 1 < n && v > pts[r + 1].id)
+				dec = true;
+			if ((uint64_t) v != r)
+				other = true;
+		}
 		const K a = KeyOf<T>::key(p.dim1), b = KeyOf<T>::key(p.dim2);
 		if constexpr (!std::is_integral<T>::value)
 			nz |= (p.dim1 == T(0) && signbit(p.dim1)) || (p.dim2 == T(0) && signbit(p.dim2));
@@ -281,6 +285,11 @@ __global__ void k_prep_keys(const Point<T, HAS_ID> *pts, const uint32_t *P, uint
 			c2[r] = ((uint64_t) b << 32) | (uint64_t) (r + 1);
 		else
 			k2[r] = b;
+		if (hist) {
+#pragma unroll
+			for (int d = 0; d < ND; d++)
+				atomicAdd(&myh[d * 256 + (uint32_t) ((a >> (8 * d)) & 0xFFu)], 1u);
+		}
 		lo1 = a < lo1 ? a : lo1;
 		hi1 = a > hi1 ? a : hi1;
 		lo2 = b < lo2 ? b : lo2;
@@ -288,9 +297,28 @@ __global__ void k_prep_keys(const Point<T, HAS_ID> *pts, const uint32_t *P, uint
 	}
 	if (__any_sync(0xFFFFFFFFu, nz) && (threadIdx.x & 31) == 0)
 		atomicOr(negzero, 1u);
+	if constexpr (SCAN_IDS && HAS_ID) {
+		if (__any_sync(0xFFFFFFFFu, dec) && (threadIdx.x & 31) == 0)
+			atomicOr(idflag, 1u);
+		if (__any_sync(0xFFFFFFFFu, other) && (threadIdx.x & 31) == 0)
+			atomicOr(idflag, 2u);
+		block_range_fold<uint32_t>(ilo, ihi, id_range);
+		__syncthreads();
+	}
 	block_range_fold<K>(lo1, hi1, range);
 	__syncthreads();
 	block_range_fold<K>(lo2, hi2, range + 2);
+	if (hist) {
+		__syncthreads();
+		for (int i = threadIdx.x; i < ND * 256; i += blockDim.x) {
+			uint32_t t = 0;
+#pragma unroll
+			for (int c = 0; c < PK_HIST_COPIES; c++)
+				t += pk_hist[c * ND * 256 + i];
+			if (t)
+				atomicAdd(&hist[i], t);
+		}
+	}
 }
 
 // Doubles: S2 = dim2-sorted position -> tb (null: identity); c2[tb] = rank << 32 | tb + 1.
@@ -900,7 +928,7 @@ T *as(void *p)
 // All construction scratch lives in one device allocation (one cudaMalloc maps it
 // far faster than a dozen stream-ordered allocations that regrow a trimmed pool).
 struct ScratchLayout {
-	size_t k1, kalt, c2, valt, k2, v32a, v32b, P, rs_status, rs_misc, flags, Ba, Bb, best, top, taken, tmax;
+	size_t k1, kalt, c2, valt, k2, v32a, v32b, P, rs_status, rs_misc, hist1, flags, Ba, Bb, best, top, taken, tmax;
 	size_t total;
 };
 
@@ -930,6 +958,7 @@ ScratchLayout scratch_layout(pst_dtype dt, pst_idtype it, uint64_t n)
 	L.P = take(it == PST_ID_U32 ? n * 4 : 0);
 	L.rs_status = take(256 * rs_tiles * 8);
 	L.rs_misc = take(rs_misc_words() * 4);
+	L.hist1 = take(RS_MAX_PASSES * 256 * 4);
 	L.flags = take(256);
 	L.Ba = take((nodes_wide + 1) * 4);
 	L.Bb = take((nodes_wide + 1) * 4);
@@ -1029,37 +1058,46 @@ void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 	PST_CUDA(cudaMemsetAsync(sc.status, 0, 256 * rs_num_tiles(n) * 8, s));
 
 	const unsigned g = grid_for(n, 256);
-	// ---- tiebreak order: (id, input index) when ids are not already non-decreasing
+	// ---- keys, made in input order; the same pass checks the ids and counts the
+	// dim1 keys' digits for their sort
+	uint32_t *hist1 = scr.at<uint32_t>(SL.hist1);
+	PST_CUDA(cudaMemsetAsync(hist1, 0, RS_MAX_PASSES * 256 * 4, s));
+	const size_t pk_smem = (size_t) PK_HIST_COPIES * sizeof(K) * 256 * 4;
+	k_prep_keys<T, HAS_ID, HAS_ID><<<g, 256, pk_smem, s>>>(pts, nullptr, n, static_cast<K *>(k1), c2,
+	                                                       scr.at<K>(SL.k2), krange, flag + 4, flag, flag + 2,
+	                                                       hist1);
+	PST_CUDA(cudaGetLastError());
+	K range[4];
+	uint32_t negzero = 0, idscan[4] = {0, 0, 0, 0};
+	PST_CUDA(cudaMemcpyAsync(range, krange, sizeof(range), cudaMemcpyDeviceToHost, s));
+	PST_CUDA(cudaMemcpyAsync(&negzero, flag + 4, 4, cudaMemcpyDeviceToHost, s));
+	PST_CUDA(cudaMemcpyAsync(idscan, flag, 16, cudaMemcpyDeviceToHost, s));
+	PST_CUDA(cudaStreamSynchronize(s));
+	// ---- tiebreak order (id, input index): the input order unless the ids decrease
+	// somewhere, then the keys are made again in the order of one sort of the ids
 	const uint32_t *P = nullptr;
 	bool ids_are_indices = true;
 	if constexpr (HAS_ID) {
-		k_ids_scan<T, HAS_ID><<<g, 256, 0, s>>>(pts, n, flag, flag + 2);
-		uint32_t host[4];
-		PST_CUDA(cudaMemcpyAsync(host, flag, 16, cudaMemcpyDeviceToHost, s));
-		PST_CUDA(cudaStreamSynchronize(s));
-		ids_are_indices = !(host[0] & 2u);
-		if (host[0] & 1u) {
+		ids_are_indices = !(idscan[0] & 2u);
+		if (idscan[0] & 1u) {
 			uint32_t *idk = static_cast<uint32_t *>(k1);  // k1 holds at least n u32
 			k_id_keys<T, HAS_ID><<<g, 256, 0, s>>>(pts, n, idk);
 			sc.keys_alt = kalt;
 			sc.vals_alt = valt;  // n u32 fit in the u64 buffers
 			sc.vals_tmp = c2;
 			uint32_t *kres, *vres;
-			radix_sort<uint32_t, uint32_t>(idk, nullptr, n, rs_passes<uint32_t>(host[2], host[3]), sc, &kres, &vres, s);
+			radix_sort<uint32_t, uint32_t>(idk, nullptr, n, rs_passes<uint32_t>(idscan[2], idscan[3]), sc, &kres,
+			                               &vres, s);
 			// ids decrease somewhere, so they are not all equal and the sort ran
 			PST_CUDA(cudaMemcpyAsync(scr.at<uint32_t>(SL.P), vres, n * 4, cudaMemcpyDeviceToDevice, s));
 			P = scr.at<uint32_t>(SL.P);
+			// the same keys in the new order: ranges and digit counts stand, so neither
+			// is made again (the sort's error bits in flag[1] are kept)
+			k_prep_keys<T, HAS_ID, false><<<g, 256, 0, s>>>(pts, P, n, static_cast<K *>(k1), c2, scr.at<K>(SL.k2),
+			                                                krange, flag + 4, nullptr, nullptr, nullptr);
+			PST_CUDA(cudaGetLastError());
 		}
 	}
-	// ---- keys in tiebreak order
-	k_prep_keys<T, HAS_ID><<<g, 256, 0, s>>>(pts, P, n, static_cast<K *>(k1), c2, scr.at<K>(SL.k2), krange,
-	                                         flag + 4);
-	PST_CUDA(cudaGetLastError());
-	K range[4];
-	uint32_t negzero = 0;
-	PST_CUDA(cudaMemcpyAsync(range, krange, sizeof(range), cudaMemcpyDeviceToHost, s));
-	PST_CUDA(cudaMemcpyAsync(&negzero, flag + 4, 4, cudaMemcpyDeviceToHost, s));
-	PST_CUDA(cudaStreamSynchronize(s));
 	if constexpr (WIDE_KEY) {
 		// dim2 ranks: stable sort of the dim2 keys in tiebreak order
 		sc.keys_alt = kalt;
@@ -1078,7 +1116,8 @@ void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 		sc.keys_alt = kalt;
 		sc.vals_alt = valt;
 		sc.vals_tmp = nullptr;
-		radix_sort<K, uint64_t>(static_cast<K *>(k1), c2, n, rs_passes<K>(range[0], range[1]), sc, &k1s, &c2s, s);
+		radix_sort<K, uint64_t>(static_cast<K *>(k1), c2, n, rs_passes<K>(range[0], range[1]), sc, &k1s, &c2s, s,
+		                        hist1);
 	}
 	alloc_tree(t, s);
 

@@ -390,9 +390,12 @@ inline int rs_passes(K kmin, K kmax)
 // vals may be null (identity payload, 32-bit payloads only).  The sorted data is in
 // the buffers returned through *keys_res / *vals_res (the input buffers or the
 // scratch ones; *vals_res stays null when passes == 0 and vals is null).  `hist` and
-// `counters` must be adjacent (rs_misc_words()).
+// `counters` must be adjacent (rs_misc_words()).  pre_hist (optional): the keys'
+// digit counts, already made (pre_hist[p * 256 + v] = keys whose digit p is v), in
+// place of the histogram pass.
 template <typename K, typename V>
-void radix_sort(K *keys, V *vals, uint64_t n, int passes, SortScratch &sc, K **keys_res, V **vals_res, cudaStream_t s)
+void radix_sort(K *keys, V *vals, uint64_t n, int passes, SortScratch &sc, K **keys_res, V **vals_res, cudaStream_t s,
+                const uint32_t *pre_hist = nullptr)
 {
 	*keys_res = keys;
 	*vals_res = vals;
@@ -406,13 +409,15 @@ void radix_sort(K *keys, V *vals, uint64_t n, int passes, SortScratch &sc, K **k
 	PST_CUDA(cudaMemsetAsync(sc.hist, 0, rs_misc_words() * 4, s));
 	const unsigned hg = (unsigned) std::min<uint64_t>((n + RS_THREADS - 1) / RS_THREADS,
 	                                                  (uint64_t) device_info().sms * 4);
-	k_rs_global_hist<K><<<hg, RS_THREADS, 4 * passes * 256 * 4, s>>>(keys, n, passes, sc.hist);
+	if (!pre_hist)
+		k_rs_global_hist<K><<<hg, RS_THREADS, 4 * passes * 256 * 4, s>>>(keys, n, passes, sc.hist);
+	const uint32_t *hist = pre_hist ? pre_hist : sc.hist;
 	K *kin = keys, *kout = static_cast<K *>(sc.keys_alt);
 	V *vin = vals;
 	V *vout = static_cast<V *>(sc.vals_alt);
 	for (int p = 0; p < passes; p++) {
 		k_rs_onesweep<K, V><<<(unsigned) tiles, RS_THREADS, rs_onesweep_smem<K, V>(), s>>>(
-		    kin, vin, kout, vout, n, 8 * p, sc.hist + 256 * p, sc.status, sc.counters + p, sc.epoch++, sc.err);
+		    kin, vin, kout, vout, n, 8 * p, hist + 256 * p, sc.status, sc.counters + p, sc.epoch++, sc.err);
 		PST_CUDA(cudaGetLastError());
 		K *kt = kin;
 		kin = kout;
