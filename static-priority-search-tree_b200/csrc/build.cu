@@ -391,7 +391,8 @@ __global__ void __launch_bounds__(AM_THREADS) k_level_argmax(const uint64_t *__r
                                                              const uint32_t *__restrict__ taken,
                                                              const uint64_t *__restrict__ tmax, uint64_t n,
                                                              const uint32_t *__restrict__ B, uint32_t nseg,
-                                                             unsigned long long *best, const uint32_t *err)
+                                                             unsigned long long *best, const uint32_t *err,
+                                                             float seg_per_pos)
 {
 	if (*err)  // after an error the bounds may hold unwritten entries
 		return;
@@ -407,16 +408,16 @@ __global__ void __launch_bounds__(AM_THREADS) k_level_argmax(const uint64_t *__r
 		uint32_t seg = 0xFFFFFFFFu;
 		uint64_t seg_end = 0;
 		if (valid) {
-			uint32_t lo = 0, hi = nseg;  // largest s with B[s] <= t0
-			while (hi - lo > 1) {
-				const uint32_t mid = (lo + hi) / 2;
-				if (B[mid] <= t0)
-					lo = mid;
-				else
-					hi = mid;
-			}
-			seg = lo;
-			seg_end = B[lo + 1];
+			// the largest s with B[s] <= t0: the level's segments are all within a few
+			// positions of n / nseg long, so s lies next to t0 * nseg / n and a short
+			// walk from there finds it (B increases, B[0] = 0)
+			uint32_t g = min((uint32_t) ((float) t0 * seg_per_pos), nseg - 1);
+			while (g > 0 && B[g] > t0)
+				g--;
+			while (g + 1 < nseg && B[g + 1] <= t0)
+				g++;
+			seg = g;
+			seg_end = B[g + 1];
 		}
 		const bool whole = valid && t1 <= seg_end;
 		uint64_t v = whole ? tmax[t] : 0;
@@ -1159,7 +1160,8 @@ void build_impl(TreeStorage &t, const void *pts_d, uint64_t n, cudaStream_t s)
 		for (uint32_t d = 0; d < L0; d++) {
 			const uint32_t nseg = 1u << d;
 			PST_CUDA(cudaMemsetAsync(best, 0, (size_t) nseg * 8, s));
-			k_level_argmax<<<am_grid, AM_THREADS, 0, s>>>(c2s, c.taken, c.tmax, n, B, nseg, best, c.err);
+			k_level_argmax<<<am_grid, AM_THREADS, 0, s>>>(c2s, c.taken, c.tmax, n, B, nseg, best, c.err,
+			                                               (float) ((double) nseg / (double) n));
 			k_level_nodes<T, HAS_ID><<<(nseg + 127) / 128, 128, 0, s>>>(c, d, B, Bn, best);
 			if (d + 1 < L0)
 				k_tile_refresh<<<(unsigned) ((nseg * 32 + AM_THREADS - 1) / AM_THREADS), AM_THREADS, 0, s>>>(
